@@ -1,0 +1,331 @@
+"""Benchmark: SEM forward+adjoint solves/s, batched vs plain, on one B200 per rank.
+
+Workload (default): batched ELBO sampling — 256 velocity models on one 100x50-element,
+order-4 mesh over 2000x1000 m (80,601 nodes), each the three-layer 1500/2200/3000 m/s
+base (interfaces at 300/650 m) plus a cubic tensor B-spline perturbation on a 10x6
+node grid with N(0, 100^2) m/s node values drawn from a seed; Ricker 10 Hz at
+(1000, 20), 100 receivers at 10 m depth, 3000 steps at the CFL limit, sponge 200 m on
+all sides, float32 wavefields, float64 misfit and gradient accumulation.  Observed data
+come from a seeded "true" perturbation.  Inputs are synthetic (no dataset involved).
+
+A step = one batched forward+adjoint pass over all 256 models.  ``value`` is
+device-timed with CUDA events (inputs resident), ``e2e`` is the same step through the
+public API with host arrays copied in and gradients/logliks copied out inside the
+timed region.  ``plain`` times one-at-a-time solves of the same models.
+
+``--impl reference`` times the oracle restatement of MUN's CPU path (torch-CPU float64,
+same library calls as the reference) on a bounded sample of the same workload.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, HERE)
+
+BYTES_PER_NODE_STEP_FWDADJ = 56  # algorithmic bytes (float32 state, float64 gradient RMW)
+
+
+def workload(nmodels=256, nelx=100, nelz=50, nt=3000, nrec=100, seed0=0):
+    from mun_b200.bspline import grid_basis, layered_velocity
+    from mun_b200.mesh import create_global_mesh
+    xmin, xmax, zmin, zmax, N = 0.0, 2000.0, 0.0, 1000.0, 4
+    coords, _, node_grid = create_global_mesh(xmin, xmax, zmin, zmax, nelx, nelz, N)
+    base = layered_velocity(coords[:, 1], [300.0, 650.0], [1500.0, 2200.0, 3000.0])
+    B = grid_basis(coords, (xmin, xmax), (zmin, zmax), 10, 6)
+    thetas = np.stack([np.random.default_rng(seed0 + i).normal(0.0, 100.0, 60) for i in range(nmodels)])
+    vels = base[None, :] + thetas @ B.T
+    theta_true = np.random.default_rng(12345).normal(0.0, 100.0, 60)
+    v_true = base + B @ theta_true
+    cmax = max(float(vels.max()), float(v_true.max()))
+    dt = 0.35 * (min((xmax - xmin) / nelx, (zmax - zmin) / nelz) / (N + 1)) / (cmax * (N + 1) * np.sqrt(2.0))
+    rec = np.stack([np.linspace(xmin, xmax, nrec), np.full(nrec, 10.0)], 1)
+    plan_kw = dict(xmin=xmin, xmax=xmax, zmin=zmin, zmax=zmax, nelx=nelx, nelz=nelz, npol=N, dt=dt,
+                   nt=nt, src_xz=(1000.0, 20.0), f0=10.0, amp=1.0, receivers=rec,
+                   pml_thickness=200.0, sponge_cmax=3000.0, coords=coords, node_grid=node_grid)
+    return dict(plan_kw=plan_kw, vels=vels, v_true=v_true, thetas=thetas, B=B, coords=coords,
+                npoints=len(coords), dt=dt, nt=nt, sigma=1e-3)
+
+
+class Clocks:
+    """nvidia-smi sampler running during the timed region."""
+
+    def __init__(self, path):
+        self.path = path
+        self.p = None
+
+    def __enter__(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.f = open(self.path, "w")
+            self.p = subprocess.Popen(["nvidia-smi", f"--query-gpu={q}", "--format=csv,noheader,nounits",
+                                       "-lms", "200"], stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.p = None
+        return self
+
+    def __exit__(self, *a):
+        if self.p is not None:
+            self.p.terminate()
+            try:
+                self.p.wait(timeout=5)
+            except Exception:
+                self.p.kill()
+            self.f.close()
+
+    def summary(self, device_index=0):
+        try:
+            rows = [l.split(",") for l in open(self.path).read().strip().splitlines()]
+            rows = [[x.strip() for x in r] for r in rows if len(r) >= 9 and r[0].strip() == str(device_index)]
+            sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+            mx = float(rows[0][2]) if rows else None
+            reasons = set()
+            names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+            for r in rows:
+                for nm, v in zip(names, r[5:9]):
+                    if v.lower().startswith("active"):
+                        reasons.add(nm)
+            return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx,
+                    "reasons": sorted(reasons), "samples": len(sm)}
+        except Exception as exc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "error": str(exc)}
+
+
+def peaks():
+    try:
+        return json.load(open(os.path.join(HERE, "MEASURED_PEAKS.json"))), "measured"
+    except Exception:
+        return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}, "fallback"
+
+
+def cpu_baseline(W, nt_sample, threads):
+    """Oracle restatement of the reference's CPU path on one model, truncated nt."""
+    import torch
+    from oracle import sem_oracle as so
+    torch.set_num_threads(threads)
+    kw = W["plan_kw"]
+    cfg = {"domain": {"xmin": kw["xmin"], "xmax": kw["xmax"], "zmin": kw["zmin"], "zmax": kw["zmax"],
+                      "nelem_x": kw["nelx"], "nelem_z": kw["nelz"]},
+           "time": {"total_time": (nt_sample - 0.5) * W["dt"], "dt": W["dt"]},
+           "source": {"position": kw["src_xz"], "frequency": kw["f0"], "amplitude": kw["amp"]},
+           "receivers": {"positions": kw["receivers"]},
+           "method": {"polynomial_order": kw["npol"], "pml_thickness": kw["pml_thickness"]},
+           "velocity": {"outside_velocity": kw["sponge_cmax"]}}
+    sim = so.build_sim(cfg, W["vels"][0], dt=W["dt"])
+    y = np.zeros((sim.nt, len(kw["receivers"])))
+    t0 = time.perf_counter()
+    so.forward_adjoint(sim, y, W["sigma"])
+    el = time.perf_counter() - t0
+    per_solve = el * (W["nt"] / nt_sample)
+    return per_solve, el
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    threads = os.cpu_count() or 1
+    W = workload(nmodels=1)
+    nt_sample = args.ref_nt
+    for _ in range(args.warmup):
+        cpu_baseline(W, nt_sample, threads)
+    times = []
+    for _ in range(args.steps):
+        per, _ = cpu_baseline(W, nt_sample, threads)
+        times.append(per)
+    per = float(np.mean(times))
+    val = 1.0 / per
+    out = {"metric": "SEM fwd+adjoint solves/s", "value": val, "unit": "solves/s",
+           "impl": "reference", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+           "ms_per_step": per * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+           "dtype": "f64", "data": "synthetic",
+           "config": {"workload": "batched ELBO sampling: 100x50 el, N=4, 80601 nodes, 3000 steps",
+                      "sample": f"1 model, {nt_sample} of 3000 steps, extrapolated linearly"},
+           "cpu_baseline": {"value": val, "unit": "solves/s", "cores": threads, "kind": "port",
+                            "sample": f"1 model x {nt_sample} steps (of 3000), x{3000 / nt_sample:.0f}"},
+           "e2e": {"value": val, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(out), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="mun", choices=["mun", "reference"])
+    ap.add_argument("--models", type=int, default=256)
+    ap.add_argument("--nt", type=int, default=3000)
+    ap.add_argument("--plain", type=int, default=6, help="one-at-a-time solves timed")
+    ap.add_argument("--tile", default="8x8")
+    ap.add_argument("--graph-chunk", type=int, default=0)
+    ap.add_argument("--ckpt-k", type=int, default=0)
+    ap.add_argument("--ref-nt", type=int, default=200)
+    ap.add_argument("--cpu-nt", type=int, default=200)
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+
+    import torch
+    import torch.distributed as dist
+    from mun_b200 import Batch, SEMPlan, SolveSpec
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+
+    W = workload(nmodels=args.models, nt=args.nt, seed0=1000 * rank)
+    plan = SEMPlan(**W["plan_kw"])
+    dev = torch.device("cuda", local)
+    tex, tez = (int(x) for x in args.tile.split("x"))
+    batch = Batch(tile=(tex, tez), graph_chunk=args.graph_chunk)
+    stream = torch.cuda.Stream()
+
+    # observed data from the "true" model, once
+    with torch.cuda.stream(stream):
+        obs = SolveSpec(plan, torch.as_tensor(W["v_true"], device=dev), shift=True)
+        batch.run([obs])
+    stream.synchronize()
+    y = obs.rec.double()
+    inv_s2 = 1.0 / (W["sigma"] ** 2 + 1e-24)
+    vel_dev = torch.as_tensor(W["vels"], device=dev)
+    n = args.models
+
+    def make_specs(v):
+        return [SolveSpec(plan, v[i], adjoint=True, y_obs=y, inv_sigma2=inv_s2, ckpt_k=args.ckpt_k)
+                for i in range(n)]
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    # ---------------- device-resident batched step
+    specs = make_specs(vel_dev)
+    with torch.cuda.stream(stream):
+        for _ in range(args.warmup):
+            batch.run(specs)
+    stream.synchronize()
+    k_used = None
+    launches_per_step = batch.last_launches
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    step_ms = []
+    clocks = Clocks(os.path.join(HERE, "gpurun_out", f"clocks_r{rank}.csv") if os.path.isdir(
+        os.path.join(HERE, "gpurun_out")) else f"/tmp/clocks_r{rank}.csv")
+    barrier()
+    torch.cuda.synchronize()
+    with clocks:
+        for _ in range(args.steps):
+            with torch.cuda.stream(stream):
+                ev0.record(stream)
+                batch.run(specs)
+                ev1.record(stream)
+            ev1.synchronize()
+            step_ms.append(ev0.elapsed_time(ev1))
+    torch.cuda.synchronize()
+    barrier()
+    ms = float(np.mean(step_ms))
+    if world > 1:
+        t = torch.tensor([ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    status = torch.cat([s.status for s in specs]).max().item()
+    value = n * world / (ms / 1e3)
+
+    # ---------------- end to end through the public API with host buffers
+    pin_v = torch.as_tensor(W["vels"]).pin_memory()
+    pin_y = y.cpu().pin_memory()
+    out_g = torch.empty((n, W["npoints"]), dtype=torch.float64).pin_memory()
+    out_l = torch.empty(n, dtype=torch.float64).pin_memory()
+    e2e_ms = []
+    for it in range(args.warmup + args.steps):
+        torch.cuda.synchronize()
+        with torch.cuda.stream(stream):
+            ev0.record(stream)
+            v = pin_v.to(dev, non_blocking=True)
+            yy = pin_y.to(dev, non_blocking=True)
+            sp = [SolveSpec(plan, v[i], adjoint=True, y_obs=yy, inv_sigma2=inv_s2, ckpt_k=args.ckpt_k)
+                  for i in range(n)]
+            batch.run(sp)
+            out_g.copy_(torch.stack([s.grad for s in sp]), non_blocking=True)
+            out_l.copy_(torch.cat([s.loglik for s in sp]), non_blocking=True)
+            ev1.record(stream)
+        ev1.synchronize()
+        if it >= args.warmup:
+            e2e_ms.append(ev0.elapsed_time(ev1))
+    e2e = float(np.mean(e2e_ms))
+    h2d = pin_v.numel() * 8 + pin_y.numel() * 8
+    d2h = out_g.numel() * 8 + out_l.numel() * 8
+
+    # ---------------- plain: one solve at a time (same models)
+    plain_ms = []
+    with torch.cuda.stream(stream):
+        for i in range(args.warmup + args.plain):
+            s = SolveSpec(plan, vel_dev[i % n], adjoint=True, y_obs=y, inv_sigma2=inv_s2,
+                          ckpt_k=args.ckpt_k)
+            ev0.record(stream)
+            batch.run([s])
+            ev1.record(stream)
+            ev1.synchronize()
+            if i >= args.warmup:
+                plain_ms.append(ev0.elapsed_time(ev1))
+    plain_ms = np.array(plain_ms)
+    plain_value = 1e3 / plain_ms.mean()
+
+    # ---------------- roofline of the dominant kernel (sem_tick_kernel<4>)
+    pk, pk_kind = peaks()
+    alg_bytes = BYTES_PER_NODE_STEP_FWDADJ * W["npoints"] * W["nt"] * n
+    achieved = alg_bytes / (ms / 1e3) / 1e9
+    peak = float(pk.get("hbm_gbs", 6650.0))
+
+    cpu = None
+    if rank == 0 and not args.no_cpu:
+        threads = os.cpu_count() or 1
+        per, el = cpu_baseline(W, args.cpu_nt, threads)
+        cpu = {"value": 1.0 / per, "unit": "solves/s", "cores": threads, "kind": "port",
+               "sample": f"1 model x {args.cpu_nt} of {W['nt']} steps ({el:.1f} s), extrapolated x{W['nt'] / args.cpu_nt:.0f}"}
+    if rank == 0:
+        out = {
+            "metric": "SEM fwd+adjoint solves/s (batched vs plain, same GPU, <=1e-4 rel); p50/p99 ms",
+            "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32 state / f64 misfit+gradient", "data": "synthetic",
+            "config": {"workload": "batched ELBO sampling (256 models, 100x50 el, N=4, 80601 nodes, "
+                                   "3000 steps, 100 receivers)",
+                       "models_per_gpu": n, "nodes": W["npoints"], "nt": W["nt"],
+                       "tile": args.tile, "graph_chunk": args.graph_chunk,
+                       "l2": "inputs larger than L2 (state+c2 of 256 models ~250 MB per field set)",
+                       "parallelism": f"replicas x{world}"},
+            "plain": {"value": plain_value, "unit": "solves/s", "p50_ms": float(np.percentile(plain_ms, 50)),
+                      "p99_ms": float(np.percentile(plain_ms, 99)), "solves": int(len(plain_ms))},
+            "batched_over_plain": value / world / plain_value,
+            "latency_ms": {"p50": float(np.percentile(step_ms, 50)), "p99": float(np.percentile(step_ms, 99))},
+            "mnode_steps_per_s": W["npoints"] * W["nt"] * n * world / (ms / 1e3) / 1e6,
+            "e2e": {"value": n * world / (e2e / 1e3), "unit": "solves/s", "h2d_bytes_per_step": int(h2d),
+                    "d2h_bytes_per_step": int(d2h)},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": None, "peak_kind": pk_kind,
+                         "note": "56 B/node-step algorithmic over the whole step time (all launches)"},
+            "cpu_baseline": cpu,
+            "gpu_launches": int(launches_per_step * args.steps),
+            "status": int(status),
+            "clocks": clocks.summary(local),
+        }
+        print(json.dumps(out), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,128 @@
+/*
+ * mun_sem.h — C ABI of the B200 (sm_100a) SEM forward/adjoint solver.
+ *
+ * This is the boundary that MUN's Python ``sem_waveform`` package would bind with
+ * ctypes.  Every entry point replaces a piece of the reference's CPU path:
+ *
+ *   sem_plan_create     <- SEMSimulation._initialize_components
+ *                          (Bspline_Coupling/SEM/sem_waveform/core.py:151-325): mesh,
+ *                          GLL operators, lumped mass, sponge, source, receivers.
+ *   sem_run             <- SEMSimulation.run / _time_stepping_loop_torch
+ *                          (core.py:334-435, 598-659) and
+ *                          SEMSimulation.run_forward_and_adjoint (core.py:1067-1371):
+ *                          forward loop, misfit, adjoint loop and the per-step
+ *                          sensitivity accumulate_sensitivity_dJdc_torch (core.py:49-85)
+ *                          for one or many solves in one launch sequence.
+ *   sem_forward         <- SEMSimulation.run (single solve convenience).
+ *   sem_forward_adjoint <- SEMSimulation.run_forward_and_adjoint up to the node-space
+ *                          gradient dJ_dv (core.py:1278), single solve.
+ *
+ * All device pointers are plain CUDA device addresses; ``stream`` is a cudaStream_t
+ * passed as void*.  Calls are stream-ordered and return a status code.  A plan is
+ * read-only after creation and may be shared by threads; a batch must be used by one
+ * thread at a time (each thread uses its own batch).
+ */
+#ifndef MUN_SEM_H
+#define MUN_SEM_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* status codes; the Python layer maps them to ValueError / RuntimeError / MemoryError */
+enum {
+  SEM_OK = 0,
+  SEM_ERR_ARG = 1,        /* bad argument (reference: ValueError)                    */
+  SEM_ERR_CUDA = 2,       /* CUDA runtime error                                      */
+  SEM_ERR_OOM = 3,        /* device allocation failed                                */
+  SEM_ERR_NONFINITE = 4,  /* NaN/Inf detected in a wavefield (reported per solve)    */
+  SEM_ERR_TIMEOUT = 5,    /* a bounded device wait gave up                           */
+  SEM_ERR_UNSUPPORTED = 6 /* polynomial order outside 1..7                           */
+};
+
+/* sem_solve_t.flags */
+enum {
+  SEM_F_ADJOINT = 1,  /* run the adjoint sweep and accumulate the gradient          */
+  SEM_F_EXACT = 2,    /* apply the sponge inside the adjoint (exact discrete adjoint) */
+  SEM_F_MISFIT = 4,   /* accumulate sum of squared residuals against y_obs          */
+  SEM_F_SHIFT = 8     /* record R u after the update (run_forward_and_adjoint);
+                         without it R u is recorded before the update (run())       */
+};
+
+typedef struct sem_plan_s sem_plan_t;
+typedef struct sem_batch_s sem_batch_t;
+
+/* Everything about one (mesh, order, dt, nt, source, receivers) signature.  All
+ * arrays are HOST pointers to float64 (converted to float32 on upload).  nxg =
+ * nelx*npol+1, nzg = nelz*npol+1. */
+typedef struct {
+  int32_t nelx, nelz, npol, nt;
+  int32_t npoints;          /* number of mesh nodes = nxg*nzg                         */
+  double dt;
+  const int64_t* node_grid; /* [npoints] gz*nxg+gx of each node in reference order    */
+  const double* gll_D;      /* [(npol+1)^2] D[a*(npol+1)+b] = l_b'(xi_a)              */
+  const double* gll_beta;   /* [npol+1] w_a * l_a  (GLL weight x Lagrange quirk factor)*/
+  const double* tab_x;      /* [3*nxg] 1/mx, Rx, sponge factor along x                */
+  const double* tab_z;      /* [3*nzg] dt^2/(J mz), Rz, sponge factor along z         */
+  const double* src_term;   /* [nt] dt^2 * s(t_it) added at the source node           */
+  int32_t src_gx, src_gz;   /* source node (structured index)                         */
+  int32_t nrec;
+  const int32_t* rec_base;  /* [nrec*2] (gx0,gz0) first node of the receiver element  */
+  const double* rec_w;      /* [nrec*(npol+1)^2] Lagrange weights, index j*(npol+1)+i */
+} sem_plan_desc_t;
+
+/* One solve inside sem_run.  Device pointers unless stated. */
+typedef struct {
+  const sem_plan_t* plan;
+  const double* velocity;   /* [npoints] nodal velocity, reference node order         */
+  int32_t flags;            /* SEM_F_*                                                */
+  int32_t ckpt_k;           /* checkpoint interval for the adjoint replay (>=2)       */
+  const double* y_obs;      /* [n_obs*nrec] observations on the misfit grid or NULL   */
+  int32_t it0, it1, decim;  /* misfit window [it0,it1) and decimation (0,nt,1 = all)  */
+  double inv_sigma2;        /* 1/(sigma^2 + 1e-24)                                    */
+  float* rec_out;           /* [nt*nrec] receiver traces                              */
+  double* loglik_out;       /* [1] -0.5*inv_sigma2*sum r^2 (SEM_F_MISFIT) or NULL     */
+  double* grad_out;         /* [npoints] dJ_dv of the reference (= d loglik / d c),
+                               reference node order (SEM_F_ADJOINT) or NULL           */
+  int32_t* status_out;      /* [1] per-solve status (SEM_OK / SEM_ERR_NONFINITE) or NULL */
+} sem_solve_t;
+
+/* Launch configuration (the autotuner's knobs). */
+typedef struct {
+  int32_t tile_ex, tile_ez;   /* elements per CTA tile in x and z                     */
+  int32_t threads;            /* threads per CTA (multiple of 32, <= 1024)            */
+  int32_t graph_chunk;        /* ticks per captured CUDA graph; 0 = plain launches    */
+} sem_launch_cfg_t;
+
+int sem_plan_create(const sem_plan_desc_t* desc, sem_plan_t** out);
+int sem_plan_destroy(sem_plan_t* plan);
+/* bytes of device workspace one solve of this plan needs with checkpoint interval k */
+int64_t sem_plan_workspace_bytes(const sem_plan_t* plan, int32_t flags, int32_t ckpt_k);
+
+int sem_batch_create(sem_batch_t** out);
+int sem_batch_destroy(sem_batch_t* batch);
+/* Run n solves (any mix of plans/orders/nt) to completion on ``stream``.  Solves of
+ * the same polynomial order share one kernel launch per time tick. */
+int sem_run(sem_batch_t* batch, const sem_solve_t* solves, int32_t n,
+            const sem_launch_cfg_t* cfg, void* stream);
+/* number of kernel launches issued by the last sem_run (for accounting) */
+int64_t sem_batch_last_launches(const sem_batch_t* batch);
+
+/* Single-solve conveniences (plain path): forward with receivers in the run()
+ * convention, and forward+adjoint in the run_forward_and_adjoint convention. */
+int sem_forward(sem_batch_t* batch, const sem_plan_t* plan, const double* velocity,
+                float* rec_out, void* stream);
+int sem_forward_adjoint(sem_batch_t* batch, const sem_plan_t* plan, const double* velocity,
+                        const double* y_obs, double inv_sigma2, int32_t exact,
+                        int32_t ckpt_k, float* clean_out, double* loglik_out,
+                        double* grad_out, void* stream);
+
+/* last error message of the calling thread (static storage) */
+const char* sem_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,92 @@
+"""ctypes binding of ``include/mun_sem.h`` (the library is ``mun_b200/_sem.so``).
+
+There is no CPU fallback: if the library is missing or fails to load, every entry
+point raises ``RuntimeError``.
+"""
+import ctypes as C
+import os
+
+from . import build as _build
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+
+SEM_OK, SEM_ERR_ARG, SEM_ERR_CUDA, SEM_ERR_OOM, SEM_ERR_NONFINITE, SEM_ERR_TIMEOUT, \
+    SEM_ERR_UNSUPPORTED = range(7)
+SEM_F_ADJOINT, SEM_F_EXACT, SEM_F_MISFIT, SEM_F_SHIFT = 1, 2, 4, 8
+
+
+class PlanDesc(C.Structure):
+    _fields_ = [("nelx", C.c_int32), ("nelz", C.c_int32), ("npol", C.c_int32), ("nt", C.c_int32),
+                ("npoints", C.c_int32), ("dt", C.c_double),
+                ("node_grid", C.POINTER(C.c_int64)), ("gll_D", C.POINTER(C.c_double)),
+                ("gll_beta", C.POINTER(C.c_double)), ("tab_x", C.POINTER(C.c_double)),
+                ("tab_z", C.POINTER(C.c_double)), ("src_term", C.POINTER(C.c_double)),
+                ("src_gx", C.c_int32), ("src_gz", C.c_int32), ("nrec", C.c_int32),
+                ("rec_base", C.POINTER(C.c_int32)), ("rec_w", C.POINTER(C.c_double))]
+
+
+class Solve(C.Structure):
+    _fields_ = [("plan", C.c_void_p), ("velocity", C.c_void_p), ("flags", C.c_int32),
+                ("ckpt_k", C.c_int32), ("y_obs", C.c_void_p), ("it0", C.c_int32),
+                ("it1", C.c_int32), ("decim", C.c_int32), ("inv_sigma2", C.c_double),
+                ("rec_out", C.c_void_p), ("loglik_out", C.c_void_p), ("grad_out", C.c_void_p),
+                ("status_out", C.c_void_p)]
+
+
+class LaunchCfg(C.Structure):
+    _fields_ = [("tile_ex", C.c_int32), ("tile_ez", C.c_int32), ("threads", C.c_int32),
+                ("graph_chunk", C.c_int32)]
+
+
+EXPORTS = ["sem_plan_create", "sem_plan_destroy", "sem_plan_workspace_bytes", "sem_batch_create",
+           "sem_batch_destroy", "sem_run", "sem_batch_last_launches", "sem_forward",
+           "sem_forward_adjoint", "sem_last_error"]
+
+_lib = None
+
+
+def load(path=None):
+    """Load (building first if the sources are newer and nvcc exists) the library."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    so = path or os.path.join(_HERE, "_sem.so")
+    if path is None:
+        try:
+            if _build.needs_build():
+                _build.build()
+        except Exception as exc:  # no nvcc: use what is there, or fail below
+            if not os.path.exists(so):
+                raise RuntimeError(f"mun_b200 CUDA library missing and cannot be built: {exc}")
+    if not os.path.exists(so):
+        raise RuntimeError(f"mun_b200 CUDA library not found at {so}")
+    lib = C.CDLL(so)
+    vp, i32, i64, dbl = C.c_void_p, C.c_int32, C.c_int64, C.c_double
+    lib.sem_plan_create.argtypes = [C.POINTER(PlanDesc), C.POINTER(vp)]
+    lib.sem_plan_destroy.argtypes = [vp]
+    lib.sem_plan_workspace_bytes.argtypes = [vp, i32, i32]
+    lib.sem_plan_workspace_bytes.restype = i64
+    lib.sem_batch_create.argtypes = [C.POINTER(vp)]
+    lib.sem_batch_destroy.argtypes = [vp]
+    lib.sem_run.argtypes = [vp, C.POINTER(Solve), i32, C.POINTER(LaunchCfg), vp]
+    lib.sem_batch_last_launches.argtypes = [vp]
+    lib.sem_batch_last_launches.restype = i64
+    lib.sem_forward.argtypes = [vp, vp, vp, vp, vp]
+    lib.sem_forward_adjoint.argtypes = [vp, vp, vp, vp, dbl, i32, i32, vp, vp, vp, vp]
+    lib.sem_last_error.restype = C.c_char_p
+    for name in EXPORTS:
+        if name not in ("sem_plan_workspace_bytes", "sem_batch_last_launches", "sem_last_error"):
+            getattr(lib, name).restype = C.c_int
+    _lib = lib
+    return lib
+
+
+def check(code):
+    if code == SEM_OK:
+        return
+    msg = load().sem_last_error().decode(errors="replace")
+    if code == SEM_ERR_ARG or code == SEM_ERR_UNSUPPORTED:
+        raise ValueError(f"mun_b200: {msg}")
+    if code == SEM_ERR_OOM:
+        raise MemoryError(f"mun_b200: {msg}")
+    raise RuntimeError(f"mun_b200 (status {code}): {msg}")

@@ -1,0 +1,996 @@
+// sem_kernels.cu — sm_100a kernels and C-ABI runtime for the 2-D acoustic SEM
+// forward solver and adjoint gradient of MUN's sem_waveform package.
+//
+// Discrete algorithm (restated, not translated):
+//   Forward step (Bspline_Coupling/SEM/sem_waveform/core.py:598-659, 1197-1211):
+//     n    = 2 b_t - d.b_{t-1} + dt^2 M^-1 (-K b_t + s_t M_src e_src)
+//     b_t+1 = d.n           (d = sponge decay, boundary.py:5-106)
+//   where the reference keeps (u_prev, u_curr) = (d.b_{t-1}, b_t); storing the
+//   undamped-by-the-second-factor pair (b_{t-1}, b_t) makes the state two fields.
+//   Adjoint step (core.py:1252-1275): the same recurrence run backwards with the
+//   source R^T r_it / sigma^2, no sponge (or the sponge, in exact mode), and the
+//   per-step sensitivity of core.py:49-85 accumulated in float64.
+//
+// Operator structure used here.  With rectangular affine elements and GLL
+// collocation, Gx = (2/dx) kron(L,D), Gz = (2/dz) kron(D,L) with L diagonal
+// (operators.py:6-42; L = diag(l) because of the 1e-12 in utils.py:31-37), so the
+// element stiffness splits into 1-D operators along grid lines:
+//   (K u)[gx,gz] = Rz[gz] * sum_{x-elements e ∋ gx} (D^T (beta c^2 (D u_e)))[i]
+//                + Rx[gx] * sum_{z-elements e ∋ gz} (D^T (beta c^2 (D u_e)))[j]
+// with beta_a = w_a l_a, Rz[gz] = J (2/dx)^2 sum_{z-elements} w_j l_j^3 and Rx the
+// same with x and z swapped; lumped mass and sponge are separable as well.  The same
+// split gives the sensitivity  dJ/dc^2 = Rz * sum beta (D u)(D lam) + Rx * (...).
+//
+// Kernel organisation (owner computes, no atomics): one CTA per tile of elements.
+// It stages the tile's node values plus an N-node halo (the neighbour elements'
+// nodes) in shared memory, evaluates every element segment that touches an owned
+// node (x-lines then z-lines), and writes each owned node once, summing the two
+// segment contributions of element-boundary nodes in a fixed order — deterministic
+// and bit-reproducible, so the checkpoint replay regenerates the forward exactly.
+//
+// Time program.  A "tick" advances every active solve of a batch by one action:
+// forward step t, one final receiver read-out, checkpoint replay step, or adjoint
+// step.  Each CTA decodes its solve's action from (tick - start_tick) with a pure
+// function, so a fixed launch sequence (capturable in a CUDA graph) drives any mix
+// of solves with different nt, checkpoint interval and polynomial order.
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <stdio.h>
+#include <string.h>
+
+#include <algorithm>
+#include <map>
+#include <mutex>
+#include <string>
+#include <tuple>
+#include <vector>
+
+#include "../../include/mun_sem.h"
+
+namespace {
+
+constexpr int kMaxN = 7;  // supported polynomial orders 1..7
+
+// ----------------------------------------------------------------------------
+// error plumbing
+// ----------------------------------------------------------------------------
+thread_local std::string g_err;
+
+int fail(int code, const std::string& msg) {
+  g_err = msg;
+  return code;
+}
+
+#define CUDA_TRY(expr)                                                           \
+  do {                                                                           \
+    cudaError_t _e = (expr);                                                     \
+    if (_e != cudaSuccess) {                                                     \
+      return fail(_e == cudaErrorMemoryAllocation ? SEM_ERR_OOM : SEM_ERR_CUDA,  \
+                  std::string(#expr) + ": " + cudaGetErrorString(_e));           \
+    }                                                                            \
+  } while (0)
+
+// ----------------------------------------------------------------------------
+// device-side solve descriptor
+// ----------------------------------------------------------------------------
+enum : int { F_ADJ = SEM_F_ADJOINT, F_EXACT = SEM_F_EXACT, F_MISFIT = SEM_F_MISFIT,
+             F_SHIFT = SEM_F_SHIFT };
+enum : int { A_NONE = 0, A_FWD = 1, A_FINAL = 2, A_REPLAY = 3, A_ADJ = 4, A_SCALE = 5 };
+
+struct SolveDev {
+  // geometry
+  int nelx, nelz, nxg, nzg, pitch;
+  int tiles_x, tiles_z, tile_base;
+  // program
+  int nt, k, nseg, flags, start_tick;
+  int it0, it1, decim;
+  int src_gx, src_gz;
+  int nrec;
+  long long fstride;  // floats per state field
+  // fields
+  const float* c2;
+  float* W;     // 2 fields   (forward scratch)
+  float* ckpt;  // 2*nseg fields; slots 0,1 hold the zero initial state
+  float* ring;  // k+2 fields (replayed segment)
+  float* L;     // 2 fields   (adjoint state)
+  double* grad; // 1 field of doubles (dJ/dc^2 accumulated over time)
+  // operators and tables
+  const float* D;     // (N+1)^2
+  const float* beta;  // N+1
+  const float* tx;    // 3*nxg
+  const float* tz;    // 3*nzg
+  const float* src_term;
+  // receivers
+  const int* rec_base;
+  const float* rec_w;
+  const int* rec_tile_off;
+  const int* rec_tile_ids;
+  const int* inj_tile_off;
+  const int* inj_tile_ids;
+  float* rec_out;
+  const double* yobs;
+  double* misfit;     // [nrec] sum of squared residuals
+  double* rmax;       // [nrec] max |residual| (sizes the adjoint source)
+  double* adj_scale;  // [1] power-of-two scale applied to the adjoint source
+  int* status;
+};
+
+__device__ __forceinline__ void decode(const SolveDev& s, int sig, int& act, int& t, int& seg) {
+  act = A_NONE;
+  t = 0;
+  seg = -1;
+  if (sig < 0) return;
+  if (sig < s.nt) { act = A_FWD; t = sig; return; }
+  sig -= s.nt;
+  if (s.flags & F_SHIFT) {
+    if (sig == 0) { act = A_FINAL; t = s.nt; return; }
+    sig -= 1;
+  }
+  if (!(s.flags & F_ADJ)) return;
+  if (sig == 0) { act = A_SCALE; return; }
+  sig -= 1;
+  const int jl = s.nseg - 1;
+  const int len_last = s.nt - jl * s.k;
+  if (sig < len_last) { act = A_ADJ; t = s.nt - 1 - sig; seg = jl; return; }
+  sig -= len_last;
+  if (sig >= 2 * s.k * jl) return;
+  const int j = jl - 1 - sig / (2 * s.k);
+  const int w = sig % (2 * s.k);
+  seg = j;
+  if (w < s.k) { act = A_REPLAY; t = j * s.k + w; }
+  else { act = A_ADJ; t = (j + 1) * s.k - 1 - (w - s.k); }
+}
+
+// where the forward state b_t lives during the forward sweep (t in [-1, nt])
+__device__ __forceinline__ float* fwd_loc(const SolveDev& s, int t) {
+  if (!(s.flags & F_ADJ)) return s.W + (long long)(t & 1) * s.fstride;
+  const int jl = s.nseg - 1;
+  if (t >= jl * s.k - 1) return s.ring + (long long)(t - jl * s.k + 1) * s.fstride;
+  if ((t + 1) % s.k == 0) return s.ckpt + (long long)(2 * ((t + 1) / s.k)) * s.fstride;
+  if (t % s.k == 0) return s.ckpt + (long long)(2 * (t / s.k) + 1) * s.fstride;
+  return s.W + (long long)(t & 1) * s.fstride;
+}
+
+// where b_t lives while segment j is replayed (t in [jk-1, jk+k])
+__device__ __forceinline__ float* replay_loc(const SolveDev& s, int j, int t) {
+  if (t == j * s.k - 1) return s.ckpt + (long long)(2 * j) * s.fstride;
+  if (t == j * s.k) return s.ckpt + (long long)(2 * j + 1) * s.fstride;
+  return s.ring + (long long)(t - j * s.k + 1) * s.fstride;
+}
+
+__host__ __device__ __forceinline__ int region_w(int tex, int N) { return ((tex + 2) * N + 1) | 1; }
+__host__ __device__ __forceinline__ int region_h(int tez, int N) { return (tez + 2) * N + 1; }
+
+// shared-memory floats needed by one CTA
+__host__ __device__ inline long long smem_floats(int N, int tex, int tez, bool adj) {
+  const int NP = N + 1;
+  const long long reg = (long long)region_w(tex, N) * region_h(tez, N);
+  const long long nro = (long long)(tez * N + 1) | 1, nco = (long long)(tex * N + 1) | 1;
+  const long long xseg = (long long)(tex + 1) * NP * nro, zseg = (long long)(tez + 1) * NP * nco;
+  long long f = 96 + 2 * reg + xseg + zseg;  // D, beta | u, c2 | K_x, K_z
+  if (adj) f += reg + xseg + zseg + nro * nco;  // forward field | S_x, S_z | injection
+  return f;
+}
+
+// ----------------------------------------------------------------------------
+// the tick kernel
+// ----------------------------------------------------------------------------
+template <int N>
+__global__ void __launch_bounds__(256) sem_tick_kernel(const SolveDev* __restrict__ solves,
+                                                       const int* __restrict__ cta_solve,
+                                                       const int* __restrict__ tick_ptr,
+                                                       int tex, int tez) {
+  constexpr int NP = N + 1;
+  extern __shared__ float smem[];
+  __shared__ SolveDev S;
+  __shared__ int s_act, s_t, s_seg;
+
+  const int sid = cta_solve[blockIdx.x];
+  if (threadIdx.x == 0) {
+    S = solves[sid];
+    int act, t, seg;
+    decode(S, *tick_ptr - S.start_tick, act, t, seg);
+    s_act = act; s_t = t; s_seg = seg;
+  }
+  __syncthreads();
+  const int act = s_act;
+  if (act == A_NONE) return;
+  const int t = s_t, seg = s_seg;
+  const bool adj = (act == A_ADJ);
+  if (act == A_SCALE) {
+    // one CTA per solve picks the power of two that brings max|r| to ~1, so the
+    // float32 adjoint field and the sensitivity products stay far from underflow
+    if (blockIdx.x == S.tile_base && threadIdx.x == 0) {
+      double m = 0.0;
+      for (int r = 0; r < S.nrec; ++r) m = fmax(m, S.rmax[r]);
+      *S.adj_scale = (m > 0.0 && isfinite(m)) ? ldexp(1.0, -ilogb(m)) : 1.0;
+    }
+    return;
+  }
+
+  // ---------------- tile geometry
+  const int lt = blockIdx.x - S.tile_base;
+  const int tx = lt % S.tiles_x, tz = lt / S.tiles_x;
+  const int ex0 = tx * tex, ex1 = min(ex0 + tex, S.nelx);
+  const int ez0 = tz * tez, ez1 = min(ez0 + tez, S.nelz);
+  const int gxo0 = ex0 * N, gxo1 = (ex1 == S.nelx) ? S.nxg : ex1 * N;
+  const int gzo0 = ez0 * N, gzo1 = (ez1 == S.nelz) ? S.nzg : ez1 * N;
+  const int nco = gxo1 - gxo0, nro = gzo1 - gzo0;
+  const int gxs = gxo0 - N, gzs = gzo0 - N;
+  const int SW = region_w(tex, N), SH = region_h(tez, N);
+  const int segx0 = max(ex0 - 1, 0), nsx = ex1 - segx0;
+  const int segz0 = max(ez0 - 1, 0), nsz = ez1 - segz0;
+  const int nrop = nro | 1, ncop = nco | 1;
+  const int REG = SW * SH;
+  const int nrop_max = (tez * N + 1) | 1, ncop_max = (tex * N + 1) | 1;
+
+  float* sD = smem;
+  float* sB = smem + 64;
+  float* su = smem + 96;                 // current field (b_t or lambda)
+  float* sc = su + REG;                  // c^2
+  float* sw = sc + REG;                  // forward field for the sensitivity (adjoint)
+  float* xr = sw + (adj ? REG : 0);
+  float* zr = xr + (tex + 1) * NP * nrop_max;
+  float* xs = zr + (tez + 1) * NP * ncop_max;
+  float* zs = xs + (tex + 1) * NP * nrop_max;
+  float* sacc = zs + (tez + 1) * NP * ncop_max;
+
+  const int nthr = blockDim.x;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = nthr >> 5;
+
+  // ---------------- which fields
+  const float* cur;
+  const float* prev = nullptr;
+  float* out = nullptr;
+  const float* fwdu = nullptr;
+  if (act == A_FWD) {
+    cur = fwd_loc(S, t); prev = fwd_loc(S, t - 1); out = fwd_loc(S, t + 1);
+  } else if (act == A_FINAL) {
+    cur = fwd_loc(S, t);
+  } else if (act == A_REPLAY) {
+    cur = replay_loc(S, seg, t); prev = replay_loc(S, seg, t - 1);
+    out = replay_loc(S, seg, t + 1);
+  } else {  // adjoint iteration it = t uses lambda_{t+1} (current) and lambda_{t+2}
+    cur = S.L + (long long)((t + 1) & 1) * S.fstride;
+    prev = S.L + (long long)(t & 1) * S.fstride;
+    out = S.L + (long long)(t & 1) * S.fstride;
+    fwdu = S.ring + (long long)(t + 1 - seg * S.k + 1) * S.fstride;
+  }
+
+  // ---------------- stage operators and the haloed tile
+  for (int i = threadIdx.x; i < NP * NP; i += nthr) sD[i] = S.D[i];
+  for (int i = threadIdx.x; i < NP; i += nthr) sB[i] = S.beta[i];
+  {
+    const int r0 = max(gzs, 0), r1 = min(gzs + SH, S.nzg);
+    const int c0 = max(gxs, 0), c1 = min(gxs + (ex1 - ex0 + 2) * N + 1, S.nxg);
+    const bool need_c = (act != A_FINAL);
+    for (int r = r0 + warp; r < r1; r += nwarps) {
+      const long long grow = (long long)r * S.pitch;
+      float* du = su + (r - gzs) * SW - gxs;
+      float* dc = sc + (r - gzs) * SW - gxs;
+      float* dw = sw + (r - gzs) * SW - gxs;
+      for (int c = c0 + lane; c < c1; c += 32) {
+        du[c] = __ldg(cur + grow + c);
+        if (need_c) dc[c] = __ldg(S.c2 + grow + c);
+        if (adj) dw[c] = __ldg(fwdu + grow + c);
+      }
+    }
+  }
+  __syncthreads();
+
+  // ---------------- receivers: record R b_t (forward sweep only)
+  if (act == A_FWD || act == A_FINAL) {
+    const int m = t - ((S.flags & F_SHIFT) ? 1 : 0);
+    if (m >= 0 && m < S.nt) {
+      const int off = S.rec_tile_off[lt], cnt = S.rec_tile_off[lt + 1] - off;
+      for (int q = warp; q < cnt; q += nwarps) {
+        const int r = S.rec_tile_ids[off + q];
+        const int bx = S.rec_base[2 * r], bz = S.rec_base[2 * r + 1];
+        const float* wr = S.rec_w + (long long)r * NP * NP;
+        float acc = 0.f;
+        for (int e = lane; e < NP * NP; e += 32) {
+          const int j = e / NP, i = e - j * NP;
+          acc = fmaf(wr[e], su[(bz + j - gzs) * SW + (bx + i - gxs)], acc);
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+        if (lane == 0) {
+          S.rec_out[(long long)m * S.nrec + r] = acc;
+          if ((S.flags & F_MISFIT) && m >= S.it0 && m < S.it1 && ((m - S.it0) % S.decim) == 0) {
+            const double res = (double)acc - S.yobs[(long long)((m - S.it0) / S.decim) * S.nrec + r];
+            S.misfit[r] += res * res;
+            S.rmax[r] = fmax(S.rmax[r], fabs(res));
+          }
+        }
+      }
+    }
+    if (act == A_FINAL) return;
+  }
+
+  // ---------------- adjoint source R^T r_it (deterministic order, warp 0)
+  const bool in_win = adj && t >= S.it0 && t < S.it1 && ((t - S.it0) % S.decim) == 0;
+  bool have_inj = false;
+  if (adj) {
+    const int off = S.inj_tile_off[lt], cnt = S.inj_tile_off[lt + 1] - off;
+    have_inj = in_win && cnt > 0;
+    if (have_inj) {
+      const double ascale = *S.adj_scale;
+      for (int i = threadIdx.x; i < nro * nco; i += nthr) sacc[i] = 0.f;
+      __syncthreads();
+      if (warp == 0) {
+        for (int q = 0; q < cnt; ++q) {
+          const int r = S.inj_tile_ids[off + q];
+          const double res = (double)S.rec_out[(long long)t * S.nrec + r] -
+                             S.yobs[(long long)((t - S.it0) / S.decim) * S.nrec + r];
+          const float rs = (float)(res * ascale);
+          const int bx = S.rec_base[2 * r], bz = S.rec_base[2 * r + 1];
+          const float* wr = S.rec_w + (long long)r * NP * NP;
+          for (int e = lane; e < NP * NP; e += 32) {
+            const int j = e / NP, i = e - j * NP;
+            const int gx = bx + i, gz = bz + j;
+            if (gx >= gxo0 && gx < gxo1 && gz >= gzo0 && gz < gzo1)
+              sacc[(gz - gzo0) * nco + (gx - gxo0)] += wr[e] * rs;
+          }
+          __syncwarp();
+        }
+      }
+    }
+  }
+
+  // ---------------- x-lines: one thread per (owned row, element segment)
+  for (int w = threadIdx.x; w < nro * nsx; w += nthr) {
+    const int r = w % nro, sg = w / nro;
+    const int ex = segx0 + sg;
+    const int base = (gzo0 + r - gzs) * SW + (ex * N - gxs);
+    float u[NP], c[NP], du[NP], q[NP];
+#pragma unroll
+    for (int a = 0; a < NP; ++a) { u[a] = su[base + a]; c[a] = sc[base + a]; }
+#pragma unroll
+    for (int a = 0; a < NP; ++a) {
+      float v = 0.f;
+#pragma unroll
+      for (int b = 0; b < NP; ++b) v = fmaf(sD[a * NP + b], u[b], v);
+      du[a] = v;
+      q[a] = sB[a] * c[a] * v;
+    }
+#pragma unroll
+    for (int i = 0; i < NP; ++i) {
+      float v = 0.f;
+#pragma unroll
+      for (int a = 0; a < NP; ++a) v = fmaf(sD[a * NP + i], q[a], v);
+      xr[(sg * NP + i) * nrop + r] = v;
+    }
+    if (adj) {
+#pragma unroll
+      for (int a = 0; a < NP; ++a) u[a] = sw[base + a];
+#pragma unroll
+      for (int a = 0; a < NP; ++a) {
+        float v = 0.f;
+#pragma unroll
+        for (int b = 0; b < NP; ++b) v = fmaf(sD[a * NP + b], u[b], v);
+        xs[(sg * NP + a) * nrop + r] = sB[a] * v * du[a];
+      }
+    }
+  }
+  // ---------------- z-lines: one thread per (owned column, element segment)
+  for (int w = threadIdx.x; w < nco * nsz; w += nthr) {
+    const int cc = w % nco, sg = w / nco;
+    const int ez = segz0 + sg;
+    const int base = (ez * N - gzs) * SW + (gxo0 + cc - gxs);
+    float u[NP], c[NP], du[NP], q[NP];
+#pragma unroll
+    for (int a = 0; a < NP; ++a) { u[a] = su[base + a * SW]; c[a] = sc[base + a * SW]; }
+#pragma unroll
+    for (int a = 0; a < NP; ++a) {
+      float v = 0.f;
+#pragma unroll
+      for (int b = 0; b < NP; ++b) v = fmaf(sD[a * NP + b], u[b], v);
+      du[a] = v;
+      q[a] = sB[a] * c[a] * v;
+    }
+#pragma unroll
+    for (int j = 0; j < NP; ++j) {
+      float v = 0.f;
+#pragma unroll
+      for (int a = 0; a < NP; ++a) v = fmaf(sD[a * NP + j], q[a], v);
+      zr[(sg * NP + j) * ncop + cc] = v;
+    }
+    if (adj) {
+#pragma unroll
+      for (int a = 0; a < NP; ++a) u[a] = sw[base + a * SW];
+#pragma unroll
+      for (int a = 0; a < NP; ++a) {
+        float v = 0.f;
+#pragma unroll
+        for (int b = 0; b < NP; ++b) v = fmaf(sD[a * NP + b], u[b], v);
+        zs[(sg * NP + a) * ncop + cc] = sB[a] * v * du[a];
+      }
+    }
+  }
+  __syncthreads();
+
+  // ---------------- owned nodes: assemble, Newmark, sponge, source / sensitivity
+  const bool damp = (act != A_ADJ) || (S.flags & F_EXACT);
+  const bool grad_on = adj && t >= S.it0 && t < S.it1;
+  bool bad = false;
+  for (int w = threadIdx.x; w < nro * nco; w += nthr) {
+    const int cc = w % nco, r = w / nco;
+    const int gx = gxo0 + cc, gz = gzo0 + r;
+    const int exr = gx / N, ia = gx - exr * N;
+    const int ezr = gz / N, ja = gz - ezr * N;
+    float X, Z, SX = 0.f, SZ = 0.f;
+    if (ia) {
+      const int o = ((exr - segx0) * NP + ia) * nrop + r;
+      X = xr[o];
+      if (adj) SX = xs[o];
+    } else {
+      X = 0.f;
+      if (exr >= 1) {
+        const int o = ((exr - 1 - segx0) * NP + N) * nrop + r;
+        X = xr[o];
+        if (adj) SX = xs[o];
+      }
+      if (exr < S.nelx) {
+        const int o = ((exr - segx0) * NP) * nrop + r;
+        X += xr[o];
+        if (adj) SX += xs[o];
+      }
+    }
+    if (ja) {
+      const int o = ((ezr - segz0) * NP + ja) * ncop + cc;
+      Z = zr[o];
+      if (adj) SZ = zs[o];
+    } else {
+      Z = 0.f;
+      if (ezr >= 1) {
+        const int o = ((ezr - 1 - segz0) * NP + N) * ncop + cc;
+        Z = zr[o];
+        if (adj) SZ = zs[o];
+      }
+      if (ezr < S.nelz) {
+        const int o = ((ezr - segz0) * NP) * ncop + cc;
+        Z += zr[o];
+        if (adj) SZ += zs[o];
+      }
+    }
+    const float ixv = __ldg(S.tx + gx), Rxv = __ldg(S.tx + S.nxg + gx);
+    const float izv = __ldg(S.tz + gz), Rzv = __ldg(S.tz + S.nzg + gz);
+    const float P = ixv * izv;
+    const float Kv = Rzv * X + Rxv * Z;
+    const long long g = (long long)gz * S.pitch + gx;
+    const float b = su[(gz - gzs) * SW + (gx - gxs)];
+    const float a = prev[g];
+    float res;
+    if (!adj) {
+      const float d = __ldg(S.tx + 2 * S.nxg + gx) * __ldg(S.tz + 2 * S.nzg + gz);
+      float n = 2.f * b - d * a - P * Kv;
+      if (gx == S.src_gx && gz == S.src_gz) n += S.src_term[t];
+      res = d * n;
+    } else {
+      const float inj = have_inj ? sacc[r * nco + cc] : 0.f;
+      if (damp) {
+        const float d = __ldg(S.tx + 2 * S.nxg + gx) * __ldg(S.tz + 2 * S.nzg + gz);
+        res = d * (2.f * b - d * a + P * (inj - Kv));
+      } else {
+        res = 2.f * b - a + P * (inj - Kv);
+      }
+      if (grad_on) S.grad[g] += (double)(Rzv * SX + Rxv * SZ);
+    }
+    out[g] = res;
+    bad |= !isfinite(res);
+  }
+  if (__any_sync(0xffffffffu, bad) && lane == 0) atomicOr(S.status, SEM_ERR_NONFINITE);
+}
+
+__global__ void tick_advance_kernel(int* tick) { *tick += 1; }
+
+// c (float64, reference order) -> c^2 (float32, pitched grid)
+__global__ void set_c2_kernel(const double* __restrict__ c, const int* __restrict__ pos,
+                              float* __restrict__ c2, int n) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const double v = c[i];
+    c2[pos[i]] = (float)(v * v);
+  }
+}
+
+// grad_out[i] = 2 c_i * acc[pos_i] * scale     (dJ/dc = 2c dJ/dc^2, core.py:84)
+__global__ void grad_out_kernel(const double* __restrict__ c, const int* __restrict__ pos,
+                                const double* __restrict__ acc, double inv_sigma2,
+                                const double* __restrict__ adj_scale, double* __restrict__ out,
+                                int n) {
+  const double scale = inv_sigma2 / *adj_scale;  // exact: adj_scale is a power of two
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    out[i] = 2.0 * c[i] * acc[pos[i]] * scale;
+}
+
+// loglik = -0.5 inv_sigma2 sum_r misfit_r   (fixed order: deterministic)
+__global__ void loglik_kernel(const double* __restrict__ misfit, int nrec, double inv_sigma2,
+                              double* __restrict__ out) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) {
+    double s = 0.0;
+    for (int r = 0; r < nrec; ++r) s += misfit[r];
+    *out = -0.5 * s * inv_sigma2;
+  }
+}
+
+__global__ void copy_status_kernel(const int* __restrict__ st, int* __restrict__ out) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) *out = *st;
+}
+
+}  // namespace
+
+// ============================================================================
+// host side
+// ============================================================================
+struct sem_plan_s {
+  int nelx, nelz, npol, nt, npoints, nxg, nzg, pitch, nrec, src_gx, src_gz, device;
+  double dt;
+  long long fstride;
+  float* D = nullptr;
+  float* beta = nullptr;
+  float* tx = nullptr;
+  float* tz = nullptr;
+  float* src_term = nullptr;
+  int* rec_base = nullptr;
+  float* rec_w = nullptr;
+  int* node_pos = nullptr;
+  std::vector<int> h_rec_base;
+  // receiver tile lists per (tile_ex, tile_ez): device arrays rec_off, rec_ids, inj_off, inj_ids
+  struct Lists { int* rec_off; int* rec_ids; int* inj_off; int* inj_ids; };
+  mutable std::map<std::pair<int, int>, Lists> lists;
+  mutable std::mutex mu;
+};
+
+namespace {
+
+template <class T>
+int upload(T** dst, const T* src, size_t n) {
+  CUDA_TRY(cudaMalloc((void**)dst, std::max<size_t>(n, 1) * sizeof(T)));
+  if (n) CUDA_TRY(cudaMemcpy(*dst, src, n * sizeof(T), cudaMemcpyHostToDevice));
+  return SEM_OK;
+}
+
+int upload_f32(float** dst, const double* src, size_t n) {
+  std::vector<float> tmp(n);
+  for (size_t i = 0; i < n; ++i) tmp[i] = (float)src[i];
+  return upload(dst, tmp.data(), n);
+}
+
+long long round_up(long long v, long long m) { return (v + m - 1) / m * m; }
+
+int tiles_of(const sem_plan_s* p, int tex, int tez, int* tx, int* tz) {
+  *tx = (p->nelx + tex - 1) / tex;
+  *tz = (p->nelz + tez - 1) / tez;
+  return (*tx) * (*tz);
+}
+
+int get_lists(const sem_plan_s* p, int tex, int tez, sem_plan_s::Lists* out) {
+  std::lock_guard<std::mutex> lk(p->mu);
+  auto key = std::make_pair(tex, tez);
+  auto it = p->lists.find(key);
+  if (it != p->lists.end()) { *out = it->second; return SEM_OK; }
+  int ntx, ntz;
+  const int ntiles = tiles_of(p, tex, tez, &ntx, &ntz);
+  const int N = p->npol;
+  std::vector<std::vector<int>> rec(ntiles), inj(ntiles);
+  for (int r = 0; r < p->nrec; ++r) {
+    const int bx = p->h_rec_base[2 * r], bz = p->h_rec_base[2 * r + 1];
+    const int ex = bx / N, ez = bz / N;
+    rec[(ez / tez) * ntx + (ex / tex)].push_back(r);
+    std::vector<int> seen;
+    for (int j = 0; j <= N; ++j)
+      for (int i = 0; i <= N; ++i) {
+        const int ox = std::min((bx + i) / (tex * N), ntx - 1);
+        const int oz = std::min((bz + j) / (tez * N), ntz - 1);
+        const int tt = oz * ntx + ox;
+        if (std::find(seen.begin(), seen.end(), tt) == seen.end()) seen.push_back(tt);
+      }
+    for (int tt : seen) inj[tt].push_back(r);
+  }
+  auto flat = [&](std::vector<std::vector<int>>& v, std::vector<int>& off, std::vector<int>& ids) {
+    off.assign(ntiles + 1, 0);
+    for (int i = 0; i < ntiles; ++i) off[i + 1] = off[i] + (int)v[i].size();
+    for (auto& x : v) ids.insert(ids.end(), x.begin(), x.end());
+  };
+  std::vector<int> ro, ri, io, ii;
+  flat(rec, ro, ri);
+  flat(inj, io, ii);
+  sem_plan_s::Lists L{};
+  int rc;
+  if ((rc = upload(&L.rec_off, ro.data(), ro.size()))) return rc;
+  if ((rc = upload(&L.rec_ids, ri.data(), ri.size()))) return rc;
+  if ((rc = upload(&L.inj_off, io.data(), io.size()))) return rc;
+  if ((rc = upload(&L.inj_ids, ii.data(), ii.size()))) return rc;
+  p->lists[key] = L;
+  *out = L;
+  return SEM_OK;
+}
+
+typedef void (*KernelFn)(const SolveDev*, const int*, const int*, int, int);
+KernelFn kernel_for(int N) {
+  switch (N) {
+    case 1: return sem_tick_kernel<1>;
+    case 2: return sem_tick_kernel<2>;
+    case 3: return sem_tick_kernel<3>;
+    case 4: return sem_tick_kernel<4>;
+    case 5: return sem_tick_kernel<5>;
+    case 6: return sem_tick_kernel<6>;
+    case 7: return sem_tick_kernel<7>;
+  }
+  return nullptr;
+}
+
+struct Workspace {
+  long long c2, W, ckpt, ring, L, grad, misfit, status;  // byte offsets
+  long long bytes;
+};
+
+Workspace layout(const sem_plan_s* p, int flags, int k, int* nseg_out) {
+  Workspace w{};
+  const long long F = p->fstride * 4;  // bytes per float field (multiple of 256)
+  const bool adj = flags & SEM_F_ADJOINT;
+  const int nseg = adj ? (p->nt + k - 1) / k : 1;
+  long long o = 0;
+  w.c2 = o; o += F;
+  w.W = o; o += 2 * F;
+  if (adj) {
+    w.ckpt = o; o += (long long)2 * nseg * F;
+    w.ring = o; o += (long long)(k + 2) * F;
+    w.L = o; o += 2 * F;
+    w.grad = o; o += 2 * F;
+  }
+  w.misfit = o; o += round_up((long long)(2 * p->nrec + 1) * 8, 256);  // misfit, rmax, scale
+  w.status = o; o += 256;
+  w.bytes = o;
+  *nseg_out = nseg;
+  return w;
+}
+
+}  // namespace
+
+struct sem_batch_s {
+  int device = -1;
+  char* arena = nullptr;
+  long long arena_bytes = 0;
+  int* d_tick = nullptr;
+  SolveDev* d_solves = nullptr;
+  int solves_cap = 0;
+  int* d_cta = nullptr;
+  long long cta_cap = 0;
+  long long last_launches = 0;
+  std::vector<SolveDev> h_solves;
+  std::vector<int> h_cta;
+};
+
+extern "C" {
+
+const char* sem_last_error(void) { return g_err.c_str(); }
+
+int sem_plan_create(const sem_plan_desc_t* d, sem_plan_t** out) {
+  if (!d || !out) return fail(SEM_ERR_ARG, "null argument");
+  if (d->npol < 1 || d->npol > kMaxN) return fail(SEM_ERR_UNSUPPORTED, "polynomial order must be 1..7");
+  if (d->nelx < 1 || d->nelz < 1 || d->nt < 1 || d->nrec < 0)
+    return fail(SEM_ERR_ARG, "bad mesh / nt / nrec");
+  const int nxg = d->nelx * d->npol + 1, nzg = d->nelz * d->npol + 1;
+  if ((long long)nxg * nzg != d->npoints) return fail(SEM_ERR_ARG, "npoints != nxg*nzg");
+  if (d->src_gx < 0 || d->src_gx >= nxg || d->src_gz < 0 || d->src_gz >= nzg)
+    return fail(SEM_ERR_ARG, "source node outside the mesh");
+  auto* p = new sem_plan_s();
+  p->nelx = d->nelx; p->nelz = d->nelz; p->npol = d->npol; p->nt = d->nt;
+  p->npoints = d->npoints; p->nxg = nxg; p->nzg = nzg; p->nrec = d->nrec;
+  p->src_gx = d->src_gx; p->src_gz = d->src_gz; p->dt = d->dt;
+  p->pitch = (int)round_up(nxg, 32);
+  p->fstride = round_up((long long)p->pitch * nzg, 64);
+  cudaGetDevice(&p->device);
+  const int NP = d->npol + 1;
+  int rc = SEM_OK;
+  std::vector<int> pos(d->npoints);
+  for (int i = 0; i < d->npoints; ++i) {
+    const long long g = d->node_grid[i];
+    if (g < 0 || g >= d->npoints) { delete p; return fail(SEM_ERR_ARG, "node_grid out of range"); }
+    pos[i] = (int)((g / nxg) * p->pitch + (g % nxg));
+  }
+  p->h_rec_base.assign(d->rec_base, d->rec_base + 2 * d->nrec);
+  for (int r = 0; r < d->nrec; ++r) {
+    const int bx = p->h_rec_base[2 * r], bz = p->h_rec_base[2 * r + 1];
+    if (bx < 0 || bz < 0 || bx % d->npol || bz % d->npol || bx + d->npol > nxg - 1 ||
+        bz + d->npol > nzg - 1) {
+      delete p;
+      return fail(SEM_ERR_ARG, "receiver element base outside the mesh");
+    }
+  }
+  if ((rc = upload_f32(&p->D, d->gll_D, NP * NP)) || (rc = upload_f32(&p->beta, d->gll_beta, NP)) ||
+      (rc = upload_f32(&p->tx, d->tab_x, 3 * nxg)) || (rc = upload_f32(&p->tz, d->tab_z, 3 * nzg)) ||
+      (rc = upload_f32(&p->src_term, d->src_term, d->nt)) ||
+      (rc = upload(&p->rec_base, d->rec_base, 2 * (size_t)d->nrec)) ||
+      (rc = upload_f32(&p->rec_w, d->rec_w, (size_t)d->nrec * NP * NP)) ||
+      (rc = upload(&p->node_pos, pos.data(), pos.size()))) {
+    sem_plan_destroy(p);
+    return rc;
+  }
+  *out = p;
+  return SEM_OK;
+}
+
+int sem_plan_destroy(sem_plan_t* p) {
+  if (!p) return SEM_OK;
+  cudaFree(p->D); cudaFree(p->beta); cudaFree(p->tx); cudaFree(p->tz); cudaFree(p->src_term);
+  cudaFree(p->rec_base); cudaFree(p->rec_w); cudaFree(p->node_pos);
+  for (auto& kv : p->lists) {
+    cudaFree(kv.second.rec_off); cudaFree(kv.second.rec_ids);
+    cudaFree(kv.second.inj_off); cudaFree(kv.second.inj_ids);
+  }
+  delete p;
+  return SEM_OK;
+}
+
+int64_t sem_plan_workspace_bytes(const sem_plan_t* p, int32_t flags, int32_t k) {
+  int nseg;
+  return layout(p, flags, std::max(2, (int)k), &nseg).bytes;
+}
+
+int sem_batch_create(sem_batch_t** out) {
+  if (!out) return fail(SEM_ERR_ARG, "null argument");
+  auto* b = new sem_batch_s();
+  cudaGetDevice(&b->device);
+  if (cudaMalloc((void**)&b->d_tick, 256) != cudaSuccess) {
+    delete b;
+    return fail(SEM_ERR_OOM, "cudaMalloc tick");
+  }
+  *out = b;
+  return SEM_OK;
+}
+
+int sem_batch_destroy(sem_batch_t* b) {
+  if (!b) return SEM_OK;
+  cudaFree(b->arena); cudaFree(b->d_tick); cudaFree(b->d_solves); cudaFree(b->d_cta);
+  delete b;
+  return SEM_OK;
+}
+
+int64_t sem_batch_last_launches(const sem_batch_t* b) { return b ? b->last_launches : -1; }
+
+int sem_run(sem_batch_t* b, const sem_solve_t* solves, int32_t n, const sem_launch_cfg_t* cfg_in,
+            void* stream_v) {
+  if (!b || (!solves && n) || n < 0) return fail(SEM_ERR_ARG, "null argument");
+  cudaStream_t stream = (cudaStream_t)stream_v;
+  sem_launch_cfg_t cfg = cfg_in ? *cfg_in : sem_launch_cfg_t{8, 8, 256, 0};
+  if (cfg.tile_ex < 1 || cfg.tile_ez < 1) return fail(SEM_ERR_ARG, "tile size must be >= 1");
+  if (cfg.threads < 32 || cfg.threads > 256 || cfg.threads % 32) cfg.threads = 256;
+  b->last_launches = 0;
+  if (n == 0) return SEM_OK;
+
+  // ---- validate and lay out workspaces
+  std::vector<Workspace> ws(n);
+  std::vector<int> nseg(n), kk(n), prog(n);
+  long long total = 0;
+  for (int i = 0; i < n; ++i) {
+    const sem_solve_t& s = solves[i];
+    if (!s.plan || !s.velocity || !s.rec_out) return fail(SEM_ERR_ARG, "solve missing plan/velocity/rec_out");
+    const bool adj = s.flags & SEM_F_ADJOINT;
+    if (adj && !(s.flags & SEM_F_SHIFT)) return fail(SEM_ERR_ARG, "adjoint requires the shifted receiver convention");
+    if ((adj || (s.flags & SEM_F_MISFIT)) && !s.y_obs) return fail(SEM_ERR_ARG, "y_obs required");
+    if (s.decim < 1 || s.it0 < 0 || s.it1 > s.plan->nt || s.it0 >= s.it1)
+      return fail(SEM_ERR_ARG, "bad misfit window");
+    kk[i] = adj ? std::max(2, std::min((int)s.ckpt_k, s.plan->nt)) : 2;
+    ws[i] = layout(s.plan, s.flags, kk[i], &nseg[i]);
+    total += ws[i].bytes;
+    const int nt = s.plan->nt;
+    prog[i] = nt + ((s.flags & SEM_F_SHIFT) ? 1 : 0) + (adj ? 1 + nt + kk[i] * (nseg[i] - 1) : 0);
+  }
+  if (total > b->arena_bytes) {
+    cudaFree(b->arena);
+    b->arena = nullptr;
+    b->arena_bytes = 0;
+    CUDA_TRY(cudaMalloc((void**)&b->arena, total));
+    b->arena_bytes = total;
+  }
+
+  // ---- group by polynomial order, build descriptors and CTA maps
+  std::vector<int> order(n);
+  for (int i = 0; i < n; ++i) order[i] = i;
+  std::stable_sort(order.begin(), order.end(),
+                   [&](int x, int y) { return solves[x].plan->npol < solves[y].plan->npol; });
+  b->h_solves.assign(n, SolveDev{});
+  b->h_cta.clear();
+  struct Group { int N; long long cta0, ncta; bool adj; };
+  std::vector<Group> groups;
+  long long off = 0;
+  int max_prog = 0;
+  std::vector<long long> base(n);
+  for (int oi = 0; oi < n; ++oi) {
+    const int i = order[oi];
+    const sem_solve_t& s = solves[i];
+    const sem_plan_s* p = s.plan;
+    if (p->device != b->device) return fail(SEM_ERR_ARG, "plan and batch on different devices");
+    sem_plan_s::Lists L;
+    int rc = get_lists(p, cfg.tile_ex, cfg.tile_ez, &L);
+    if (rc) return rc;
+    int ntx, ntz;
+    const int ntiles = tiles_of(p, cfg.tile_ex, cfg.tile_ez, &ntx, &ntz);
+    if (groups.empty() || groups.back().N != p->npol)
+      groups.push_back(Group{p->npol, (long long)b->h_cta.size(), 0, false});
+    Group& G = groups.back();
+    G.adj |= (s.flags & SEM_F_ADJOINT) != 0;
+    char* a = b->arena + off;
+    base[i] = off;
+    SolveDev& d = b->h_solves[oi];
+    d.nelx = p->nelx; d.nelz = p->nelz; d.nxg = p->nxg; d.nzg = p->nzg; d.pitch = p->pitch;
+    d.tiles_x = ntx; d.tiles_z = ntz;
+    d.tile_base = (int)(b->h_cta.size() - G.cta0);
+    d.nt = p->nt; d.k = kk[i]; d.nseg = nseg[i]; d.flags = s.flags; d.start_tick = 0;
+    d.it0 = s.it0; d.it1 = s.it1; d.decim = s.decim;
+    d.src_gx = p->src_gx; d.src_gz = p->src_gz; d.nrec = p->nrec;
+    d.fstride = p->fstride;
+    d.c2 = (const float*)(a + ws[i].c2);
+    d.W = (float*)(a + ws[i].W);
+    d.ckpt = (s.flags & SEM_F_ADJOINT) ? (float*)(a + ws[i].ckpt) : nullptr;
+    d.ring = (s.flags & SEM_F_ADJOINT) ? (float*)(a + ws[i].ring) : nullptr;
+    d.L = (s.flags & SEM_F_ADJOINT) ? (float*)(a + ws[i].L) : nullptr;
+    d.grad = (s.flags & SEM_F_ADJOINT) ? (double*)(a + ws[i].grad) : nullptr;
+    d.D = p->D; d.beta = p->beta; d.tx = p->tx; d.tz = p->tz; d.src_term = p->src_term;
+    d.rec_base = p->rec_base; d.rec_w = p->rec_w;
+    d.rec_tile_off = L.rec_off; d.rec_tile_ids = L.rec_ids;
+    d.inj_tile_off = L.inj_off; d.inj_tile_ids = L.inj_ids;
+    d.rec_out = s.rec_out; d.yobs = s.y_obs;
+    d.misfit = (double*)(a + ws[i].misfit);
+    d.rmax = d.misfit + p->nrec;
+    d.adj_scale = d.misfit + 2 * p->nrec;
+    d.status = (int*)(a + ws[i].status);
+    for (int c = 0; c < ntiles; ++c) b->h_cta.push_back(oi - 0);
+    G.ncta += ntiles;
+    max_prog = std::max(max_prog, prog[i]);
+    off += ws[i].bytes;
+  }
+  // cta map entries are indices into the group's descriptor sub-array
+  for (auto& G : groups) {
+    const int first = b->h_cta[G.cta0];
+    for (long long c = G.cta0; c < G.cta0 + G.ncta; ++c) b->h_cta[c] -= first;
+  }
+  if (n > b->solves_cap) {
+    cudaFree(b->d_solves);
+    b->d_solves = nullptr;
+    CUDA_TRY(cudaMalloc((void**)&b->d_solves, sizeof(SolveDev) * n));
+    b->solves_cap = n;
+  }
+  if ((long long)b->h_cta.size() > b->cta_cap) {
+    cudaFree(b->d_cta);
+    b->d_cta = nullptr;
+    CUDA_TRY(cudaMalloc((void**)&b->d_cta, sizeof(int) * b->h_cta.size()));
+    b->cta_cap = b->h_cta.size();
+  }
+  CUDA_TRY(cudaMemcpyAsync(b->d_solves, b->h_solves.data(), sizeof(SolveDev) * n,
+                           cudaMemcpyHostToDevice, stream));
+  CUDA_TRY(cudaMemcpyAsync(b->d_cta, b->h_cta.data(), sizeof(int) * b->h_cta.size(),
+                           cudaMemcpyHostToDevice, stream));
+
+  // ---- zero the state that must start at zero, stage c^2
+  for (int oi = 0; oi < n; ++oi) {
+    const int i = order[oi];
+    const sem_solve_t& s = solves[i];
+    const sem_plan_s* p = s.plan;
+    char* a = b->arena + base[i];
+    const long long F = p->fstride * 4;
+    if (s.flags & SEM_F_ADJOINT) {
+      CUDA_TRY(cudaMemsetAsync(a + ws[i].ckpt, 0, 2 * F, stream));
+      if (nseg[i] == 1) CUDA_TRY(cudaMemsetAsync(a + ws[i].ring, 0, 2 * F, stream));
+      CUDA_TRY(cudaMemsetAsync(a + ws[i].L, 0, 2 * F, stream));
+      CUDA_TRY(cudaMemsetAsync(a + ws[i].grad, 0, 2 * F, stream));
+    } else {
+      CUDA_TRY(cudaMemsetAsync(a + ws[i].W, 0, 2 * F, stream));
+    }
+    CUDA_TRY(cudaMemsetAsync(a + ws[i].misfit, 0, ws[i].status - ws[i].misfit + 256, stream));
+    set_c2_kernel<<<std::min(1024, (p->npoints + 255) / 256), 256, 0, stream>>>(
+        s.velocity, p->node_pos, (float*)(a + ws[i].c2), p->npoints);
+    b->last_launches++;
+  }
+  CUDA_TRY(cudaMemsetAsync(b->d_tick, 0, sizeof(int), stream));
+  CUDA_TRY(cudaGetLastError());
+
+  // ---- per-group launch parameters
+  struct Launch { KernelFn fn; long long cta0, ncta; size_t smem; };
+  std::vector<Launch> launches;
+  for (auto& G : groups) {
+    KernelFn fn = kernel_for(G.N);
+    if (!fn) return fail(SEM_ERR_UNSUPPORTED, "polynomial order");
+    const size_t smem = (size_t)smem_floats(G.N, cfg.tile_ex, cfg.tile_ez, G.adj) * sizeof(float);
+    if (smem > 227 * 1024) return fail(SEM_ERR_ARG, "tile too large for shared memory");
+    CUDA_TRY(cudaFuncSetAttribute((const void*)fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    launches.push_back(Launch{fn, G.cta0, G.ncta, smem});
+  }
+  // solve descriptor sub-array of each group starts at the first solve of that group
+  std::vector<const SolveDev*> gdesc;
+  {
+    int oi = 0;
+    for (auto& G : groups) {
+      gdesc.push_back(b->d_solves + oi);
+      while (oi < n && solves[order[oi]].plan->npol == G.N) ++oi;
+    }
+  }
+  auto launch_tick = [&]() -> int {
+    for (size_t gi = 0; gi < launches.size(); ++gi) {
+      const Launch& Lc = launches[gi];
+      Lc.fn<<<(unsigned)Lc.ncta, cfg.threads, Lc.smem, stream>>>(gdesc[gi], b->d_cta + Lc.cta0,
+                                                                 b->d_tick, cfg.tile_ex, cfg.tile_ez);
+    }
+    tick_advance_kernel<<<1, 1, 0, stream>>>(b->d_tick);
+    return SEM_OK;
+  };
+
+  // ---- the tick loop: plain launches or captured chunks
+  const long long per_tick = (long long)launches.size() + 1;
+  bool graphed = false;
+  if (cfg.graph_chunk > 0 && stream != nullptr && stream != cudaStreamLegacy &&
+      stream != cudaStreamPerThread) {
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    const int chunk = std::min(cfg.graph_chunk, max_prog);
+    if (cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
+      for (int c = 0; c < chunk; ++c) launch_tick();
+      cudaError_t e = cudaStreamEndCapture(stream, &graph);
+      if (e == cudaSuccess && cudaGraphInstantiate(&exec, graph, 0) == cudaSuccess) {
+        const int reps = (max_prog + chunk - 1) / chunk;
+        for (int r = 0; r < reps; ++r) CUDA_TRY(cudaGraphLaunch(exec, stream));
+        b->last_launches += (long long)reps * chunk * per_tick;
+        graphed = true;
+      }
+      if (exec) cudaGraphExecDestroy(exec);
+      if (graph) cudaGraphDestroy(graph);
+    }
+    cudaGetLastError();  // clear a failed capture
+  }
+  if (!graphed) {
+    for (int tick = 0; tick < max_prog; ++tick) launch_tick();
+    b->last_launches += (long long)max_prog * per_tick;
+  }
+  CUDA_TRY(cudaGetLastError());
+
+  // ---- outputs
+  for (int oi = 0; oi < n; ++oi) {
+    const int i = order[oi];
+    const sem_solve_t& s = solves[i];
+    const sem_plan_s* p = s.plan;
+    char* a = b->arena + base[i];
+    if ((s.flags & SEM_F_ADJOINT) && s.grad_out) {
+      grad_out_kernel<<<std::min(1024, (p->npoints + 255) / 256), 256, 0, stream>>>(
+          s.velocity, p->node_pos, (const double*)(a + ws[i].grad), s.inv_sigma2,
+          (const double*)(a + ws[i].misfit) + 2 * p->nrec, s.grad_out, p->npoints);
+      b->last_launches++;
+    }
+    if ((s.flags & SEM_F_MISFIT) && s.loglik_out) {
+      loglik_kernel<<<1, 32, 0, stream>>>((const double*)(a + ws[i].misfit), p->nrec, s.inv_sigma2,
+                                          s.loglik_out);
+      b->last_launches++;
+    }
+    if (s.status_out) {
+      copy_status_kernel<<<1, 32, 0, stream>>>((const int*)(a + ws[i].status), s.status_out);
+      b->last_launches++;
+    }
+  }
+  CUDA_TRY(cudaGetLastError());
+  return SEM_OK;
+}
+
+int sem_forward(sem_batch_t* b, const sem_plan_t* plan, const double* velocity, float* rec_out,
+                void* stream) {
+  if (!plan) return fail(SEM_ERR_ARG, "null plan");
+  sem_solve_t s{};
+  s.plan = plan; s.velocity = velocity; s.flags = 0; s.ckpt_k = 2;
+  s.it0 = 0; s.it1 = plan->nt; s.decim = 1; s.rec_out = rec_out;
+  return sem_run(b, &s, 1, nullptr, stream);
+}
+
+int sem_forward_adjoint(sem_batch_t* b, const sem_plan_t* plan, const double* velocity,
+                        const double* y_obs, double inv_sigma2, int32_t exact, int32_t ckpt_k,
+                        float* clean_out, double* loglik_out, double* grad_out, void* stream) {
+  if (!plan) return fail(SEM_ERR_ARG, "null plan");
+  sem_solve_t s{};
+  s.plan = plan; s.velocity = velocity;
+  s.flags = SEM_F_ADJOINT | SEM_F_MISFIT | SEM_F_SHIFT | (exact ? SEM_F_EXACT : 0);
+  s.ckpt_k = ckpt_k; s.y_obs = y_obs; s.it0 = 0; s.it1 = plan->nt; s.decim = 1;
+  s.inv_sigma2 = inv_sigma2; s.rec_out = clean_out; s.loglik_out = loglik_out; s.grad_out = grad_out;
+  return sem_run(b, &s, 1, nullptr, stream);
+}
+
+}  // extern "C"

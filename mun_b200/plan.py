@@ -1,0 +1,152 @@
+"""Host-side set-up of one solver plan and its C handle.
+
+Computes, in float64 on the host, everything the kernels read that does not depend on
+the velocity: 1-D operator tables, sponge factors, source term, receiver weights and
+the node permutation.  Mirrors ``SEMSimulation._initialize_components``
+(``Bspline_Coupling/SEM/sem_waveform/core.py:151-325``) and the helpers it calls:
+``operators.py:6-84`` (GLL operators, lumped mass), ``boundary.py:5-58`` (sponge),
+``sources.py:3-21`` (Ricker), ``receivers.py:6-80`` / layered ``core.py:90-172``
+(receiver interpolation), ``mesh.py:45-54`` (source snapping).
+"""
+import ctypes as C
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _lib
+from .gll import diff_matrix, gll_points, gll_weights, lagrange_basis, lagrange_diag
+from .mesh import create_global_mesh, find_closest_node, grid_coords_1d
+
+
+def ricker_source(nt, dt, f0, amp, t0=0.1, gate=0.3):
+    """Ricker wavelet minus its trapezoid mean over [0, (nt-1) dt], zero for t >= gate."""
+    t = np.arange(nt) * dt
+    a = (np.pi * f0 * (t - t0)) ** 2
+    s = (1.0 - 2.0 * a) * np.exp(-a) * amp
+    if nt > 1:
+        s = s - np.trapezoid(s, t) / (t[-1] - t[0])
+    s[~(t < gate)] = 0.0
+    return s
+
+
+def sponge_sigma_1d(coord, cmin, cmax_coord, thickness, c_max, R=1e-8):
+    """Cubic-ramp damping profile along one axis (boundary.py:5-58)."""
+    m = 3
+    d = float(thickness)
+    d0 = -(m + 1) * float(c_max) * np.log(R) / (2.0 * d)
+    s = np.zeros_like(coord)
+    lo, hi = coord < cmin + d, coord > cmax_coord - d
+    s[lo] = d0 * ((cmin + d - coord[lo]) / d) ** m
+    s[hi] = d0 * ((coord[hi] - (cmax_coord - d)) / d) ** m
+    return s
+
+
+def receiver_weights(positions, xmin, zmin, dx, dz, nelx, nelz, npol):
+    """(base (nrec,2) int32 = first node of the receiver element, weights (nrec,(N+1)^2))."""
+    nodes = gll_points(npol)
+    ng = npol + 1
+    pos = np.asarray(positions, dtype=np.float64).reshape(-1, 2)
+    base = np.zeros((len(pos), 2), dtype=np.int32)
+    w = np.zeros((len(pos), ng * ng))
+    for r, (rx, rz) in enumerate(pos):
+        ex = min(max(int((rx - xmin) / dx), 0), nelx - 1)
+        ez = min(max(int((rz - zmin) / dz), 0), nelz - 1)
+        xi = 2.0 * (rx - (xmin + ex * dx)) / dx - 1.0
+        eta = 2.0 * (rz - (zmin + ez * dz)) / dz - 1.0
+        lx = np.array([float(lagrange_basis(xi, i, nodes)) for i in range(ng)])
+        lz = np.array([float(lagrange_basis(eta, j, nodes)) for j in range(ng)])
+        w[r] = (lz[:, None] * lx[None, :]).reshape(-1)
+        base[r] = (ex * npol, ez * npol)
+    return base, w
+
+
+def build_plan_arrays(xmin, xmax, zmin, zmax, nelx, nelz, npol, dt, nt, src_xz, f0, amp,
+                      receivers, pml_thickness, sponge_cmax, coords=None, node_grid=None):
+    """All float64 inputs of ``sem_plan_create`` for one mesh/time/source/receiver set."""
+    N = int(npol)
+    nodes = gll_points(N)
+    w = gll_weights(nodes)
+    D = diff_matrix(nodes)
+    lq = lagrange_diag(nodes)
+    dx = (xmax - xmin) / nelx
+    dz = (zmax - zmin) / nelz
+    J = dx * dz * 0.25
+    sxi2, seta2 = (2.0 / dx) ** 2, (2.0 / dz) ** 2
+    nxg, nzg = nelx * N + 1, nelz * N + 1
+
+    def assemble_1d(nel, vals):
+        out = np.zeros(nel * N + 1)
+        for e in range(nel):
+            out[e * N:(e + 1) * N + 1] += vals
+        return out
+
+    mx = assemble_1d(nelx, w)
+    mz = assemble_1d(nelz, w)
+    wl3x = assemble_1d(nelx, w * lq ** 3)
+    wl3z = assemble_1d(nelz, w * lq ** 3)
+    xg = grid_coords_1d(xmin, xmax, nelx, N)
+    zg = grid_coords_1d(zmin, zmax, nelz, N)
+    dec_x = np.exp(-sponge_sigma_1d(xg, xmin, xmax, pml_thickness, sponge_cmax) * dt)
+    dec_z = np.exp(-sponge_sigma_1d(zg, zmin, zmax, pml_thickness, sponge_cmax) * dt)
+    tab_x = np.concatenate([1.0 / mx, J * seta2 * wl3x, dec_x])
+    tab_z = np.concatenate([dt * dt / (J * mz), J * sxi2 * wl3z, dec_z])
+    if coords is None or node_grid is None:
+        coords, _, node_grid = create_global_mesh(xmin, xmax, zmin, zmax, nelx, nelz, N)
+    src_node = find_closest_node(float(src_xz[0]), float(src_xz[1]), coords)
+    g = int(node_grid[src_node])
+    src = ricker_source(nt, dt, f0, amp)
+    base, rw = receiver_weights(receivers, xmin, zmin, dx, dz, nelx, nelz, N)
+    return dict(nelx=int(nelx), nelz=int(nelz), npol=N, nt=int(nt), dt=float(dt),
+                npoints=int(nxg * nzg), node_grid=np.ascontiguousarray(node_grid, dtype=np.int64),
+                gll_D=np.ascontiguousarray(D), gll_beta=w * lq, tab_x=tab_x, tab_z=tab_z,
+                src_term=dt * dt * src, src_gx=g % nxg, src_gz=g // nxg, src_node=src_node,
+                nrec=len(base), rec_base=np.ascontiguousarray(base), rec_w=np.ascontiguousarray(rw),
+                src_wavelet=src)
+
+
+def _dptr(a):
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+class SEMPlan:
+    """Owns a ``sem_plan_t`` (device-resident tables for one solver signature)."""
+
+    def __init__(self, **kw):
+        import torch
+        if not torch.cuda.is_available():
+            raise RuntimeError("mun_b200 needs a CUDA device (no CPU fallback)")
+        torch.cuda.init()
+        a = build_plan_arrays(**kw)
+        self.arrays = a
+        self.nt, self.npoints, self.nrec, self.npol = a["nt"], a["npoints"], a["nrec"], a["npol"]
+        self.dt = a["dt"]
+        self.nelx, self.nelz = a["nelx"], a["nelz"]
+        lib = _lib.load()
+        d = _lib.PlanDesc()
+        d.nelx, d.nelz, d.npol, d.nt, d.npoints, d.dt = (a["nelx"], a["nelz"], a["npol"], a["nt"],
+                                                         a["npoints"], a["dt"])
+        self._keep = [np.ascontiguousarray(a[k]) for k in
+                      ("node_grid", "gll_D", "gll_beta", "tab_x", "tab_z", "src_term", "rec_base", "rec_w")]
+        ng, Dm, beta, tx, tz, st, rb, rw = self._keep
+        d.node_grid = ng.ctypes.data_as(C.POINTER(C.c_int64))
+        d.gll_D, d.gll_beta, d.tab_x, d.tab_z, d.src_term = (_dptr(Dm), _dptr(beta), _dptr(tx),
+                                                             _dptr(tz), _dptr(st))
+        d.src_gx, d.src_gz, d.nrec = a["src_gx"], a["src_gz"], a["nrec"]
+        d.rec_base = rb.ctypes.data_as(C.POINTER(C.c_int32))
+        d.rec_w = _dptr(rw)
+        h = C.c_void_p()
+        _lib.check(lib.sem_plan_create(C.byref(d), C.byref(h)))
+        self.handle = h
+        self._lib = lib
+
+    def workspace_bytes(self, flags, ckpt_k):
+        return int(self._lib.sem_plan_workspace_bytes(self.handle, flags, ckpt_k))
+
+    def __del__(self):
+        h = getattr(self, "handle", None)
+        if h is not None and h.value:
+            try:
+                self._lib.sem_plan_destroy(h)
+            except Exception:
+                pass
+            self.handle = None
