@@ -2,11 +2,14 @@
 // forward solver and adjoint gradient of MUN's sem_waveform package.
 //
 // Discrete algorithm (restated, not translated):
-//   Forward step (Bspline_Coupling/SEM/sem_waveform/core.py:598-659, 1197-1211):
-//     n    = 2 b_t - d.b_{t-1} + dt^2 M^-1 (-K b_t + s_t M_src e_src)
-//     b_t+1 = d.n           (d = sponge decay, boundary.py:5-106)
-//   where the reference keeps (u_prev, u_curr) = (d.b_{t-1}, b_t); storing the
-//   undamped-by-the-second-factor pair (b_{t-1}, b_t) makes the state two fields.
+//   Forward step (Bspline_Coupling/SEM/sem_waveform/core.py:598-659, 1197-1211) keeps
+//   (u_prev, u_curr) and computes u_next = 2 u_curr - u_prev + dt^2 M^-1 (-K u_curr + f),
+//   then multiplies all three by the sponge decay d (boundary.py:5-106) and rotates.
+//   Here the state is (b, v) = (u_curr, u_curr - u_prev), which is the same recurrence:
+//     w = v - dt^2 M^-1 K b + dt^2 s_t e_src,   v' = d.w,   b' = d.(b + w)
+//   but keeps float32 rounding out of the velocity: storing two displacement levels
+//   rounds each independently and every rounding acts as a velocity kick amplified by
+//   1/(omega dt) (about 10-20x larger seismogram error, measured).
 //   Adjoint step (core.py:1252-1275): the same recurrence run backwards with the
 //   source R^T r_it / sigma^2, no sponge (or the sponge, in exact mode), and the
 //   per-step sensitivity of core.py:49-85 accumulated in float64.
@@ -50,7 +53,8 @@
 
 namespace {
 
-constexpr int kMaxN = 7;  // supported polynomial orders 1..7
+constexpr int kMaxN = 7;       // supported polynomial orders 1..7
+constexpr int kMaxInj = 1024;  // receivers whose element touches one tile (checked on the host)
 
 // ----------------------------------------------------------------------------
 // error plumbing
@@ -90,10 +94,12 @@ struct SolveDev {
   long long fstride;  // floats per state field
   // fields
   const float* c2;
-  float* W;     // 2 fields   (forward scratch)
-  float* ckpt;  // 2*nseg fields; slots 0,1 hold the zero initial state
-  float* ring;  // k+2 fields (replayed segment)
-  float* L;     // 2 fields   (adjoint state)
+  float* W;     // 2 fields: displacement b ping-pong
+  float* V;     // 1 field: increment v (updated in place by its owner)
+  float* ckpt;  // 2*nseg fields: (b, v) at t = j*k; slots 0,1 = the zero initial state
+  float* ring;  // k+1 fields: b at t = j*k .. j*k+k of the segment being replayed
+  float* L;     // 2 fields: adjoint lambda ping-pong
+  float* Mu;    // 1 field: adjoint increment (in place)
   double* grad; // 1 field of doubles (dJ/dc^2 accumulated over time)
   // operators and tables
   const float* D;     // (N+1)^2
@@ -142,21 +148,28 @@ __device__ __forceinline__ void decode(const SolveDev& s, int sig, int& act, int
   else { act = A_ADJ; t = (j + 1) * s.k - 1 - (w - s.k); }
 }
 
-// where the forward state b_t lives during the forward sweep (t in [-1, nt])
-__device__ __forceinline__ float* fwd_loc(const SolveDev& s, int t) {
+// where b_t / v_t live during the forward sweep (t in [0, nt])
+__device__ __forceinline__ const float* fwd_b(const SolveDev& s, int t) {
   if (!(s.flags & F_ADJ)) return s.W + (long long)(t & 1) * s.fstride;
   const int jl = s.nseg - 1;
-  if (t >= jl * s.k - 1) return s.ring + (long long)(t - jl * s.k + 1) * s.fstride;
-  if ((t + 1) % s.k == 0) return s.ckpt + (long long)(2 * ((t + 1) / s.k)) * s.fstride;
-  if (t % s.k == 0) return s.ckpt + (long long)(2 * (t / s.k) + 1) * s.fstride;
+  if (t >= jl * s.k) return s.ring + (long long)(t - jl * s.k) * s.fstride;
+  if (t % s.k == 0) return s.ckpt + (long long)(2 * (t / s.k)) * s.fstride;
   return s.W + (long long)(t & 1) * s.fstride;
 }
-
-// where b_t lives while segment j is replayed (t in [jk-1, jk+k])
-__device__ __forceinline__ float* replay_loc(const SolveDev& s, int j, int t) {
-  if (t == j * s.k - 1) return s.ckpt + (long long)(2 * j) * s.fstride;
+__device__ __forceinline__ const float* fwd_v(const SolveDev& s, int t) {
+  if (!(s.flags & F_ADJ)) return s.V;
+  const int jl = s.nseg - 1;
+  if (t < jl * s.k && t % s.k == 0) return s.ckpt + (long long)(2 * (t / s.k) + 1) * s.fstride;
+  return s.V;
+}
+// where b_t / v_t live while segment j is replayed (t in [jk, jk+k])
+__device__ __forceinline__ const float* rep_b(const SolveDev& s, int j, int t) {
+  if (t == j * s.k) return s.ckpt + (long long)(2 * j) * s.fstride;
+  return s.ring + (long long)(t - j * s.k) * s.fstride;
+}
+__device__ __forceinline__ const float* rep_v(const SolveDev& s, int j, int t) {
   if (t == j * s.k) return s.ckpt + (long long)(2 * j + 1) * s.fstride;
-  return s.ring + (long long)(t - j * s.k + 1) * s.fstride;
+  return s.V;
 }
 
 __host__ __device__ __forceinline__ int region_w(int tex, int N) { return ((tex + 2) * N + 1) | 1; }
@@ -169,7 +182,7 @@ __host__ __device__ inline long long smem_floats(int N, int tex, int tez, bool a
   const long long nro = (long long)(tez * N + 1) | 1, nco = (long long)(tex * N + 1) | 1;
   const long long xseg = (long long)(tex + 1) * NP * nro, zseg = (long long)(tez + 1) * NP * nco;
   long long f = 96 + 2 * reg + xseg + zseg;  // D, beta | u, c2 | K_x, K_z
-  if (adj) f += reg + xseg + zseg + nro * nco;  // forward field | S_x, S_z | injection
+  if (adj) f += reg + xseg + zseg + nro * nco + kMaxInj;  // forward field | S_x, S_z | injection
   return f;
 }
 
@@ -187,8 +200,14 @@ __global__ void __launch_bounds__(256) sem_tick_kernel(const SolveDev* __restric
   __shared__ int s_act, s_t, s_seg;
 
   const int sid = cta_solve[blockIdx.x];
+  {
+    static_assert(sizeof(SolveDev) % 8 == 0, "descriptor is copied as 8-byte words");
+    const unsigned long long* src = reinterpret_cast<const unsigned long long*>(solves + sid);
+    unsigned long long* dst = reinterpret_cast<unsigned long long*>(&S);
+    for (int i = threadIdx.x; i < (int)(sizeof(SolveDev) / 8); i += blockDim.x) dst[i] = src[i];
+  }
+  __syncthreads();
   if (threadIdx.x == 0) {
-    S = solves[sid];
     int act, t, seg;
     decode(S, *tick_ptr - S.start_tick, act, t, seg);
     s_act = act; s_t = t; s_seg = seg;
@@ -239,23 +258,26 @@ __global__ void __launch_bounds__(256) sem_tick_kernel(const SolveDev* __restric
   const int nthr = blockDim.x;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = nthr >> 5;
 
-  // ---------------- which fields
+  // ---------------- which fields (b: read with halo; v: read/written by the owner only)
   const float* cur;
-  const float* prev = nullptr;
+  const float* vin = nullptr;
   float* out = nullptr;
+  float* vout = nullptr;
   const float* fwdu = nullptr;
   if (act == A_FWD) {
-    cur = fwd_loc(S, t); prev = fwd_loc(S, t - 1); out = fwd_loc(S, t + 1);
+    cur = fwd_b(S, t); vin = fwd_v(S, t);
+    out = (float*)fwd_b(S, t + 1); vout = (float*)fwd_v(S, t + 1);
   } else if (act == A_FINAL) {
-    cur = fwd_loc(S, t);
+    cur = fwd_b(S, t);
   } else if (act == A_REPLAY) {
-    cur = replay_loc(S, seg, t); prev = replay_loc(S, seg, t - 1);
-    out = replay_loc(S, seg, t + 1);
-  } else {  // adjoint iteration it = t uses lambda_{t+1} (current) and lambda_{t+2}
+    cur = rep_b(S, seg, t); vin = rep_v(S, seg, t);
+    out = (float*)rep_b(S, seg, t + 1); vout = (float*)rep_v(S, seg, t + 1);
+  } else {  // adjoint iteration it = t: lambda_{t+1} -> lambda_t, forward b_{t+1}
     cur = S.L + (long long)((t + 1) & 1) * S.fstride;
-    prev = S.L + (long long)(t & 1) * S.fstride;
     out = S.L + (long long)(t & 1) * S.fstride;
-    fwdu = S.ring + (long long)(t + 1 - seg * S.k + 1) * S.fstride;
+    vin = S.Mu;
+    vout = S.Mu;
+    fwdu = S.ring + (long long)(t + 1 - seg * S.k) * S.fstride;
   }
 
   // ---------------- stage operators and the haloed tile
@@ -308,22 +330,29 @@ __global__ void __launch_bounds__(256) sem_tick_kernel(const SolveDev* __restric
     if (act == A_FINAL) return;
   }
 
-  // ---------------- adjoint source R^T r_it (deterministic order, warp 0)
+  // ---------------- adjoint source R^T r_it: residuals of this tile's receivers are
+  // formed in parallel, then one warp adds them node by node in receiver order
+  // (deterministic; receivers of one element never race)
   const bool in_win = adj && t >= S.it0 && t < S.it1 && ((t - S.it0) % S.decim) == 0;
   bool have_inj = false;
   if (adj) {
     const int off = S.inj_tile_off[lt], cnt = S.inj_tile_off[lt + 1] - off;
     have_inj = in_win && cnt > 0;
     if (have_inj) {
+      float* sres = sacc + nrop_max * ncop_max;  // cnt <= kMaxInj floats
       const double ascale = *S.adj_scale;
+      const long long yrow = (long long)((t - S.it0) / S.decim) * S.nrec;
       for (int i = threadIdx.x; i < nro * nco; i += nthr) sacc[i] = 0.f;
+      for (int q = threadIdx.x; q < cnt; q += nthr) {
+        const int r = S.inj_tile_ids[off + q];
+        const double res = (double)S.rec_out[(long long)t * S.nrec + r] - S.yobs[yrow + r];
+        sres[q] = (float)(res * ascale);
+      }
       __syncthreads();
       if (warp == 0) {
         for (int q = 0; q < cnt; ++q) {
           const int r = S.inj_tile_ids[off + q];
-          const double res = (double)S.rec_out[(long long)t * S.nrec + r] -
-                             S.yobs[(long long)((t - S.it0) / S.decim) * S.nrec + r];
-          const float rs = (float)(res * ascale);
+          const float rs = sres[q];
           const int bx = S.rec_base[2 * r], bz = S.rec_base[2 * r + 1];
           const float* wr = S.rec_w + (long long)r * NP * NP;
           for (int e = lane; e < NP * NP; e += 32) {
@@ -460,23 +489,26 @@ __global__ void __launch_bounds__(256) sem_tick_kernel(const SolveDev* __restric
     const float Kv = Rzv * X + Rxv * Z;
     const long long g = (long long)gz * S.pitch + gx;
     const float b = su[(gz - gzs) * SW + (gx - gxs)];
-    const float a = prev[g];
-    float res;
+    const float v = vin[g];
+    float wv;
     if (!adj) {
-      const float d = __ldg(S.tx + 2 * S.nxg + gx) * __ldg(S.tz + 2 * S.nzg + gz);
-      float n = 2.f * b - d * a - P * Kv;
-      if (gx == S.src_gx && gz == S.src_gz) n += S.src_term[t];
-      res = d * n;
+      wv = v - P * Kv;
+      if (gx == S.src_gx && gz == S.src_gz) wv += S.src_term[t];
     } else {
       const float inj = have_inj ? sacc[r * nco + cc] : 0.f;
-      if (damp) {
-        const float d = __ldg(S.tx + 2 * S.nxg + gx) * __ldg(S.tz + 2 * S.nzg + gz);
-        res = d * (2.f * b - d * a + P * (inj - Kv));
-      } else {
-        res = 2.f * b - a + P * (inj - Kv);
-      }
+      wv = v + P * (inj - Kv);
       if (grad_on) S.grad[g] += (double)(Rzv * SX + Rxv * SZ);
     }
+    float res, vres;
+    if (damp) {
+      const float d = __ldg(S.tx + 2 * S.nxg + gx) * __ldg(S.tz + 2 * S.nzg + gz);
+      vres = d * wv;
+      res = d * (b + wv);
+    } else {
+      vres = wv;
+      res = b + wv;
+    }
+    vout[g] = vres;
     out[g] = res;
     bad |= !isfinite(res);
   }
@@ -593,6 +625,8 @@ int get_lists(const sem_plan_s* p, int tex, int tez, sem_plan_s::Lists* out) {
     for (int i = 0; i < ntiles; ++i) off[i + 1] = off[i] + (int)v[i].size();
     for (auto& x : v) ids.insert(ids.end(), x.begin(), x.end());
   };
+  for (auto& v : inj)
+    if ((int)v.size() > kMaxInj) return fail(SEM_ERR_ARG, "too many receivers in one tile; use smaller tiles");
   std::vector<int> ro, ri, io, ii;
   flat(rec, ro, ri);
   flat(inj, io, ii);
@@ -622,7 +656,7 @@ KernelFn kernel_for(int N) {
 }
 
 struct Workspace {
-  long long c2, W, ckpt, ring, L, grad, misfit, status;  // byte offsets
+  long long c2, W, V, ckpt, ring, L, Mu, grad, misfit, status;  // byte offsets
   long long bytes;
 };
 
@@ -634,10 +668,12 @@ Workspace layout(const sem_plan_s* p, int flags, int k, int* nseg_out) {
   long long o = 0;
   w.c2 = o; o += F;
   w.W = o; o += 2 * F;
+  w.V = o; o += F;
   if (adj) {
     w.ckpt = o; o += (long long)2 * nseg * F;
-    w.ring = o; o += (long long)(k + 2) * F;
+    w.ring = o; o += (long long)(k + 1) * F;
     w.L = o; o += 2 * F;
+    w.Mu = o; o += F;
     w.grad = o; o += 2 * F;
   }
   w.misfit = o; o += round_up((long long)(2 * p->nrec + 1) * 8, 256);  // misfit, rmax, scale
@@ -825,9 +861,11 @@ int sem_run(sem_batch_t* b, const sem_solve_t* solves, int32_t n, const sem_laun
     d.fstride = p->fstride;
     d.c2 = (const float*)(a + ws[i].c2);
     d.W = (float*)(a + ws[i].W);
+    d.V = (float*)(a + ws[i].V);
     d.ckpt = (s.flags & SEM_F_ADJOINT) ? (float*)(a + ws[i].ckpt) : nullptr;
     d.ring = (s.flags & SEM_F_ADJOINT) ? (float*)(a + ws[i].ring) : nullptr;
     d.L = (s.flags & SEM_F_ADJOINT) ? (float*)(a + ws[i].L) : nullptr;
+    d.Mu = (s.flags & SEM_F_ADJOINT) ? (float*)(a + ws[i].Mu) : nullptr;
     d.grad = (s.flags & SEM_F_ADJOINT) ? (double*)(a + ws[i].grad) : nullptr;
     d.D = p->D; d.beta = p->beta; d.tx = p->tx; d.tz = p->tz; d.src_term = p->src_term;
     d.rec_base = p->rec_base; d.rec_w = p->rec_w;
@@ -872,13 +910,14 @@ int sem_run(sem_batch_t* b, const sem_solve_t* solves, int32_t n, const sem_laun
     const sem_plan_s* p = s.plan;
     char* a = b->arena + base[i];
     const long long F = p->fstride * 4;
+    // zero initial state: b_0 (ckpt 0 or ring 0 or W 0), v_0 (ckpt 1 or V), adjoint state
+    CUDA_TRY(cudaMemsetAsync(a + ws[i].W, 0, F, stream));
+    CUDA_TRY(cudaMemsetAsync(a + ws[i].V, 0, F, stream));
     if (s.flags & SEM_F_ADJOINT) {
       CUDA_TRY(cudaMemsetAsync(a + ws[i].ckpt, 0, 2 * F, stream));
-      if (nseg[i] == 1) CUDA_TRY(cudaMemsetAsync(a + ws[i].ring, 0, 2 * F, stream));
-      CUDA_TRY(cudaMemsetAsync(a + ws[i].L, 0, 2 * F, stream));
+      CUDA_TRY(cudaMemsetAsync(a + ws[i].ring, 0, F, stream));
+      CUDA_TRY(cudaMemsetAsync(a + ws[i].L, 0, 3 * F, stream));   // L[0], L[1], Mu
       CUDA_TRY(cudaMemsetAsync(a + ws[i].grad, 0, 2 * F, stream));
-    } else {
-      CUDA_TRY(cudaMemsetAsync(a + ws[i].W, 0, 2 * F, stream));
     }
     CUDA_TRY(cudaMemsetAsync(a + ws[i].misfit, 0, ws[i].status - ws[i].misfit + 256, stream));
     set_c2_kernel<<<std::min(1024, (p->npoints + 255) / 256), 256, 0, stream>>>(

@@ -1,0 +1,9 @@
+"""Drop-in replacement for MUN's ``sem_waveform`` package, running on a B200.
+
+    from mun_b200.sem_waveform import SEMSimulation          # instead of
+    from sem_waveform import SEMSimulation                   # MUN's CPU package
+"""
+from .core import SEMSimulation
+
+__version__ = "1.0.0"
+__all__ = ["SEMSimulation"]

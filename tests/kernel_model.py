@@ -75,12 +75,12 @@ def sens_apply(a, ug, wg):
 
 
 def forward(a, c, shift=False):
-    """Two-field forward recurrence exactly as the kernel runs it (float64)."""
+    """(b, v) forward recurrence exactly as the kernel runs it (float64)."""
     ix, Rx, dx, iz, Rz, dz = tables(a)
     d = dz[:, None] * dx[None, :]
     P = mass_inv_dt2(a)
     nxg, nzg = grids(a)
-    prev = np.zeros((nzg, nxg))
+    v = np.zeros((nzg, nxg))
     cur = np.zeros((nzg, nxg))
     N = a["npol"]
     nrec = a["nrec"]
@@ -98,9 +98,9 @@ def forward(a, c, shift=False):
     for t in range(a["nt"]):
         if not shift:
             rec[t] = read(cur)
-        n = 2 * cur - d * prev - P * K_apply(a, c, cur)
-        n[a["src_gz"], a["src_gx"]] += a["src_term"][t]
-        prev, cur = cur, d * n
+        w = v - P * K_apply(a, c, cur)
+        w[a["src_gz"], a["src_gx"]] += a["src_term"][t]
+        v, cur = d * w, d * (cur + w)
         hist.append(cur)
         if shift:
             rec[t] = read(cur)

@@ -1,0 +1,66 @@
+"""The drop-in SEMSimulation on the GPU against the reference's own outputs (same
+config dicts, same call sequence as tests/golden/make_golden.py)."""
+import numpy as np
+import pytest
+
+from mun_b200.sem_waveform import SEMSimulation
+from tests.goldens import load, rel_l2
+
+pytestmark = pytest.mark.gpu
+TOL = 1e-4
+
+
+def test_layered_cfg0_call_sequence():
+    g = load("layered_cfg0")
+    sim = SEMSimulation(g["config"])
+    run = sim.run(ctrl_offsets_flat=np.zeros(12))
+    e_run = rel_l2(run["receiver_data"], g["rec_run"])
+    nt = int(g["nt"])
+    obs = sim.run_forward_and_adjoint({"bspline_ctrl": np.asarray(g["ctrl_true"]).reshape(-1),
+                                       "y_obs": np.zeros((nt, 50)), "obs_dt": sim.dt, "obs_nt": nt,
+                                       "noise_std": 1e-9, "verbose": False})
+    e_obs = rel_l2(obs["clean_data"], g["y_obs"])
+    res = sim.run_forward_and_adjoint({"bspline_ctrl": np.asarray(g["ctrl"]).reshape(-1),
+                                       "y_obs": g["y_obs"], "obs_dt": sim.dt, "obs_nt": nt,
+                                       "noise_std": 1e-9, "verbose": False})
+    e_clean = rel_l2(res["clean_data"], g["clean"])
+    e_ll = abs(res["loglik"] - float(g["loglik"])) / abs(float(g["loglik"]))
+    e_g = rel_l2(res["grad_wrt_ctrl"], g["grad_ctrl"])
+    e_dv = rel_l2(-sim.dJ_dv, g["dL_dv"])
+    print(f"layered cfg0: run {e_run:.2e} obs {e_obs:.2e} clean {e_clean:.2e} loglik {e_ll:.2e} "
+          f"dL/dv {e_dv:.2e} grad_ctrl {e_g:.2e}")
+    assert max(e_run, e_obs, e_clean, e_ll, e_dv, e_g) <= TOL
+    assert res["dt"] == float(g["dt"]) and res["nt"] == nt
+
+
+def test_canonical_circle_call_sequence():
+    g = load("circle_n5")
+    sim = SEMSimulation(g["config"])
+    run = sim.run()
+    e_run = rel_l2(run["receiver_data"], g["rec_run"])
+    ctrl0 = np.asarray(g["ctrl"])
+    y = sim.run_forward_and_adjoint({"bspline_ctrl": (ctrl0 + 25.0).reshape(-1),
+                                     "y_obs": np.zeros((sim.nt, 24)), "obs_dt": sim.dt,
+                                     "obs_nt": sim.nt, "noise_std": 0.0})["clean_data"]
+    res = sim.run_forward_and_adjoint({"bspline_ctrl": ctrl0.reshape(-1), "y_obs": g["y_obs"],
+                                       "obs_dt": sim.dt, "obs_nt": sim.nt, "noise_std": 1e-8})
+    e_y = rel_l2(y, g["y_obs"])
+    e_ll = abs(res["loglik"] - float(g["loglik"])) / abs(float(g["loglik"]))
+    e_g = rel_l2(res["grad_wrt_ctrl"], g["grad_ctrl"])
+    print(f"circle n5: run {e_run:.2e} y {e_y:.2e} loglik {e_ll:.2e} grad_ctrl {e_g:.2e}")
+    assert max(e_run, e_y, e_ll, e_g) <= TOL
+
+
+def test_batch_method_equals_single_calls():
+    g = load("layered_cfg0")
+    sim = SEMSimulation(g["config"])
+    nt = int(g["nt"])
+    rng = np.random.default_rng(0)
+    params = [{"bspline_ctrl": (np.asarray(g["ctrl"]) + rng.normal(0, 10, (6, 2))).reshape(-1),
+               "y_obs": g["y_obs"], "obs_dt": float(g["dt"]), "obs_nt": nt, "noise_std": 1e-9}
+              for _ in range(4)]
+    batched = sim.run_forward_and_adjoint_batch(params, ckpt_k=64)
+    for p, b in zip(params, batched):
+        s = sim.run_forward_and_adjoint(p)
+        assert s["loglik"] == b["loglik"]
+        np.testing.assert_array_equal(s["grad_wrt_ctrl"], b["grad_wrt_ctrl"])

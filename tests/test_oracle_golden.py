@@ -68,3 +68,15 @@ def test_circle_n5_solver_matches_reference():
     out = so.forward_adjoint(sim2, g["y_obs"], float(g["sigma"]))
     assert rel_l2(out["clean"], g["clean"]) < 1e-10
     assert rel_l2(out["dL_dv"], g["dL_dv"]) < 1e-9
+
+
+def test_layered_cfg0_oracle_matches_reference():
+    g = load("layered_cfg0")
+    sim = so.build_sim(g["config"], g["velocity"], dt=float(g["dt"]))
+    assert sim.nt == int(g["nt"]) and sim.src_node == int(g["src_node"])
+    rec, _ = so.forward(sim, convention="run")
+    assert rel_l2(rec, g["rec_run"]) < 1e-10
+    out = so.forward_adjoint(sim, g["y_obs"], float(g["sigma"]))
+    assert rel_l2(out["clean"], g["clean"]) < 1e-10
+    assert abs(out["loglik"] - float(g["loglik"])) <= 1e-9 * abs(float(g["loglik"]))
+    assert rel_l2(out["dL_dv"], g["dL_dv"]) < 1e-8

@@ -25,7 +25,7 @@ def smem_floats(N, tex, tez, adj):
     xseg, zseg = (tex + 1) * NP * nro, (tez + 1) * NP * nco
     f = 96 + 2 * reg + xseg + zseg
     if adj:
-        f += reg + xseg + zseg + nro * nco
+        f += reg + xseg + zseg + nro * nco + 1024
     return f
 
 

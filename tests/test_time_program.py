@@ -41,74 +41,89 @@ def decode(nt, k, nseg, adj, shift, sig):
     return A_ADJ, (j + 1) * k - 1 - (w - k), j
 
 
-def fwd_loc(nt, k, nseg, adj, t):
+def fwd_b(nt, k, nseg, adj, t):
     if not adj:
         return ("W", t & 1)
     jl = nseg - 1
-    if t >= jl * k - 1:
-        return ("ring", t - jl * k + 1)
-    if (t + 1) % k == 0:
-        return ("ckpt", 2 * ((t + 1) // k))
+    if t >= jl * k:
+        return ("ring", t - jl * k)
     if t % k == 0:
-        return ("ckpt", 2 * (t // k) + 1)
+        return ("ckpt", 2 * (t // k))
     return ("W", t & 1)
 
 
-def replay_loc(k, j, t):
-    if t == j * k - 1:
-        return ("ckpt", 2 * j)
-    if t == j * k:
-        return ("ckpt", 2 * j + 1)
-    return ("ring", t - j * k + 1)
+def fwd_v(nt, k, nseg, adj, t):
+    if not adj:
+        return ("V", 0)
+    jl = nseg - 1
+    if t < jl * k and t % k == 0:
+        return ("ckpt", 2 * (t // k) + 1)
+    return ("V", 0)
+
+
+def rep_b(k, j, t):
+    return ("ckpt", 2 * j) if t == j * k else ("ring", t - j * k)
+
+
+def rep_v(k, j, t):
+    return ("ckpt", 2 * j + 1) if t == j * k else ("V", 0)
 
 
 def simulate(nt, k, adj, shift):
+    """Symbolic run: mem maps a slot to ('b', t) or ('v', t)."""
     nseg = -(-nt // k) if adj else 1
     mem = {}
     if adj:
         if nseg == 1:
-            mem[("ring", 0)], mem[("ring", 1)] = -1, 0
+            mem[("ring", 0)] = ("b", 0)
+            mem[("V", 0)] = ("v", 0)
         else:
-            mem[("ckpt", 0)], mem[("ckpt", 1)] = -1, 0
+            mem[("ckpt", 0)], mem[("ckpt", 1)] = ("b", 0), ("v", 0)
     else:
-        mem[("W", 1)], mem[("W", 0)] = -1, 0
-    lam = {0: nt + 1 if (nt + 1) % 2 == 0 else nt, 1: nt if nt % 2 == 1 else nt + 1}
-    lam = {(nt) & 1: nt, (nt + 1) & 1: nt + 1}  # lambda_nt, lambda_nt+1 = 0
+        mem[("W", 0)], mem[("V", 0)] = ("b", 0), ("v", 0)
+    lam = {nt & 1: nt}
+    mu = nt
     prog = nt + (1 if shift else 0) + (1 + nt + k * (nseg - 1) if adj else 0)
     adj_seen = []
+
+    def check(loc):
+        kind, slot = loc
+        if kind == "ring":
+            assert 0 <= slot <= k
+        if kind == "ckpt":
+            assert 0 <= slot < 2 * nseg
+        if kind == "W":
+            assert slot in (0, 1)
+        return loc
+
     for sig in range(prog + 3):
         act, t, seg = decode(nt, k, nseg, adj, shift, sig)
         if sig >= prog:
             assert act == A_NONE
             continue
-
-        def check(loc):
-            kind, slot = loc
-            if kind == "ring":
-                assert 0 <= slot <= k + 1
-            if kind == "ckpt":
-                assert 0 <= slot < 2 * nseg
-            if kind == "W":
-                assert slot in (0, 1)
-            return loc
         if act == A_FWD:
-            assert mem[check(fwd_loc(nt, k, nseg, adj, t - 1))] == t - 1
-            assert mem[check(fwd_loc(nt, k, nseg, adj, t))] == t
-            mem[check(fwd_loc(nt, k, nseg, adj, t + 1))] = t + 1
+            rb, rv = check(fwd_b(nt, k, nseg, adj, t)), check(fwd_v(nt, k, nseg, adj, t))
+            wb, wv = check(fwd_b(nt, k, nseg, adj, t + 1)), check(fwd_v(nt, k, nseg, adj, t + 1))
+            assert mem[rb] == ("b", t) and mem[rv] == ("v", t)
+            assert wb != rb  # b is read with a halo by other tiles: never in place
+            mem[wb], mem[wv] = ("b", t + 1), ("v", t + 1)
         elif act == A_FINAL:
-            assert mem[fwd_loc(nt, k, nseg, adj, nt)] == nt
-        elif act == A_REPLAY:
-            assert mem[check(replay_loc(k, seg, t - 1))] == t - 1
-            assert mem[check(replay_loc(k, seg, t))] == t
-            mem[check(replay_loc(k, seg, t + 1))] = t + 1
+            assert mem[fwd_b(nt, k, nseg, adj, nt)] == ("b", nt)
         elif act == A_SCALE:
-            assert not adj_seen and all(v <= nt for v in mem.values())
+            assert not adj_seen
+        elif act == A_REPLAY:
+            rb, rv = check(rep_b(k, seg, t)), check(rep_v(k, seg, t))
+            wb, wv = check(rep_b(k, seg, t + 1)), check(rep_v(k, seg, t + 1))
+            assert mem[rb] == ("b", t) and mem[rv] == ("v", t)
+            assert wb != rb
+            mem[wb], mem[wv] = ("b", t + 1), ("v", t + 1)
         elif act == A_ADJ:
-            slot = t + 1 - seg * k + 1
-            assert 0 <= slot <= k + 1
-            assert mem[("ring", slot)] == t + 1
-            assert lam[(t + 1) & 1] == t + 1 and lam[t & 1] == t + 2
+            slot = t + 1 - seg * k
+            assert 1 <= slot <= k
+            assert mem[("ring", slot)] == ("b", t + 1)
+            assert lam[(t + 1) & 1] == t + 1 and mu == t + 1
             lam[t & 1] = t
+            mu = t
             adj_seen.append(t)
         else:
             raise AssertionError(f"tick {sig} of {prog} decoded to nothing")
