@@ -174,6 +174,7 @@ def main():
     ap.add_argument("--plain", type=int, default=6, help="one-at-a-time solves timed")
     ap.add_argument("--tile", default="8x8")
     ap.add_argument("--graph-chunk", type=int, default=0)
+    ap.add_argument("--kernel", type=int, default=0, help="0 auto, 1 tile, 2 strip")
     ap.add_argument("--ckpt-k", type=int, default=0)
     ap.add_argument("--ref-nt", type=int, default=200)
     ap.add_argument("--cpu-nt", type=int, default=200)
@@ -198,7 +199,7 @@ def main():
     plan = SEMPlan(**W["plan_kw"])
     dev = torch.device("cuda", local)
     tex, tez = (int(x) for x in args.tile.split("x"))
-    batch = Batch(tile=(tex, tez), graph_chunk=args.graph_chunk)
+    batch = Batch(tile=(tex, tez), graph_chunk=args.graph_chunk, kernel=args.kernel)
     stream = torch.cuda.Stream()
 
     # observed data from the "true" model, once
@@ -225,8 +226,8 @@ def main():
         for _ in range(args.warmup):
             batch.run(specs)
     stream.synchronize()
-    k_used = None
     launches_per_step = batch.last_launches
+    kernel_used = batch.last_kernel
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     step_ms = []
     clocks = Clocks(os.path.join(HERE, "gpurun_out", f"clocks_r{rank}.csv") if os.path.isdir(
@@ -276,18 +277,20 @@ def main():
     h2d = pin_v.numel() * 8 + pin_y.numel() * 8
     d2h = out_g.numel() * 8 + out_l.numel() * 8
 
-    # ---------------- plain: one solve at a time (same models)
+    # ---------------- plain: one solve at a time (same models, best single-solve kernel)
     plain_ms = []
+    pbatch = Batch(tile=(tex, tez), graph_chunk=args.graph_chunk, kernel=0)
     with torch.cuda.stream(stream):
         for i in range(args.warmup + args.plain):
             s = SolveSpec(plan, vel_dev[i % n], adjoint=True, y_obs=y, inv_sigma2=inv_s2,
                           ckpt_k=args.ckpt_k)
             ev0.record(stream)
-            batch.run([s])
+            pbatch.run([s])
             ev1.record(stream)
             ev1.synchronize()
             if i >= args.warmup:
                 plain_ms.append(ev0.elapsed_time(ev1))
+    plain_kernel = pbatch.last_kernel
     plain_ms = np.array(plain_ms)
     plain_value = 1e3 / plain_ms.mean()
 
@@ -313,10 +316,11 @@ def main():
             "config": {"workload": "batched ELBO sampling (256 models, 100x50 el, N=4, 80601 nodes, "
                                    "3000 steps, 100 receivers)",
                        "models_per_gpu": n, "nodes": W["npoints"], "nt": W["nt"],
-                       "tile": args.tile, "graph_chunk": args.graph_chunk,
+                       "kernel": kernel_used, "tile": args.tile, "graph_chunk": args.graph_chunk,
                        "l2": "inputs larger than L2 (state+c2 of 256 models ~250 MB per field set)",
                        "parallelism": f"replicas x{world}"},
-            "plain": {"value": plain_value, "unit": "solves/s", "p50_ms": float(np.percentile(plain_ms, 50)),
+            "plain": {"value": plain_value, "unit": "solves/s", "kernel": plain_kernel,
+                      "p50_ms": float(np.percentile(plain_ms, 50)),
                       "p99_ms": float(np.percentile(plain_ms, 99)), "solves": int(len(plain_ms))},
             "batched_over_plain": value / world / plain_value,
             "latency_ms": {"p50": float(np.percentile(step_ms, 50)), "p99": float(np.percentile(step_ms, 99))},

@@ -91,9 +91,13 @@ typedef struct {
 
 /* Launch configuration (the autotuner's knobs). */
 typedef struct {
-  int32_t tile_ex, tile_ez;   /* elements per CTA tile in x and z                     */
-  int32_t threads;            /* threads per CTA (multiple of 32, <= 1024)            */
+  int32_t tile_ex, tile_ez;   /* tile kernel: elements per CTA tile in x and z        */
+  int32_t threads;            /* tile kernel: threads per CTA (multiple of 32, <= 256) */
   int32_t graph_chunk;        /* ticks per captured CUDA graph; 0 = plain launches    */
+  int32_t kernel;             /* 0 auto, 1 tile kernel (one CTA per element tile),
+                                 2 strip kernel (one CTA per full-height strip, TMA-
+                                 staged element-row bands); auto picks strips when the
+                                 batch has at least one strip per SM                   */
 } sem_launch_cfg_t;
 
 int sem_plan_create(const sem_plan_desc_t* desc, sem_plan_t** out);
@@ -109,6 +113,8 @@ int sem_run(sem_batch_t* batch, const sem_solve_t* solves, int32_t n,
             const sem_launch_cfg_t* cfg, void* stream);
 /* number of kernel launches issued by the last sem_run (for accounting) */
 int64_t sem_batch_last_launches(const sem_batch_t* batch);
+/* kernel variant used by the last sem_run: 1 tile, 2 strip */
+int32_t sem_batch_last_kernel(const sem_batch_t* batch);
 
 /* Single-solve conveniences (plain path): forward with receivers in the run()
  * convention, and forward+adjoint in the run_forward_and_adjoint convention. */

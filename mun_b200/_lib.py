@@ -35,11 +35,12 @@ class Solve(C.Structure):
 
 class LaunchCfg(C.Structure):
     _fields_ = [("tile_ex", C.c_int32), ("tile_ez", C.c_int32), ("threads", C.c_int32),
-                ("graph_chunk", C.c_int32)]
+                ("graph_chunk", C.c_int32), ("kernel", C.c_int32)]
 
 
 EXPORTS = ["sem_plan_create", "sem_plan_destroy", "sem_plan_workspace_bytes", "sem_batch_create",
-           "sem_batch_destroy", "sem_run", "sem_batch_last_launches", "sem_forward",
+           "sem_batch_destroy", "sem_run", "sem_batch_last_launches", "sem_batch_last_kernel",
+           "sem_forward",
            "sem_forward_adjoint", "sem_last_error"]
 
 _lib = None
@@ -71,11 +72,14 @@ def load(path=None):
     lib.sem_run.argtypes = [vp, C.POINTER(Solve), i32, C.POINTER(LaunchCfg), vp]
     lib.sem_batch_last_launches.argtypes = [vp]
     lib.sem_batch_last_launches.restype = i64
+    lib.sem_batch_last_kernel.argtypes = [vp]
+    lib.sem_batch_last_kernel.restype = i32
     lib.sem_forward.argtypes = [vp, vp, vp, vp, vp]
     lib.sem_forward_adjoint.argtypes = [vp, vp, vp, vp, dbl, i32, i32, vp, vp, vp, vp]
     lib.sem_last_error.restype = C.c_char_p
     for name in EXPORTS:
-        if name not in ("sem_plan_workspace_bytes", "sem_batch_last_launches", "sem_last_error"):
+        if name not in ("sem_plan_workspace_bytes", "sem_batch_last_launches", "sem_batch_last_kernel",
+                        "sem_last_error"):
             getattr(lib, name).restype = C.c_int
     _lib = lib
     return lib

@@ -186,8 +186,36 @@ __host__ __device__ inline long long smem_floats(int N, int tex, int tez, bool a
   return f;
 }
 
+
+// One owned node: combine the line operators, advance (b, v) or (lambda, mu), apply
+// the sponge.  Shared by both kernel variants so their arithmetic is identical.
+//   forward:  w = v - P K + src          adjoint: w = mu + P (inj - K)
+//   v' = d w, b' = d (b + w)   (d = 1 in the reference-mode adjoint)
+__device__ __forceinline__ void advance_node(bool adj, bool damp, float b, float v, float X,
+                                             float Z, float ixv, float Rxv, float dxv, float izv,
+                                             float Rzv, float dzv, float extra, float& bout,
+                                             float& vout) {
+  const float P = ixv * izv;
+  const float Kv = Rzv * X + Rxv * Z;
+  float wv;
+  if (!adj) {
+    wv = v - P * Kv;
+    wv += extra;
+  } else {
+    wv = v + P * (extra - Kv);
+  }
+  if (damp) {
+    const float d = dxv * dzv;
+    vout = d * wv;
+    bout = d * (b + wv);
+  } else {
+    vout = wv;
+    bout = b + wv;
+  }
+}
+
 // ----------------------------------------------------------------------------
-// the tick kernel
+// tile kernel: one CTA per tile of elements (used for small batches)
 // ----------------------------------------------------------------------------
 template <int N>
 __global__ void __launch_bounds__(256) sem_tick_kernel(const SolveDev* __restrict__ solves,
@@ -485,32 +513,448 @@ __global__ void __launch_bounds__(256) sem_tick_kernel(const SolveDev* __restric
     }
     const float ixv = __ldg(S.tx + gx), Rxv = __ldg(S.tx + S.nxg + gx);
     const float izv = __ldg(S.tz + gz), Rzv = __ldg(S.tz + S.nzg + gz);
-    const float P = ixv * izv;
-    const float Kv = Rzv * X + Rxv * Z;
+    const float dxv = __ldg(S.tx + 2 * S.nxg + gx), dzv = __ldg(S.tz + 2 * S.nzg + gz);
     const long long g = (long long)gz * S.pitch + gx;
     const float b = su[(gz - gzs) * SW + (gx - gxs)];
     const float v = vin[g];
-    float wv;
+    float extra = 0.f;
     if (!adj) {
-      wv = v - P * Kv;
-      if (gx == S.src_gx && gz == S.src_gz) wv += S.src_term[t];
+      if (gx == S.src_gx && gz == S.src_gz) extra = S.src_term[t];
     } else {
-      const float inj = have_inj ? sacc[r * nco + cc] : 0.f;
-      wv = v + P * (inj - Kv);
+      extra = have_inj ? sacc[r * nco + cc] : 0.f;
       if (grad_on) S.grad[g] += (double)(Rzv * SX + Rxv * SZ);
     }
     float res, vres;
-    if (damp) {
-      const float d = __ldg(S.tx + 2 * S.nxg + gx) * __ldg(S.tz + 2 * S.nzg + gz);
-      vres = d * wv;
-      res = d * (b + wv);
-    } else {
-      vres = wv;
-      res = b + wv;
-    }
+    advance_node(adj, damp, b, v, X, Z, ixv, Rxv, dxv, izv, Rzv, dzv, extra, res, vres);
     vout[g] = vres;
     out[g] = res;
     bad |= !isfinite(res);
+  }
+  if (__any_sync(0xffffffffu, bad) && lane == 0) atomicOr(S.status, SEM_ERR_NONFINITE);
+}
+
+// ----------------------------------------------------------------------------
+// strip kernel: one CTA per full-height strip of element columns (large batches)
+//
+// Threads map to grid columns: N left-halo columns, the strip's owned columns and the
+// shared column on its right.  The CTA sweeps the strip one element row at a time.
+// Each band of N+1 grid rows (every field the step reads) is staged by TMA bulk
+// copies into a ring of kStages shared-memory slots, issued kStages bands ahead and
+// completed on an mbarrier.  Per band: x-lines through a two-phase exchange of
+// per-node fluxes in shared memory, z-lines in registers (the band holds the whole
+// element column segment), then the node update for the band's N rows.
+// ----------------------------------------------------------------------------
+constexpr int kStripThreads = 128;
+constexpr int kStages = 3;
+constexpr long long kWaitNs = 2000000000LL;  // bounded mbarrier waits: 2 s
+
+__host__ __device__ inline int strip_ew_max(int N) { return (kStripThreads - N - 1) / N; }
+__host__ __device__ inline int strip_bw(int N) { return (kStripThreads + 3 + 3) & ~3; }  // smem row
+
+__device__ __forceinline__ uint32_t smem_addr(const void* p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void mbar_init(unsigned long long* bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(unsigned long long* bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)),
+               "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(unsigned long long* bar, unsigned parity) {
+  unsigned ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n}"
+      : "=r"(ok)
+      : "r"(smem_addr(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+__device__ __forceinline__ long long global_ns() {
+  long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+// wait for a TMA phase; gives up after kWaitNs and reports false
+__device__ __forceinline__ bool mbar_wait(unsigned long long* bar, unsigned parity) {
+  if (mbar_try_wait(bar, parity)) return true;
+  const long long t0 = global_ns();
+  while (!mbar_try_wait(bar, parity))
+    if (global_ns() - t0 > kWaitNs) return false;
+  return true;
+}
+__device__ __forceinline__ void bulk_load(void* dst, const void* src, unsigned bytes,
+                                          unsigned long long* bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+          smem_addr(dst)),
+      "l"(src), "r"(bytes), "r"(smem_addr(bar))
+      : "memory");
+}
+
+// shared-memory floats of one strip CTA (stages + exchange arrays + injection rows)
+__host__ __device__ inline long long strip_smem_floats(int N, bool adj) {
+  const int BW = strip_bw(N);
+  const int nfloat = adj ? 4 : 3;  // cur, c2, v (+ forward field)
+  const int ndouble = adj ? 1 : 0;  // gradient accumulator
+  const long long stage = ((long long)(nfloat + 2 * ndouble) * (N + 1) * BW + 31) & ~31LL;
+  const long long xch = (long long)(adj ? 4 : 2) * (N + 1) * kStripThreads;
+  const long long inj = adj ? (long long)(N + 1) * kStripThreads + kMaxInj : 0;
+  return 64 + 96 + kStages * stage + xch + inj;  // barriers, D/beta, ...
+}
+
+template <int N>
+__global__ void __launch_bounds__(kStripThreads) sem_strip_kernel(const SolveDev* __restrict__ solves,
+                                                                  const int* __restrict__ cta_solve,
+                                                                  const int* __restrict__ tick_ptr,
+                                                                  int ew_unused, int unused) {
+  constexpr int NP = N + 1;
+  constexpr int BW = (kStripThreads + 3 + 3) & ~3;
+  extern __shared__ __align__(128) float smem[];
+  __shared__ SolveDev S;
+  __shared__ int s_act, s_t, s_seg, s_abort;
+
+  const int sid = cta_solve[blockIdx.x];
+  {
+    const unsigned long long* src = reinterpret_cast<const unsigned long long*>(solves + sid);
+    unsigned long long* dst = reinterpret_cast<unsigned long long*>(&S);
+    for (int i = threadIdx.x; i < (int)(sizeof(SolveDev) / 8); i += blockDim.x) dst[i] = src[i];
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int act, t, seg;
+    decode(S, *tick_ptr - S.start_tick, act, t, seg);
+    s_act = act; s_t = t; s_seg = seg; s_abort = 0;
+  }
+  __syncthreads();
+  const int act = s_act;
+  if (act == A_NONE) return;
+  const int t = s_t, seg = s_seg;
+  if (act == A_SCALE) {
+    if (blockIdx.x == S.tile_base && threadIdx.x == 0) {
+      double m = 0.0;
+      for (int r = 0; r < S.nrec; ++r) m = fmax(m, S.rmax[r]);
+      *S.adj_scale = (m > 0.0 && isfinite(m)) ? ldexp(1.0, -ilogb(m)) : 1.0;
+    }
+    return;
+  }
+  const bool adj = (act == A_ADJ);
+  const bool final_only = (act == A_FINAL);
+
+  // ---------------- strip geometry (tiles_x = number of strips, tiles_z = elements/strip)
+  const int strip = blockIdx.x - S.tile_base;
+  const int EW = S.tiles_z;
+  const int e0 = strip * EW, e1 = min(e0 + EW, S.nelx);
+  const int sx0 = e0 * N;                                   // first owned column
+  const int so1 = (e1 == S.nelx) ? S.nxg : e1 * N;          // owned columns [sx0, so1)
+  const int NC = (e1 - e0) * N + N + 1;                     // thread columns
+  const int X0 = (sx0 - N) & ~3;                            // 16-byte aligned copy origin
+  const int off = (sx0 - N) - X0;                           // smem column of thread 0
+  const int cs = max(X0, 0), ce = min(X0 + BW, S.pitch);    // copied columns
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int gx = sx0 - N + tid;
+  const bool col_valid = tid < NC && gx >= 0 && gx < S.nxg;
+  const bool owned = col_valid && gx >= sx0 && gx < so1;
+  const int sc = tid + off;                                 // this thread's smem column
+
+  // ---------------- shared memory carve-up
+  unsigned long long* bars = reinterpret_cast<unsigned long long*>(smem);  // kStages barriers
+  float* sD = smem + 64;
+  float* sB = sD + 64;
+  const int nfloat = (adj ? 4 : 3), ndouble = (adj ? 1 : 0);
+  const long long stage_f = ((long long)(nfloat + 2 * ndouble) * NP * BW + 31) & ~31LL;
+  float* stages = smem + 64 + 96;
+  float* xch = stages + kStages * stage_f;
+  float* Qr = xch;                       // [NP][kStripThreads]
+  float* Ql = Qr + NP * kStripThreads;
+  float* Sr = Ql + NP * kStripThreads;   // adjoint only
+  float* Sl = Sr + NP * kStripThreads;
+  float* sacc = xch + (adj ? 4 : 2) * NP * kStripThreads;  // [NP][kStripThreads]
+  float* sres = sacc + NP * kStripThreads;
+
+  // ---------------- which fields
+  const float* cur;
+  const float* vin = nullptr;
+  float* out = nullptr;
+  float* vout = nullptr;
+  const float* fwdu = nullptr;
+  if (act == A_FWD) {
+    cur = fwd_b(S, t); vin = fwd_v(S, t);
+    out = (float*)fwd_b(S, t + 1); vout = (float*)fwd_v(S, t + 1);
+  } else if (act == A_FINAL) {
+    cur = fwd_b(S, t);
+  } else if (act == A_REPLAY) {
+    cur = rep_b(S, seg, t); vin = rep_v(S, seg, t);
+    out = (float*)rep_b(S, seg, t + 1); vout = (float*)rep_v(S, seg, t + 1);
+  } else {
+    cur = S.L + (long long)((t + 1) & 1) * S.fstride;
+    out = S.L + (long long)(t & 1) * S.fstride;
+    vin = S.Mu;
+    vout = S.Mu;
+    fwdu = S.ring + (long long)(t + 1 - seg * S.k) * S.fstride;
+  }
+  const float* fsrc[4] = {cur, S.c2, vin, fwdu};
+  const int nload = final_only ? 1 : nfloat;  // FINAL reads only b
+
+  if (tid == 0) {
+    for (int s = 0; s < kStages; ++s) mbar_init(bars + s, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  for (int i = tid; i < NP * NP; i += kStripThreads) sD[i] = S.D[i];
+  for (int i = tid; i < NP; i += kStripThreads) sB[i] = S.beta[i];
+  __syncthreads();
+
+  // issue the TMA copies of element row `ez` into ring slot ez % kStages
+  auto issue = [&](int ez) {
+    const int slot = ez % kStages;
+    float* st = stages + slot * stage_f;
+    const unsigned rowb = (unsigned)(ce - cs) * 4u;
+    unsigned total = (unsigned)nload * NP * rowb + (unsigned)(final_only ? 0 : ndouble) * NP * rowb * 2u;
+    mbar_expect_tx(bars + slot, total);
+    for (int f = 0; f < nload; ++f)
+      for (int a = 0; a < NP; ++a) {
+        const long long grow = (long long)(ez * N + a) * S.pitch;
+        bulk_load(st + (f * NP + a) * BW + (cs - X0), fsrc[f] + grow + cs, rowb, bars + slot);
+      }
+    if (ndouble && !final_only) {
+      double* gs = reinterpret_cast<double*>(st + nfloat * NP * BW);
+      for (int a = 0; a < NP; ++a) {
+        const long long grow = (long long)(ez * N + a) * S.pitch;
+        bulk_load(gs + a * BW + (cs - X0), S.grad + grow + cs, rowb * 2u, bars + slot);
+      }
+    }
+  };
+  if (tid == 0)
+    for (int ez = 0; ez < min(kStages, S.nelz); ++ez) issue(ez);
+
+  // per-column tables
+  float ixv = 0.f, Rxv = 0.f, dxv = 0.f;
+  if (owned) { ixv = S.tx[gx]; Rxv = S.tx[S.nxg + gx]; dxv = S.tx[2 * S.nxg + gx]; }
+  const int e_r = col_valid ? gx / N : 0, ia = col_valid ? gx - e_r * N : 0;
+  const bool damp = (act != A_ADJ) || (S.flags & F_EXACT);
+  const bool grad_on = adj && t >= S.it0 && t < S.it1;
+  const bool in_win = adj && t >= S.it0 && t < S.it1 && ((t - S.it0) % S.decim) == 0;
+  const int ms = t - ((S.flags & F_SHIFT) ? 1 : 0);
+  const bool rec_on = (act == A_FWD || act == A_FINAL) && ms >= 0 && ms < S.nt;
+  float zc = 0.f, szc = 0.f;  // z-line carries into the next band's first row
+  int abort_ez = -1;
+  if (adj) for (int a = 0; a < NP; ++a) sacc[a * kStripThreads + tid] = 0.f;
+  bool bad = false;
+
+  for (int ez = 0; ez < S.nelz; ++ez) {
+    const int slot = ez % kStages;
+    const float* st = stages + slot * stage_f;
+    const float* Bs = st;
+    const float* Cs = st + NP * BW;
+    const float* Vs = st + 2 * NP * BW;
+    const float* Us = st + 3 * NP * BW;
+    const double* Gs = reinterpret_cast<const double*>(st + nfloat * NP * BW);
+    if (!mbar_wait(bars + slot, (unsigned)((ez / kStages) & 1))) s_abort = 1;
+    __syncthreads();
+    if (s_abort) { abort_ez = ez; break; }
+    const int rows = (ez == S.nelz - 1) ? NP : N;  // the last band also owns the bottom row
+
+    // ---- receivers recorded from this band (one warp per receiver)
+    if (rec_on) {
+      const int li = strip * S.nelz + ez;
+      const int off0 = S.rec_tile_off[li], cnt = S.rec_tile_off[li + 1] - off0;
+      for (int q = warp; q < cnt; q += kStripThreads / 32) {
+        const int r = S.rec_tile_ids[off0 + q];
+        const int bx = S.rec_base[2 * r];
+        const float* wr = S.rec_w + (long long)r * NP * NP;
+        float acc = 0.f;
+        for (int e = lane; e < NP * NP; e += 32) {
+          const int j = e / NP, i = e - j * NP;
+          acc = fmaf(wr[e], Bs[j * BW + (bx + i - X0)], acc);
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+        if (lane == 0) {
+          S.rec_out[(long long)ms * S.nrec + r] = acc;
+          if ((S.flags & F_MISFIT) && ms >= S.it0 && ms < S.it1 && ((ms - S.it0) % S.decim) == 0) {
+            const double res = (double)acc - S.yobs[(long long)((ms - S.it0) / S.decim) * S.nrec + r];
+            S.misfit[r] += res * res;
+            S.rmax[r] = fmax(S.rmax[r], fabs(res));
+          }
+        }
+      }
+    }
+    if (!final_only) {
+      // ---- adjoint source of receivers in this element row
+      if (in_win) {
+        const int li = strip * S.nelz + ez;
+        const int off0 = S.inj_tile_off[li], cnt = S.inj_tile_off[li + 1] - off0;
+        if (cnt > 0) {
+          const double ascale = *S.adj_scale;
+          const long long yrow = (long long)((t - S.it0) / S.decim) * S.nrec;
+          for (int q = tid; q < cnt; q += kStripThreads) {
+            const int r = S.inj_tile_ids[off0 + q];
+            const double res = (double)S.rec_out[(long long)t * S.nrec + r] - S.yobs[yrow + r];
+            sres[q] = (float)(res * ascale);
+          }
+          __syncthreads();
+          if (warp == 0) {
+            for (int q = 0; q < cnt; ++q) {
+              const int r = S.inj_tile_ids[off0 + q];
+              const float rs = sres[q];
+              const int bx = S.rec_base[2 * r];
+              const float* wr = S.rec_w + (long long)r * NP * NP;
+              for (int e = lane; e < NP * NP; e += 32) {
+                const int j = e / NP, i = e - j * NP;
+                const int c = bx + i - (sx0 - N);
+                const int gxx = bx + i;
+                if (gxx >= sx0 && gxx < so1) sacc[j * kStripThreads + c] += wr[e] * rs;
+              }
+              __syncwarp();
+            }
+          }
+        }
+      }
+      // ---- phase A: per-node x-line fluxes q = beta c^2 (D u) (and D u_fwd for S)
+      if (col_valid) {
+        for (int a = 0; a < rows; ++a) {
+          const float* br = Bs + a * BW;
+          if (e_r < S.nelx && tid < NC - 1) {
+            const float* ub = br + sc - ia;
+            float v = 0.f;
+#pragma unroll
+            for (int b = 0; b < NP; ++b) v = fmaf(sD[ia * NP + b], ub[b], v);
+            Qr[a * kStripThreads + tid] = sB[ia] * Cs[a * BW + sc] * v;
+            if (adj) {
+              const float* wb = Us + a * BW + sc - ia;
+              float dw = 0.f;
+#pragma unroll
+              for (int b = 0; b < NP; ++b) dw = fmaf(sD[ia * NP + b], wb[b], dw);
+              Sr[a * kStripThreads + tid] = sB[ia] * dw * v;
+            }
+          }
+          if (ia == 0 && e_r >= 1 && tid >= N) {
+            const float* ub = br + sc - N;
+            float v = 0.f;
+#pragma unroll
+            for (int b = 0; b < NP; ++b) v = fmaf(sD[N * NP + b], ub[b], v);
+            Ql[a * kStripThreads + tid] = sB[N] * Cs[a * BW + sc] * v;
+            if (adj) {
+              const float* wb = Us + a * BW + sc - N;
+              float dw = 0.f;
+#pragma unroll
+              for (int b = 0; b < NP; ++b) dw = fmaf(sD[N * NP + b], wb[b], dw);
+              Sl[a * kStripThreads + tid] = sB[N] * dw * v;
+            }
+          }
+        }
+      }
+      __syncthreads();
+      // ---- z-lines in registers + phase B + node update for the band's rows
+      if (owned) {
+        float u[NP], cq[NP], du[NP], rz[NP], sz[NP];
+#pragma unroll
+        for (int a = 0; a < NP; ++a) { u[a] = Bs[a * BW + sc]; cq[a] = Cs[a * BW + sc]; }
+#pragma unroll
+        for (int a = 0; a < NP; ++a) {
+          float v = 0.f;
+#pragma unroll
+          for (int b = 0; b < NP; ++b) v = fmaf(sD[a * NP + b], u[b], v);
+          du[a] = v;
+          cq[a] = sB[a] * cq[a] * v;
+        }
+#pragma unroll
+        for (int j = 0; j < NP; ++j) {
+          float v = 0.f;
+#pragma unroll
+          for (int a = 0; a < NP; ++a) v = fmaf(sD[a * NP + j], cq[a], v);
+          rz[j] = v;
+        }
+        if (adj) {
+#pragma unroll
+          for (int a = 0; a < NP; ++a) u[a] = Us[a * BW + sc];
+#pragma unroll
+          for (int a = 0; a < NP; ++a) {
+            float v = 0.f;
+#pragma unroll
+            for (int b = 0; b < NP; ++b) v = fmaf(sD[a * NP + b], u[b], v);
+            sz[a] = sB[a] * v * du[a];
+          }
+        }
+        const int cl = tid - ia;                         // column of the right segment's start
+        for (int a = 0; a < rows; ++a) {
+          const float* qr = Qr + a * kStripThreads;
+          const float* ql = Ql + a * kStripThreads;
+          float X, SX = 0.f;
+          if (ia) {
+            float v = 0.f;
+#pragma unroll
+            for (int p = 0; p < N; ++p) v = fmaf(sD[p * NP + ia], qr[cl + p], v);
+            X = fmaf(sD[N * NP + ia], ql[cl + N], v);
+            if (adj) SX = Sr[a * kStripThreads + tid];
+          } else {
+            X = 0.f;
+            if (e_r >= 1) {
+              float v = 0.f;
+#pragma unroll
+              for (int p = 0; p < N; ++p) v = fmaf(sD[p * NP + N], qr[tid - N + p], v);
+              X = fmaf(sD[N * NP + N], ql[tid], v);
+              if (adj) SX = Sl[a * kStripThreads + tid];
+            }
+            if (e_r < S.nelx) {
+              float v = 0.f;
+#pragma unroll
+              for (int p = 0; p < N; ++p) v = fmaf(sD[p * NP + 0], qr[tid + p], v);
+              X += fmaf(sD[N * NP + 0], ql[tid + N], v);
+              if (adj) SX += Sr[a * kStripThreads + tid];
+            }
+          }
+          // z-line value of this row: rows 1..N-1 interior, row 0 adds the previous band
+          float Z, SZ = 0.f;
+          if (a == 0) {
+            Z = 0.f;
+            if (ez >= 1) Z = zc;
+            Z += rz[0];
+            if (adj) { SZ = 0.f; if (ez >= 1) SZ = szc; SZ += sz[0]; }
+          } else if (a < N) {
+            Z = rz[a];
+            if (adj) SZ = sz[a];
+          } else {  // bottom row of the mesh
+            Z = rz[N];
+            if (adj) SZ = sz[N];
+          }
+          const int gz = ez * N + a;
+          const float izv = S.tz[gz], Rzv = S.tz[S.nzg + gz], dzv = S.tz[2 * S.nzg + gz];
+          const long long g = (long long)gz * S.pitch + gx;
+          float extra = 0.f;
+          if (!adj) {
+            if (gx == S.src_gx && gz == S.src_gz) extra = S.src_term[t];
+          } else {
+            extra = in_win ? sacc[a * kStripThreads + tid] : 0.f;
+            if (grad_on) S.grad[g] = Gs[a * BW + sc] + (double)(Rzv * SX + Rxv * SZ);
+          }
+          float res, vres;
+          advance_node(adj, damp, Bs[a * BW + sc], Vs[a * BW + sc], X, Z, ixv, Rxv, dxv, izv, Rzv, dzv,
+                       extra, res, vres);
+          out[g] = res;
+          vout[g] = vres;
+          bad |= !isfinite(res);
+        }
+        zc = rz[N];
+        if (adj) szc = sz[N];
+      }
+      if (adj && in_win) {  // carry the injection row shared with the next band
+        const float carry = sacc[N * kStripThreads + tid];
+        for (int a = 1; a < NP; ++a) sacc[a * kStripThreads + tid] = 0.f;
+        sacc[tid] = carry;
+      }
+    }
+    __syncthreads();  // everyone is done with this slot and with the exchange arrays
+    if (tid == 0 && ez + kStages < S.nelz) issue(ez + kStages);
+  }
+  if (abort_ez >= 0) {
+    if (tid == 0) atomicOr(S.status, SEM_ERR_TIMEOUT);
+    // drain the bands still in flight (bounded) before the shared memory is released
+    for (int b = abort_ez; b < min(abort_ez + kStages, S.nelz); ++b)
+      mbar_wait(bars + b % kStages, (unsigned)((b / kStages) & 1));
+    return;
   }
   if (__any_sync(0xffffffffu, bad) && lane == 0) atomicOr(S.status, SEM_ERR_NONFINITE);
 }
@@ -568,7 +1012,8 @@ struct sem_plan_s {
   float* rec_w = nullptr;
   int* node_pos = nullptr;
   std::vector<int> h_rec_base;
-  // receiver tile lists per (tile_ex, tile_ez): device arrays rec_off, rec_ids, inj_off, inj_ids
+  // receiver lists per tile (tile kernel, key (tile_ex, tile_ez)) or per strip band
+  // (strip kernel, key (-1, elements per strip)): device arrays rec_off/ids, inj_off/ids
   struct Lists { int* rec_off; int* rec_ids; int* inj_off; int* inj_ids; };
   mutable std::map<std::pair<int, int>, Lists> lists;
   mutable std::mutex mu;
@@ -597,6 +1042,30 @@ int tiles_of(const sem_plan_s* p, int tex, int tez, int* tx, int* tz) {
   return (*tx) * (*tz);
 }
 
+int upload_lists(const sem_plan_s* p, std::pair<int, int> key, std::vector<std::vector<int>>& rec,
+                 std::vector<std::vector<int>>& inj, sem_plan_s::Lists* out) {
+  const int nl = (int)rec.size();
+  for (auto& v : inj)
+    if ((int)v.size() > kMaxInj) return fail(SEM_ERR_ARG, "too many receivers in one tile; use smaller tiles");
+  auto flat = [&](std::vector<std::vector<int>>& v, std::vector<int>& off, std::vector<int>& ids) {
+    off.assign(nl + 1, 0);
+    for (int i = 0; i < nl; ++i) off[i + 1] = off[i] + (int)v[i].size();
+    for (auto& x : v) ids.insert(ids.end(), x.begin(), x.end());
+  };
+  std::vector<int> ro, ri, io, ii;
+  flat(rec, ro, ri);
+  flat(inj, io, ii);
+  sem_plan_s::Lists L{};
+  int rc;
+  if ((rc = upload(&L.rec_off, ro.data(), ro.size()))) return rc;
+  if ((rc = upload(&L.rec_ids, ri.data(), ri.size()))) return rc;
+  if ((rc = upload(&L.inj_off, io.data(), io.size()))) return rc;
+  if ((rc = upload(&L.inj_ids, ii.data(), ii.size()))) return rc;
+  p->lists[key] = L;
+  *out = L;
+  return SEM_OK;
+}
+
 int get_lists(const sem_plan_s* p, int tex, int tez, sem_plan_s::Lists* out) {
   std::lock_guard<std::mutex> lk(p->mu);
   auto key = std::make_pair(tex, tez);
@@ -620,28 +1089,45 @@ int get_lists(const sem_plan_s* p, int tex, int tez, sem_plan_s::Lists* out) {
       }
     for (int tt : seen) inj[tt].push_back(r);
   }
-  auto flat = [&](std::vector<std::vector<int>>& v, std::vector<int>& off, std::vector<int>& ids) {
-    off.assign(ntiles + 1, 0);
-    for (int i = 0; i < ntiles; ++i) off[i + 1] = off[i] + (int)v[i].size();
-    for (auto& x : v) ids.insert(ids.end(), x.begin(), x.end());
-  };
-  for (auto& v : inj)
-    if ((int)v.size() > kMaxInj) return fail(SEM_ERR_ARG, "too many receivers in one tile; use smaller tiles");
-  std::vector<int> ro, ri, io, ii;
-  flat(rec, ro, ri);
-  flat(inj, io, ii);
-  sem_plan_s::Lists L{};
-  int rc;
-  if ((rc = upload(&L.rec_off, ro.data(), ro.size()))) return rc;
-  if ((rc = upload(&L.rec_ids, ri.data(), ri.size()))) return rc;
-  if ((rc = upload(&L.inj_off, io.data(), io.size()))) return rc;
-  if ((rc = upload(&L.inj_ids, ii.data(), ii.size()))) return rc;
-  p->lists[key] = L;
-  *out = L;
-  return SEM_OK;
+  return upload_lists(p, key, rec, inj, out);
+}
+
+// strip kernel lists, indexed strip * nelz + element row
+int get_strip_lists(const sem_plan_s* p, int ew, sem_plan_s::Lists* out) {
+  std::lock_guard<std::mutex> lk(p->mu);
+  auto key = std::make_pair(-1, ew);
+  auto it = p->lists.find(key);
+  if (it != p->lists.end()) { *out = it->second; return SEM_OK; }
+  const int N = p->npol;
+  const int ns = (p->nelx + ew - 1) / ew;
+  std::vector<std::vector<int>> rec((size_t)ns * p->nelz), inj((size_t)ns * p->nelz);
+  for (int r = 0; r < p->nrec; ++r) {
+    const int bx = p->h_rec_base[2 * r], bz = p->h_rec_base[2 * r + 1];
+    const int ex = bx / N, ez = bz / N;
+    rec[(size_t)(ex / ew) * p->nelz + ez].push_back(r);
+    for (int s = 0; s < ns; ++s) {
+      const int sx0 = s * ew * N;
+      const int so1 = (std::min((s + 1) * ew, p->nelx) == p->nelx) ? p->nxg : (s + 1) * ew * N;
+      if (bx + N >= sx0 && bx < so1) inj[(size_t)s * p->nelz + ez].push_back(r);
+    }
+  }
+  return upload_lists(p, key, rec, inj, out);
 }
 
 typedef void (*KernelFn)(const SolveDev*, const int*, const int*, int, int);
+KernelFn strip_kernel_for(int N) {
+  switch (N) {
+    case 1: return sem_strip_kernel<1>;
+    case 2: return sem_strip_kernel<2>;
+    case 3: return sem_strip_kernel<3>;
+    case 4: return sem_strip_kernel<4>;
+    case 5: return sem_strip_kernel<5>;
+    case 6: return sem_strip_kernel<6>;
+    case 7: return sem_strip_kernel<7>;
+  }
+  return nullptr;
+}
+
 KernelFn kernel_for(int N) {
   switch (N) {
     case 1: return sem_tick_kernel<1>;
@@ -695,6 +1181,7 @@ struct sem_batch_s {
   int* d_cta = nullptr;
   long long cta_cap = 0;
   long long last_launches = 0;
+  int last_kernel = 0;
   std::vector<SolveDev> h_solves;
   std::vector<int> h_cta;
 };
@@ -787,12 +1274,15 @@ int sem_batch_destroy(sem_batch_t* b) {
 
 int64_t sem_batch_last_launches(const sem_batch_t* b) { return b ? b->last_launches : -1; }
 
+int32_t sem_batch_last_kernel(const sem_batch_t* b) { return b ? b->last_kernel : -1; }
+
 int sem_run(sem_batch_t* b, const sem_solve_t* solves, int32_t n, const sem_launch_cfg_t* cfg_in,
             void* stream_v) {
   if (!b || (!solves && n) || n < 0) return fail(SEM_ERR_ARG, "null argument");
   cudaStream_t stream = (cudaStream_t)stream_v;
-  sem_launch_cfg_t cfg = cfg_in ? *cfg_in : sem_launch_cfg_t{8, 8, 256, 0};
+  sem_launch_cfg_t cfg = cfg_in ? *cfg_in : sem_launch_cfg_t{8, 8, 256, 0, 0};
   if (cfg.tile_ex < 1 || cfg.tile_ez < 1) return fail(SEM_ERR_ARG, "tile size must be >= 1");
+  if (cfg.kernel < 0 || cfg.kernel > 2) return fail(SEM_ERR_ARG, "kernel must be 0 (auto), 1 (tile), 2 (strip)");
   if (cfg.threads < 32 || cfg.threads > 256 || cfg.threads % 32) cfg.threads = 256;
   b->last_launches = 0;
   if (n == 0) return SEM_OK;
@@ -815,6 +1305,20 @@ int sem_run(sem_batch_t* b, const sem_solve_t* solves, int32_t n, const sem_laun
     const int nt = s.plan->nt;
     prog[i] = nt + ((s.flags & SEM_F_SHIFT) ? 1 : 0) + (adj ? 1 + nt + kk[i] * (nseg[i] - 1) : 0);
   }
+  // kernel variant: strips when the batch alone fills the GPU, tiles otherwise
+  bool use_strip = (cfg.kernel == 2);
+  if (cfg.kernel == 0) {
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    long long strips = 0;
+    for (int i = 0; i < n; ++i) {
+      const sem_plan_s* p = solves[i].plan;
+      strips += (p->nelx + strip_ew_max(p->npol) - 1) / strip_ew_max(p->npol);
+    }
+    use_strip = strips >= sms;
+  }
+  b->last_kernel = use_strip ? 2 : 1;
   if (total > b->arena_bytes) {
     cudaFree(b->arena);
     b->arena = nullptr;
@@ -841,10 +1345,19 @@ int sem_run(sem_batch_t* b, const sem_solve_t* solves, int32_t n, const sem_laun
     const sem_plan_s* p = s.plan;
     if (p->device != b->device) return fail(SEM_ERR_ARG, "plan and batch on different devices");
     sem_plan_s::Lists L;
-    int rc = get_lists(p, cfg.tile_ex, cfg.tile_ez, &L);
+    int ntx, ntz, ntiles, rc;
+    if (use_strip) {
+      const int ewm = strip_ew_max(p->npol);
+      ntx = (p->nelx + ewm - 1) / ewm;             // strips
+      ntz = (p->nelx + ntx - 1) / ntx;             // elements per strip (balanced)
+      ntx = (p->nelx + ntz - 1) / ntz;
+      ntiles = ntx;
+      rc = get_strip_lists(p, ntz, &L);
+    } else {
+      ntiles = tiles_of(p, cfg.tile_ex, cfg.tile_ez, &ntx, &ntz);
+      rc = get_lists(p, cfg.tile_ex, cfg.tile_ez, &L);
+    }
     if (rc) return rc;
-    int ntx, ntz;
-    const int ntiles = tiles_of(p, cfg.tile_ex, cfg.tile_ez, &ntx, &ntz);
     if (groups.empty() || groups.back().N != p->npol)
       groups.push_back(Group{p->npol, (long long)b->h_cta.size(), 0, false});
     Group& G = groups.back();
@@ -931,9 +1444,11 @@ int sem_run(sem_batch_t* b, const sem_solve_t* solves, int32_t n, const sem_laun
   struct Launch { KernelFn fn; long long cta0, ncta; size_t smem; };
   std::vector<Launch> launches;
   for (auto& G : groups) {
-    KernelFn fn = kernel_for(G.N);
+    KernelFn fn = use_strip ? strip_kernel_for(G.N) : kernel_for(G.N);
     if (!fn) return fail(SEM_ERR_UNSUPPORTED, "polynomial order");
-    const size_t smem = (size_t)smem_floats(G.N, cfg.tile_ex, cfg.tile_ez, G.adj) * sizeof(float);
+    const size_t smem = (size_t)(use_strip ? strip_smem_floats(G.N, G.adj)
+                                           : smem_floats(G.N, cfg.tile_ex, cfg.tile_ez, G.adj)) *
+                        sizeof(float);
     if (smem > 227 * 1024) return fail(SEM_ERR_ARG, "tile too large for shared memory");
     CUDA_TRY(cudaFuncSetAttribute((const void*)fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     launches.push_back(Launch{fn, G.cta0, G.ncta, smem});
@@ -950,8 +1465,8 @@ int sem_run(sem_batch_t* b, const sem_solve_t* solves, int32_t n, const sem_laun
   auto launch_tick = [&]() -> int {
     for (size_t gi = 0; gi < launches.size(); ++gi) {
       const Launch& Lc = launches[gi];
-      Lc.fn<<<(unsigned)Lc.ncta, cfg.threads, Lc.smem, stream>>>(gdesc[gi], b->d_cta + Lc.cta0,
-                                                                 b->d_tick, cfg.tile_ex, cfg.tile_ez);
+      Lc.fn<<<(unsigned)Lc.ncta, use_strip ? kStripThreads : cfg.threads, Lc.smem, stream>>>(
+          gdesc[gi], b->d_cta + Lc.cta0, b->d_tick, cfg.tile_ex, cfg.tile_ez);
     }
     tick_advance_kernel<<<1, 1, 0, stream>>>(b->d_tick);
     return SEM_OK;

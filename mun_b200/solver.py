@@ -70,12 +70,13 @@ def choose_ckpt_k(plan, n_solves, budget_bytes=None):
 class Batch:
     """Owns a ``sem_batch_t`` (workspace arena, descriptors, tick counter)."""
 
-    def __init__(self, tile=(8, 8), threads=256, graph_chunk=0):
+    def __init__(self, tile=(8, 8), threads=256, graph_chunk=0, kernel=0):
         lib = _lib.load()
         h = C.c_void_p()
         _lib.check(lib.sem_batch_create(C.byref(h)))
         self.handle, self._lib = h, lib
         self.tile, self.threads, self.graph_chunk = tuple(tile), int(threads), int(graph_chunk)
+        self.kernel = int(kernel)  # 0 auto, 1 tile, 2 strip
         self._side = None
 
     def __del__(self):
@@ -92,7 +93,11 @@ class Batch:
     def last_launches(self):
         return int(self._lib.sem_batch_last_launches(self.handle))
 
-    def run(self, specs, tile=None, graph_chunk=None, memory_budget=None):
+    @property
+    def last_kernel(self):
+        return {1: "tile", 2: "strip"}.get(int(self._lib.sem_batch_last_kernel(self.handle)), "none")
+
+    def run(self, specs, tile=None, graph_chunk=None, memory_budget=None, kernel=None):
         n = len(specs)
         arr = (_lib.Solve * max(n, 1))()
         keep = []
@@ -145,7 +150,8 @@ class Batch:
             a.status_out = s.status.data_ptr()
         t = tile or self.tile
         cfg = _lib.LaunchCfg(int(t[0]), int(t[1]), self.threads,
-                             int(self.graph_chunk if graph_chunk is None else graph_chunk))
+                             int(self.graph_chunk if graph_chunk is None else graph_chunk),
+                             int(self.kernel if kernel is None else kernel))
         cur = torch.cuda.current_stream()
         if cfg.graph_chunk > 0 and cur.cuda_stream == 0:
             # graphs cannot be captured on the legacy default stream: use a side stream

@@ -104,3 +104,22 @@ def test_nonfinite_velocity_sets_status():
     s = SolveSpec(plan, dev(v))
     Batch().run([s])
     assert int(s.status.item()) != 0
+
+
+def test_misfit_window_matches_oracle():
+    """CO2 misfit window with decimation (single_cubic core.py:1441-1552) vs the oracle."""
+    g = load("inject_n3")
+    plan = plan_for(g["config"], g["dt"], g["nt"])
+    y = aligned_obs(g)
+    nt = int(g["nt"])
+    win = (nt // 5, 4 * nt // 5, 2)
+    yw = y[win[0]:win[1]][::win[2]]
+    s = SolveSpec(plan, dev(g["velocity"]), adjoint=True, y_obs=dev(yw), window=win,
+                  inv_sigma2=1.0 / float(g["sigma"]) ** 2)
+    Batch().run([s])
+    sim = so.build_sim(g["config"], g["velocity"], dt=float(g["dt"]))
+    ref = so.forward_adjoint(sim, yw, float(g["sigma"]), window=win)
+    e_g = rel_l2(-s.grad.cpu().numpy(), ref["dL_dv"])
+    e_l = abs(float(s.loglik.item()) - ref["loglik"]) / abs(ref["loglik"])
+    print(f"window: dL/dv {e_g:.2e} loglik {e_l:.2e}")
+    assert e_g <= TOL and e_l <= TOL
