@@ -536,20 +536,23 @@ __global__ void __launch_bounds__(256) sem_tick_kernel(const SolveDev* __restric
 // ----------------------------------------------------------------------------
 // strip kernel: one CTA per full-height strip of element columns (large batches)
 //
-// Threads map to grid columns: N left-halo columns, the strip's owned columns and the
-// shared column on its right.  The CTA sweeps the strip one element row at a time.
-// Each band of N+1 grid rows (every field the step reads) is staged by TMA bulk
-// copies into a ring of kStages shared-memory slots, issued kStages bands ahead and
-// completed on an mbarrier.  Per band: x-lines through a two-phase exchange of
-// per-node fluxes in shared memory, z-lines in registers (the band holds the whole
-// element column segment), then the node update for the band's N rows.
+// Columns: N left-halo columns, the strip's owned columns and the shared column on its
+// right (kStripCols threads per band row).  The CTA sweeps the strip one element row
+// ("band", N+1 grid rows) at a time; each band of every field the step reads is
+// staged by TMA bulk copies (cp.async.bulk + mbarrier) into a ring of kStages slots,
+// issued kStages bands ahead.  One thread per (band row, column): phase A forms the
+// per-node fluxes beta c^2 (D u) of the x-line and z-line segments through the node,
+// phase B contracts them with D^T and advances the node.  Both directions use the
+// same arithmetic order as the tile kernel (bitwise-equal results).
 // ----------------------------------------------------------------------------
-constexpr int kStripThreads = 128;
+constexpr int kStripCols = 128;
 constexpr int kStages = 3;
+constexpr int kStripInj = 256;               // receivers per band of one strip (host-checked)
 constexpr long long kWaitNs = 2000000000LL;  // bounded mbarrier waits: 2 s
 
-__host__ __device__ inline int strip_ew_max(int N) { return (kStripThreads - N - 1) / N; }
-__host__ __device__ inline int strip_bw(int N) { return (kStripThreads + 3 + 3) & ~3; }  // smem row
+__host__ __device__ inline int strip_ew_max(int N) { return (kStripCols - N - 1) / N; }
+__host__ __device__ inline int strip_bw(int N) { return (kStripCols + 3 + 3) & ~3; }  // smem row
+__host__ __device__ inline int strip_threads(int N) { return N * kStripCols; }
 
 __device__ __forceinline__ uint32_t smem_addr(const void* p) {
   return (uint32_t)__cvta_generic_to_shared(p);
@@ -594,24 +597,31 @@ __device__ __forceinline__ void bulk_load(void* dst, const void* src, unsigned b
       : "memory");
 }
 
-// shared-memory floats of one strip CTA (stages + exchange arrays + injection rows)
-__host__ __device__ inline long long strip_smem_floats(int N, bool adj) {
-  const int BW = strip_bw(N);
+__host__ __device__ inline long long strip_stage_floats(int N, bool adj) {
   const int nfloat = adj ? 4 : 3;  // cur, c2, v (+ forward field)
   const int ndouble = adj ? 1 : 0;  // gradient accumulator
-  const long long stage = ((long long)(nfloat + 2 * ndouble) * (N + 1) * BW + 31) & ~31LL;
-  const long long xch = (long long)(adj ? 4 : 2) * (N + 1) * kStripThreads;
-  const long long inj = adj ? (long long)(N + 1) * kStripThreads + kMaxInj : 0;
-  return 64 + 96 + kStages * stage + xch + inj;  // barriers, D/beta, ...
+  return ((long long)(nfloat + 2 * ndouble) * (N + 1) * strip_bw(N) + 31) & ~31LL;
+}
+// exchange arrays: Qr, Ql (x) and Qz (z) fluxes [+ Sr, Sl, Sz], z carries, injection rows
+__host__ __device__ inline long long strip_xch_floats(int N, bool adj) {
+  const long long row = kStripCols;
+  long long f = 3LL * (N + 1) * row + 2 * row;                    // Qr Ql Qz | zcarry[2]
+  if (adj) f += 3LL * (N + 1) * row + 2 * row + (N + 1) * row + kStripInj;  // S | scarry | inj
+  return (f + 31) & ~31LL;
+}
+__host__ __device__ inline long long strip_smem_floats(int N, bool adj) {
+  return 64 + 96 + kStages * strip_stage_floats(N, adj) + strip_xch_floats(N, adj);
 }
 
 template <int N>
-__global__ void __launch_bounds__(kStripThreads) sem_strip_kernel(const SolveDev* __restrict__ solves,
-                                                                  const int* __restrict__ cta_solve,
-                                                                  const int* __restrict__ tick_ptr,
-                                                                  int ew_unused, int unused) {
+__global__ void __launch_bounds__(N * kStripCols) sem_strip_kernel(const SolveDev* __restrict__ solves,
+                                                                   const int* __restrict__ cta_solve,
+                                                                   const int* __restrict__ tick_ptr,
+                                                                   int unused0, int unused1) {
   constexpr int NP = N + 1;
-  constexpr int BW = (kStripThreads + 3 + 3) & ~3;
+  constexpr int BW = (kStripCols + 3 + 3) & ~3;
+  constexpr int NT = N * kStripCols;
+  constexpr int R = kStripCols;  // row stride of the exchange arrays
   extern __shared__ __align__(128) float smem[];
   __shared__ SolveDev S;
   __shared__ int s_act, s_t, s_seg, s_abort;
@@ -620,7 +630,7 @@ __global__ void __launch_bounds__(kStripThreads) sem_strip_kernel(const SolveDev
   {
     const unsigned long long* src = reinterpret_cast<const unsigned long long*>(solves + sid);
     unsigned long long* dst = reinterpret_cast<unsigned long long*>(&S);
-    for (int i = threadIdx.x; i < (int)(sizeof(SolveDev) / 8); i += blockDim.x) dst[i] = src[i];
+    for (int i = threadIdx.x; i < (int)(sizeof(SolveDev) / 8); i += NT) dst[i] = src[i];
   }
   __syncthreads();
   if (threadIdx.x == 0) {
@@ -649,30 +659,34 @@ __global__ void __launch_bounds__(kStripThreads) sem_strip_kernel(const SolveDev
   const int e0 = strip * EW, e1 = min(e0 + EW, S.nelx);
   const int sx0 = e0 * N;                                   // first owned column
   const int so1 = (e1 == S.nelx) ? S.nxg : e1 * N;          // owned columns [sx0, so1)
-  const int NC = (e1 - e0) * N + N + 1;                     // thread columns
+  const int NC = (e1 - e0) * N + N + 1;                     // columns in use
   const int X0 = (sx0 - N) & ~3;                            // 16-byte aligned copy origin
-  const int off = (sx0 - N) - X0;                           // smem column of thread 0
+  const int off = (sx0 - N) - X0;
   const int cs = max(X0, 0), ce = min(X0 + BW, S.pitch);    // copied columns
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const int gx = sx0 - N + tid;
-  const bool col_valid = tid < NC && gx >= 0 && gx < S.nxg;
+  const int col = tid % R, row = tid / R;                   // this thread's column and band row
+  const int gx = sx0 - N + col;
+  const bool col_valid = col < NC && gx >= 0 && gx < S.nxg;
   const bool owned = col_valid && gx >= sx0 && gx < so1;
-  const int sc = tid + off;                                 // this thread's smem column
+  const int sc = col + off;
 
-  // ---------------- shared memory carve-up
-  unsigned long long* bars = reinterpret_cast<unsigned long long*>(smem);  // kStages barriers
+  // ---------------- shared memory
+  unsigned long long* bars = reinterpret_cast<unsigned long long*>(smem);
   float* sD = smem + 64;
   float* sB = sD + 64;
   const int nfloat = (adj ? 4 : 3), ndouble = (adj ? 1 : 0);
-  const long long stage_f = ((long long)(nfloat + 2 * ndouble) * NP * BW + 31) & ~31LL;
+  const long long stage_f = strip_stage_floats(N, adj || final_only ? adj : false);
   float* stages = smem + 64 + 96;
-  float* xch = stages + kStages * stage_f;
-  float* Qr = xch;                       // [NP][kStripThreads]
-  float* Ql = Qr + NP * kStripThreads;
-  float* Sr = Ql + NP * kStripThreads;   // adjoint only
-  float* Sl = Sr + NP * kStripThreads;
-  float* sacc = xch + (adj ? 4 : 2) * NP * kStripThreads;  // [NP][kStripThreads]
-  float* sres = sacc + NP * kStripThreads;
+  float* Qr = stages + kStages * stage_f;  // [NP][R]
+  float* Ql = Qr + NP * R;                 // [NP][R]
+  float* Qz = Ql + NP * R;                 // [NP][R]
+  float* zcar = Qz + NP * R;               // [2][R]
+  float* Sr = zcar + 2 * R;                // adjoint: [NP][R] x3, [2][R]
+  float* Sl = Sr + NP * R;
+  float* Sz = Sl + NP * R;
+  float* scar = Sz + NP * R;
+  float* sacc = scar + 2 * R;              // [NP][R]
+  float* sres = sacc + NP * R;             // [kStripInj]
 
   // ---------------- which fields
   const float* cur;
@@ -695,53 +709,52 @@ __global__ void __launch_bounds__(kStripThreads) sem_strip_kernel(const SolveDev
     vout = S.Mu;
     fwdu = S.ring + (long long)(t + 1 - seg * S.k) * S.fstride;
   }
-  const float* fsrc[4] = {cur, S.c2, vin, fwdu};
-  const int nload = final_only ? 1 : nfloat;  // FINAL reads only b
+  const int nload = final_only ? 1 : nfloat;
 
   if (tid == 0) {
     for (int s = 0; s < kStages; ++s) mbar_init(bars + s, 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
-  for (int i = tid; i < NP * NP; i += kStripThreads) sD[i] = S.D[i];
-  for (int i = tid; i < NP; i += kStripThreads) sB[i] = S.beta[i];
+  for (int i = tid; i < NP * NP; i += NT) sD[i] = S.D[i];
+  for (int i = tid; i < NP; i += NT) sB[i] = S.beta[i];
   __syncthreads();
 
-  // issue the TMA copies of element row `ez` into ring slot ez % kStages
+  // TMA: element row `ez` of every field into ring slot ez % kStages
   auto issue = [&](int ez) {
     const int slot = ez % kStages;
     float* st = stages + slot * stage_f;
     const unsigned rowb = (unsigned)(ce - cs) * 4u;
-    unsigned total = (unsigned)nload * NP * rowb + (unsigned)(final_only ? 0 : ndouble) * NP * rowb * 2u;
+    const unsigned total = (unsigned)nload * NP * rowb +
+                           (final_only ? 0u : (unsigned)ndouble * NP * rowb * 2u);
     mbar_expect_tx(bars + slot, total);
-    for (int f = 0; f < nload; ++f)
-      for (int a = 0; a < NP; ++a) {
-        const long long grow = (long long)(ez * N + a) * S.pitch;
-        bulk_load(st + (f * NP + a) * BW + (cs - X0), fsrc[f] + grow + cs, rowb, bars + slot);
-      }
+    for (int f = 0; f < nload; ++f) {
+      const float* base = (f == 0) ? cur : (f == 1) ? S.c2 : (f == 2) ? vin : fwdu;
+      for (int a = 0; a < NP; ++a)
+        bulk_load(st + (f * NP + a) * BW + (cs - X0), base + (long long)(ez * N + a) * S.pitch + cs,
+                  rowb, bars + slot);
+    }
     if (ndouble && !final_only) {
       double* gs = reinterpret_cast<double*>(st + nfloat * NP * BW);
-      for (int a = 0; a < NP; ++a) {
-        const long long grow = (long long)(ez * N + a) * S.pitch;
-        bulk_load(gs + a * BW + (cs - X0), S.grad + grow + cs, rowb * 2u, bars + slot);
-      }
+      for (int a = 0; a < NP; ++a)
+        bulk_load(gs + a * BW + (cs - X0), S.grad + (long long)(ez * N + a) * S.pitch + cs,
+                  rowb * 2u, bars + slot);
     }
   };
   if (tid == 0)
     for (int ez = 0; ez < min(kStages, S.nelz); ++ez) issue(ez);
 
-  // per-column tables
   float ixv = 0.f, Rxv = 0.f, dxv = 0.f;
-  if (owned) { ixv = S.tx[gx]; Rxv = S.tx[S.nxg + gx]; dxv = S.tx[2 * S.nxg + gx]; }
+  if (owned) { ixv = __ldg(S.tx + gx); Rxv = __ldg(S.tx + S.nxg + gx); dxv = __ldg(S.tx + 2 * S.nxg + gx); }
   const int e_r = col_valid ? gx / N : 0, ia = col_valid ? gx - e_r * N : 0;
   const bool damp = (act != A_ADJ) || (S.flags & F_EXACT);
   const bool grad_on = adj && t >= S.it0 && t < S.it1;
   const bool in_win = adj && t >= S.it0 && t < S.it1 && ((t - S.it0) % S.decim) == 0;
   const int ms = t - ((S.flags & F_SHIFT) ? 1 : 0);
   const bool rec_on = (act == A_FWD || act == A_FINAL) && ms >= 0 && ms < S.nt;
-  float zc = 0.f, szc = 0.f;  // z-line carries into the next band's first row
-  int abort_ez = -1;
-  if (adj) for (int a = 0; a < NP; ++a) sacc[a * kStripThreads + tid] = 0.f;
+  if (adj && in_win)
+    for (int i = tid; i < NP * R; i += NT) sacc[i] = 0.f;
   bool bad = false;
+  int abort_ez = -1;
 
   for (int ez = 0; ez < S.nelz; ++ez) {
     const int slot = ez % kStages;
@@ -754,13 +767,12 @@ __global__ void __launch_bounds__(kStripThreads) sem_strip_kernel(const SolveDev
     if (!mbar_wait(bars + slot, (unsigned)((ez / kStages) & 1))) s_abort = 1;
     __syncthreads();
     if (s_abort) { abort_ez = ez; break; }
-    const int rows = (ez == S.nelz - 1) ? NP : N;  // the last band also owns the bottom row
+    const bool last = (ez == S.nelz - 1);  // the last band also owns the bottom grid row
 
-    // ---- receivers recorded from this band (one warp per receiver)
-    if (rec_on) {
+    if (rec_on) {  // receivers read out of this band, one warp each
       const int li = strip * S.nelz + ez;
       const int off0 = S.rec_tile_off[li], cnt = S.rec_tile_off[li + 1] - off0;
-      for (int q = warp; q < cnt; q += kStripThreads / 32) {
+      for (int q = warp; q < cnt; q += NT / 32) {
         const int r = S.rec_tile_ids[off0 + q];
         const int bx = S.rec_base[2 * r];
         const float* wr = S.rec_w + (long long)r * NP * NP;
@@ -782,14 +794,13 @@ __global__ void __launch_bounds__(kStripThreads) sem_strip_kernel(const SolveDev
       }
     }
     if (!final_only) {
-      // ---- adjoint source of receivers in this element row
-      if (in_win) {
+      if (in_win) {  // adjoint source of receivers in this element row
         const int li = strip * S.nelz + ez;
         const int off0 = S.inj_tile_off[li], cnt = S.inj_tile_off[li + 1] - off0;
         if (cnt > 0) {
           const double ascale = *S.adj_scale;
           const long long yrow = (long long)((t - S.it0) / S.decim) * S.nrec;
-          for (int q = tid; q < cnt; q += kStripThreads) {
+          for (int q = tid; q < cnt; q += NT) {
             const int r = S.inj_tile_ids[off0 + q];
             const double res = (double)S.rec_out[(long long)t * S.nrec + r] - S.yobs[yrow + r];
             sres[q] = (float)(res * ascale);
@@ -803,155 +814,152 @@ __global__ void __launch_bounds__(kStripThreads) sem_strip_kernel(const SolveDev
               const float* wr = S.rec_w + (long long)r * NP * NP;
               for (int e = lane; e < NP * NP; e += 32) {
                 const int j = e / NP, i = e - j * NP;
-                const int c = bx + i - (sx0 - N);
                 const int gxx = bx + i;
-                if (gxx >= sx0 && gxx < so1) sacc[j * kStripThreads + c] += wr[e] * rs;
+                if (gxx >= sx0 && gxx < so1) sacc[j * R + (gxx - (sx0 - N))] += wr[e] * rs;
               }
               __syncwarp();
             }
           }
         }
       }
-      // ---- phase A: per-node x-line fluxes q = beta c^2 (D u) (and D u_fwd for S)
+      // ---- phase A: fluxes at (row, col); rows handled: row, and row N (row 0 threads)
       if (col_valid) {
-        for (int a = 0; a < rows; ++a) {
-          const float* br = Bs + a * BW;
-          if (e_r < S.nelx && tid < NC - 1) {
-            const float* ub = br + sc - ia;
-            float v = 0.f;
+        for (int a = row; a < NP; a += N) {
+          if (a < N || last) {  // x-line fluxes are needed for output rows only
+            const float* br = Bs + a * BW;
+            if (e_r < S.nelx && col < NC - 1) {
+              const float* ub = br + sc - ia;
+              float v = 0.f;
 #pragma unroll
-            for (int b = 0; b < NP; ++b) v = fmaf(sD[ia * NP + b], ub[b], v);
-            Qr[a * kStripThreads + tid] = sB[ia] * Cs[a * BW + sc] * v;
-            if (adj) {
-              const float* wb = Us + a * BW + sc - ia;
-              float dw = 0.f;
+              for (int b = 0; b < NP; ++b) v = fmaf(sD[ia * NP + b], ub[b], v);
+              Qr[a * R + col] = sB[ia] * Cs[a * BW + sc] * v;
+              if (adj) {
+                const float* wb = Us + a * BW + sc - ia;
+                float dw = 0.f;
 #pragma unroll
-              for (int b = 0; b < NP; ++b) dw = fmaf(sD[ia * NP + b], wb[b], dw);
-              Sr[a * kStripThreads + tid] = sB[ia] * dw * v;
+                for (int b = 0; b < NP; ++b) dw = fmaf(sD[ia * NP + b], wb[b], dw);
+                Sr[a * R + col] = sB[ia] * dw * v;
+              }
+            }
+            if (ia == 0 && e_r >= 1 && col >= N) {
+              const float* ub = br + sc - N;
+              float v = 0.f;
+#pragma unroll
+              for (int b = 0; b < NP; ++b) v = fmaf(sD[N * NP + b], ub[b], v);
+              Ql[a * R + col] = sB[N] * Cs[a * BW + sc] * v;
+              if (adj) {
+                const float* wb = Us + a * BW + sc - N;
+                float dw = 0.f;
+#pragma unroll
+                for (int b = 0; b < NP; ++b) dw = fmaf(sD[N * NP + b], wb[b], dw);
+                Sl[a * R + col] = sB[N] * dw * v;
+              }
             }
           }
-          if (ia == 0 && e_r >= 1 && tid >= N) {
-            const float* ub = br + sc - N;
+          if (owned) {  // z-line flux at band point a
             float v = 0.f;
 #pragma unroll
-            for (int b = 0; b < NP; ++b) v = fmaf(sD[N * NP + b], ub[b], v);
-            Ql[a * kStripThreads + tid] = sB[N] * Cs[a * BW + sc] * v;
+            for (int b = 0; b < NP; ++b) v = fmaf(sD[a * NP + b], Bs[b * BW + sc], v);
+            Qz[a * R + col] = sB[a] * Cs[a * BW + sc] * v;
             if (adj) {
-              const float* wb = Us + a * BW + sc - N;
               float dw = 0.f;
 #pragma unroll
-              for (int b = 0; b < NP; ++b) dw = fmaf(sD[N * NP + b], wb[b], dw);
-              Sl[a * kStripThreads + tid] = sB[N] * dw * v;
+              for (int b = 0; b < NP; ++b) dw = fmaf(sD[a * NP + b], Us[b * BW + sc], dw);
+              Sz[a * R + col] = sB[a] * dw * v;
             }
           }
         }
       }
       __syncthreads();
-      // ---- z-lines in registers + phase B + node update for the band's rows
+      // ---- phase B: contract, combine, advance the node
       if (owned) {
-        float u[NP], cq[NP], du[NP], rz[NP], sz[NP];
-#pragma unroll
-        for (int a = 0; a < NP; ++a) { u[a] = Bs[a * BW + sc]; cq[a] = Cs[a * BW + sc]; }
-#pragma unroll
-        for (int a = 0; a < NP; ++a) {
-          float v = 0.f;
-#pragma unroll
-          for (int b = 0; b < NP; ++b) v = fmaf(sD[a * NP + b], u[b], v);
-          du[a] = v;
-          cq[a] = sB[a] * cq[a] * v;
-        }
-#pragma unroll
-        for (int j = 0; j < NP; ++j) {
-          float v = 0.f;
-#pragma unroll
-          for (int a = 0; a < NP; ++a) v = fmaf(sD[a * NP + j], cq[a], v);
-          rz[j] = v;
-        }
-        if (adj) {
-#pragma unroll
-          for (int a = 0; a < NP; ++a) u[a] = Us[a * BW + sc];
-#pragma unroll
-          for (int a = 0; a < NP; ++a) {
-            float v = 0.f;
-#pragma unroll
-            for (int b = 0; b < NP; ++b) v = fmaf(sD[a * NP + b], u[b], v);
-            sz[a] = sB[a] * v * du[a];
-          }
-        }
-        const int cl = tid - ia;                         // column of the right segment's start
-        for (int a = 0; a < rows; ++a) {
-          const float* qr = Qr + a * kStripThreads;
-          const float* ql = Ql + a * kStripThreads;
+        const float* cin = zcar + (ez & 1) * R;
+        float* cnext = zcar + ((ez + 1) & 1) * R;
+        const float* sin_ = scar + (ez & 1) * R;
+        float* snext = scar + ((ez + 1) & 1) * R;
+        for (int a = row; a < (last ? NP : N); a += N) {
+          const int aq = a;
+          const float* qr = Qr + aq * R;
+          const float* ql = Ql + aq * R;
+          const int cl = col - ia;
           float X, SX = 0.f;
           if (ia) {
             float v = 0.f;
 #pragma unroll
             for (int p = 0; p < N; ++p) v = fmaf(sD[p * NP + ia], qr[cl + p], v);
             X = fmaf(sD[N * NP + ia], ql[cl + N], v);
-            if (adj) SX = Sr[a * kStripThreads + tid];
+            if (adj) SX = Sr[aq * R + col];
           } else {
             X = 0.f;
             if (e_r >= 1) {
               float v = 0.f;
 #pragma unroll
-              for (int p = 0; p < N; ++p) v = fmaf(sD[p * NP + N], qr[tid - N + p], v);
-              X = fmaf(sD[N * NP + N], ql[tid], v);
-              if (adj) SX = Sl[a * kStripThreads + tid];
+              for (int p = 0; p < N; ++p) v = fmaf(sD[p * NP + N], qr[col - N + p], v);
+              X = fmaf(sD[N * NP + N], ql[col], v);
+              if (adj) SX = Sl[aq * R + col];
             }
             if (e_r < S.nelx) {
               float v = 0.f;
 #pragma unroll
-              for (int p = 0; p < N; ++p) v = fmaf(sD[p * NP + 0], qr[tid + p], v);
-              X += fmaf(sD[N * NP + 0], ql[tid + N], v);
-              if (adj) SX += Sr[a * kStripThreads + tid];
+              for (int p = 0; p < N; ++p) v = fmaf(sD[p * NP + 0], qr[col + p], v);
+              X += fmaf(sD[N * NP + 0], ql[col + N], v);
+              if (adj) SX += Sr[aq * R + col];
             }
           }
-          // z-line value of this row: rows 1..N-1 interior, row 0 adds the previous band
           float Z, SZ = 0.f;
-          if (a == 0) {
-            Z = 0.f;
-            if (ez >= 1) Z = zc;
-            Z += rz[0];
-            if (adj) { SZ = 0.f; if (ez >= 1) SZ = szc; SZ += sz[0]; }
-          } else if (a < N) {
-            Z = rz[a];
-            if (adj) SZ = sz[a];
-          } else {  // bottom row of the mesh
-            Z = rz[N];
-            if (adj) SZ = sz[N];
+          if (a < N) {
+            float v = 0.f;
+#pragma unroll
+            for (int p = 0; p < NP; ++p) v = fmaf(sD[p * NP + a], Qz[p * R + col], v);
+            if (a == 0) {
+              Z = 0.f;
+              if (ez >= 1) Z = cin[col];
+              Z += v;
+              if (adj) { SZ = 0.f; if (ez >= 1) SZ = sin_[col]; SZ += Sz[col]; }
+              // carry of this element's last point into the next band's first row
+              float w = 0.f;
+#pragma unroll
+              for (int p = 0; p < NP; ++p) w = fmaf(sD[p * NP + N], Qz[p * R + col], w);
+              cnext[col] = w;
+              if (adj) snext[col] = Sz[N * R + col];
+            } else {
+              Z = v;
+              if (adj) SZ = Sz[a * R + col];
+            }
+          } else {  // bottom row of the mesh: only the element above
+            Z = cnext[col];
+            if (adj) SZ = snext[col];
           }
           const int gz = ez * N + a;
-          const float izv = S.tz[gz], Rzv = S.tz[S.nzg + gz], dzv = S.tz[2 * S.nzg + gz];
+          const float izv = __ldg(S.tz + gz), Rzv = __ldg(S.tz + S.nzg + gz), dzv = __ldg(S.tz + 2 * S.nzg + gz);
           const long long g = (long long)gz * S.pitch + gx;
           float extra = 0.f;
           if (!adj) {
             if (gx == S.src_gx && gz == S.src_gz) extra = S.src_term[t];
           } else {
-            extra = in_win ? sacc[a * kStripThreads + tid] : 0.f;
+            extra = in_win ? sacc[a * R + col] : 0.f;
             if (grad_on) S.grad[g] = Gs[a * BW + sc] + (double)(Rzv * SX + Rxv * SZ);
           }
           float res, vres;
-          advance_node(adj, damp, Bs[a * BW + sc], Vs[a * BW + sc], X, Z, ixv, Rxv, dxv, izv, Rzv, dzv,
-                       extra, res, vres);
+          advance_node(adj, damp, Bs[a * BW + sc], Vs[a * BW + sc], X, Z, ixv, Rxv, dxv, izv, Rzv,
+                       dzv, extra, res, vres);
           out[g] = res;
           vout[g] = vres;
           bad |= !isfinite(res);
         }
-        zc = rz[N];
-        if (adj) szc = sz[N];
-      }
-      if (adj && in_win) {  // carry the injection row shared with the next band
-        const float carry = sacc[N * kStripThreads + tid];
-        for (int a = 1; a < NP; ++a) sacc[a * kStripThreads + tid] = 0.f;
-        sacc[tid] = carry;
       }
     }
-    __syncthreads();  // everyone is done with this slot and with the exchange arrays
+    __syncthreads();  // done with this slot, the flux arrays and the injection rows
+    if (adj && in_win && !final_only && row == 0) {  // carry the injection row shared with the next band
+      const float carry = sacc[N * R + col];
+      for (int a = 1; a < NP; ++a) sacc[a * R + col] = 0.f;
+      sacc[col] = carry;
+    }
     if (tid == 0 && ez + kStages < S.nelz) issue(ez + kStages);
+    if (adj && in_win) __syncthreads();
   }
   if (abort_ez >= 0) {
     if (tid == 0) atomicOr(S.status, SEM_ERR_TIMEOUT);
-    // drain the bands still in flight (bounded) before the shared memory is released
     for (int b = abort_ez; b < min(abort_ez + kStages, S.nelz); ++b)
       mbar_wait(bars + b % kStages, (unsigned)((b / kStages) & 1));
     return;
@@ -1111,6 +1119,8 @@ int get_strip_lists(const sem_plan_s* p, int ew, sem_plan_s::Lists* out) {
       if (bx + N >= sx0 && bx < so1) inj[(size_t)s * p->nelz + ez].push_back(r);
     }
   }
+  for (auto& v : inj)
+    if ((int)v.size() > kStripInj) return fail(SEM_ERR_ARG, "too many receivers in one strip band");
   return upload_lists(p, key, rec, inj, out);
 }
 
@@ -1441,7 +1451,7 @@ int sem_run(sem_batch_t* b, const sem_solve_t* solves, int32_t n, const sem_laun
   CUDA_TRY(cudaGetLastError());
 
   // ---- per-group launch parameters
-  struct Launch { KernelFn fn; long long cta0, ncta; size_t smem; };
+  struct Launch { KernelFn fn; long long cta0, ncta; size_t smem; int N; };
   std::vector<Launch> launches;
   for (auto& G : groups) {
     KernelFn fn = use_strip ? strip_kernel_for(G.N) : kernel_for(G.N);
@@ -1451,7 +1461,7 @@ int sem_run(sem_batch_t* b, const sem_solve_t* solves, int32_t n, const sem_laun
                         sizeof(float);
     if (smem > 227 * 1024) return fail(SEM_ERR_ARG, "tile too large for shared memory");
     CUDA_TRY(cudaFuncSetAttribute((const void*)fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    launches.push_back(Launch{fn, G.cta0, G.ncta, smem});
+    launches.push_back(Launch{fn, G.cta0, G.ncta, smem, G.N});
   }
   // solve descriptor sub-array of each group starts at the first solve of that group
   std::vector<const SolveDev*> gdesc;
@@ -1465,7 +1475,7 @@ int sem_run(sem_batch_t* b, const sem_solve_t* solves, int32_t n, const sem_laun
   auto launch_tick = [&]() -> int {
     for (size_t gi = 0; gi < launches.size(); ++gi) {
       const Launch& Lc = launches[gi];
-      Lc.fn<<<(unsigned)Lc.ncta, use_strip ? kStripThreads : cfg.threads, Lc.smem, stream>>>(
+      Lc.fn<<<(unsigned)Lc.ncta, use_strip ? strip_threads(Lc.N) : cfg.threads, Lc.smem, stream>>>(
           gdesc[gi], b->d_cta + Lc.cta0, b->d_tick, cfg.tile_ex, cfg.tile_ez);
     }
     tick_advance_kernel<<<1, 1, 0, stream>>>(b->d_tick);
