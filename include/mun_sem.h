@@ -125,6 +125,29 @@ int sem_forward_adjoint(sem_batch_t* batch, const sem_plan_t* plan, const double
                         int32_t ckpt_k, float* clean_out, double* loglik_out,
                         double* grad_out, void* stream);
 
+/* Allocation-free forward solve (receivers in the run() convention), for callers that
+ * cannot allocate device memory while they run: a caller inside a memory pool that owns
+ * the whole device, a real-time loop that must not hit cudaMalloc's implicit device
+ * synchronisation, or an embedding whose allocator is not the CUDA runtime's.
+ * No counterpart in the reference (MUN allocates its history with torch on every call).
+ *
+ * It uses a fixed 32 MiB scratch array that lives in this library's device image, so it
+ * calls no cudaMalloc/cudaFree and nothing that allocates.  Every GPU that loads the
+ * library holds that array until the process exits.  The plan must already exist
+ * (sem_plan_create allocates; do it at set-up).  Limit: 4 float fields of
+ * pitch x (nelz*npol+1) floats (pitch = nxg rounded up to 32) plus the tile map and
+ * receiver sums must fit in 32 MiB, about 1.9 million mesh nodes; larger meshes
+ * return SEM_ERR_ARG with the required size in sem_last_error().
+ *
+ * The first call on a device looks up the array's device address
+ * (cudaGetSymbolAddress) with that device current; make that first call before any
+ * stream capture.  All calls share the one array and it keeps the last call's
+ * contents (the call clears what must start at zero): calls that overlap on the GPU,
+ * from different streams or threads, race and give wrong results.  status_out
+ * (device, may be NULL) receives SEM_OK or SEM_ERR_NONFINITE. */
+int sem_forward_noalloc(const sem_plan_t* plan, const double* velocity, float* rec_out,
+                        int32_t* status_out, void* stream);
+
 /* last error message of the calling thread (static storage) */
 const char* sem_last_error(void);
 

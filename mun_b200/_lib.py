@@ -41,7 +41,7 @@ class LaunchCfg(C.Structure):
 EXPORTS = ["sem_plan_create", "sem_plan_destroy", "sem_plan_workspace_bytes", "sem_batch_create",
            "sem_batch_destroy", "sem_run", "sem_batch_last_launches", "sem_batch_last_kernel",
            "sem_forward",
-           "sem_forward_adjoint", "sem_last_error"]
+           "sem_forward_adjoint", "sem_forward_noalloc", "sem_last_error"]
 
 _lib = None
 
@@ -76,6 +76,7 @@ def load(path=None):
     lib.sem_batch_last_kernel.restype = i32
     lib.sem_forward.argtypes = [vp, vp, vp, vp, vp]
     lib.sem_forward_adjoint.argtypes = [vp, vp, vp, vp, dbl, i32, i32, vp, vp, vp, vp]
+    lib.sem_forward_noalloc.argtypes = [vp, vp, vp, vp, vp]
     lib.sem_last_error.restype = C.c_char_p
     for name in EXPORTS:
         if name not in ("sem_plan_workspace_bytes", "sem_batch_last_launches", "sem_batch_last_kernel",

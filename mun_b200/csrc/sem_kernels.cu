@@ -1002,6 +1002,27 @@ __global__ void copy_status_kernel(const int* __restrict__ st, int* __restrict__
   if (threadIdx.x == 0 && blockIdx.x == 0) *out = *st;
 }
 
+// ----------------------------------------------------------------------------
+// Scratch of the allocation-free forward entry point (sem_forward_noalloc).  Every
+// GPU that loads this library holds it until the process exits.  Host code must not
+// use the symbol's name as an address: it takes the device address once per device
+// with cudaGetSymbolAddress.
+// ----------------------------------------------------------------------------
+constexpr size_t kNoAllocScratchBytes = 32u << 20;  // 32 MiB
+constexpr int kNoAllocTile = 8;                      // 8x8-element tiles, 256 threads
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+
+// writes the solve descriptor (passed by value), the CTA map and the tick counter
+// into the scratch, and clears the state that must start at zero
+__global__ void noalloc_setup_kernel(SolveDev d, SolveDev* desc, int* cta, int ncta, int* tick,
+                                     float* zero_f, long long nzero_f, int* status) {
+  const long long i0 = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  if (i0 == 0) { *desc = d; *tick = 0; *status = 0; }
+  for (long long i = i0; i < ncta; i += stride) cta[i] = 0;
+  for (long long i = i0; i < nzero_f; i += stride) zero_f[i] = 0.f;
+}
+
 }  // namespace
 
 // ============================================================================
@@ -1241,6 +1262,13 @@ int sem_plan_create(const sem_plan_desc_t* d, sem_plan_t** out) {
       (rc = upload(&p->node_pos, pos.data(), pos.size()))) {
     sem_plan_destroy(p);
     return rc;
+  }
+  {
+    sem_plan_s::Lists L;  // lists of the default 8x8 tiles, used by sem_forward_noalloc
+    if ((rc = get_lists(p, kNoAllocTile, kNoAllocTile, &L))) {
+      sem_plan_destroy(p);
+      return rc;
+    }
   }
   *out = p;
   return SEM_OK;
@@ -1532,6 +1560,93 @@ int sem_run(sem_batch_t* b, const sem_solve_t* solves, int32_t n, const sem_laun
       b->last_launches++;
     }
   }
+  CUDA_TRY(cudaGetLastError());
+  return SEM_OK;
+}
+
+int sem_forward_noalloc(const sem_plan_t* p, const double* velocity, float* rec_out,
+                        int32_t* status_out, void* stream_v) {
+  if (!p || !velocity || !rec_out) return fail(SEM_ERR_ARG, "null argument");
+  cudaStream_t stream = (cudaStream_t)stream_v;
+  int dev = -1;
+  CUDA_TRY(cudaGetDevice(&dev));
+  if (dev != p->device) return fail(SEM_ERR_ARG, "plan was created on another device");
+  // device address of the scratch array, looked up once per device
+  static std::mutex mu;
+  static std::map<int, char*> base_of;
+  char* base = nullptr;
+  {
+    std::lock_guard<std::mutex> lk(mu);
+    auto it = base_of.find(dev);
+    if (it == base_of.end()) {
+      void* ptr = nullptr;
+      cudaError_t e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
+      if (e != cudaSuccess)
+        return fail(SEM_ERR_CUDA, std::string("cudaGetSymbolAddress(scratch): ") + cudaGetErrorString(e));
+      base_of[dev] = (char*)ptr;
+      base = (char*)ptr;
+    } else {
+      base = it->second;
+    }
+  }
+  // receiver lists of the default tiles were built when the plan was created
+  sem_plan_s::Lists L{};
+  {
+    std::lock_guard<std::mutex> lk(p->mu);
+    auto it = p->lists.find(std::make_pair(kNoAllocTile, kNoAllocTile));
+    if (it == p->lists.end()) return fail(SEM_ERR_ARG, "plan has no default tile lists");
+    L = it->second;
+  }
+  int ntx, ntz;
+  const int ntiles = tiles_of(p, kNoAllocTile, kNoAllocTile, &ntx, &ntz);
+  // scratch layout: descriptor | tick | CTA map | c^2 | b[2] | v | misfit block | status
+  const long long F = p->fstride * 4;
+  long long o = 0;
+  const long long o_desc = o; o += round_up(sizeof(SolveDev), 256);
+  const long long o_tick = o; o += 256;
+  const long long o_cta = o; o += round_up((long long)ntiles * 4, 256);
+  const long long o_c2 = o; o += F;
+  const long long o_W = o; o += 2 * F;
+  const long long o_V = o; o += F;
+  const long long o_mis = o; o += round_up((long long)(2 * p->nrec + 1) * 8, 256);
+  const long long o_st = o; o += 256;
+  if (o > (long long)kNoAllocScratchBytes)
+    return fail(SEM_ERR_ARG, "mesh too large for sem_forward_noalloc: needs " + std::to_string(o) +
+                                 " bytes of scratch, the limit is " + std::to_string(kNoAllocScratchBytes));
+  SolveDev d{};
+  d.nelx = p->nelx; d.nelz = p->nelz; d.nxg = p->nxg; d.nzg = p->nzg; d.pitch = p->pitch;
+  d.tiles_x = ntx; d.tiles_z = ntz; d.tile_base = 0;
+  d.nt = p->nt; d.k = 2; d.nseg = 1; d.flags = 0; d.start_tick = 0;
+  d.it0 = 0; d.it1 = p->nt; d.decim = 1;
+  d.src_gx = p->src_gx; d.src_gz = p->src_gz; d.nrec = p->nrec;
+  d.fstride = p->fstride;
+  d.c2 = (const float*)(base + o_c2);
+  d.W = (float*)(base + o_W);
+  d.V = (float*)(base + o_V);
+  d.D = p->D; d.beta = p->beta; d.tx = p->tx; d.tz = p->tz; d.src_term = p->src_term;
+  d.rec_base = p->rec_base; d.rec_w = p->rec_w;
+  d.rec_tile_off = L.rec_off; d.rec_tile_ids = L.rec_ids;
+  d.inj_tile_off = L.inj_off; d.inj_tile_ids = L.inj_ids;
+  d.rec_out = rec_out; d.yobs = nullptr;
+  d.misfit = (double*)(base + o_mis);
+  d.rmax = d.misfit + p->nrec;
+  d.adj_scale = d.misfit + 2 * p->nrec;
+  d.status = (int*)(base + o_st);
+  // b_0 = 0 and v_0 = 0: W[0] (first state) and V; the previous call left its state here
+  noalloc_setup_kernel<<<256, 256, 0, stream>>>(d, (SolveDev*)(base + o_desc), (int*)(base + o_cta), ntiles,
+                                                (int*)(base + o_tick), (float*)(base + o_W),
+                                                3 * p->fstride, (int*)(base + o_st));
+  set_c2_kernel<<<std::min(1024, (p->npoints + 255) / 256), 256, 0, stream>>>(
+      velocity, p->node_pos, (float*)(base + o_c2), p->npoints);
+  KernelFn fn = kernel_for(p->npol);
+  const size_t smem = (size_t)smem_floats(p->npol, kNoAllocTile, kNoAllocTile, false) * sizeof(float);
+  CUDA_TRY(cudaFuncSetAttribute((const void*)fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  for (int tick = 0; tick < p->nt; ++tick) {
+    fn<<<ntiles, 256, smem, stream>>>((const SolveDev*)(base + o_desc), (const int*)(base + o_cta),
+                                      (const int*)(base + o_tick), kNoAllocTile, kNoAllocTile);
+    tick_advance_kernel<<<1, 1, 0, stream>>>((int*)(base + o_tick));
+  }
+  if (status_out) copy_status_kernel<<<1, 32, 0, stream>>>((const int*)(base + o_st), status_out);
   CUDA_TRY(cudaGetLastError());
   return SEM_OK;
 }
