@@ -148,6 +148,68 @@ int sem_forward_adjoint(sem_batch_t* batch, const sem_plan_t* plan, const double
 int sem_forward_noalloc(const sem_plan_t* plan, const double* velocity, float* rec_out,
                         int32_t* status_out, void* stream);
 
+/* ---------------------------------------------------------------------------------
+ * Serving engine: continuous batching (no counterpart in the reference, whose
+ * drivers call SEMSimulation one request at a time: MCMC.py:193-208,
+ * RQS_Coupling.py:295-351).  Solves are queued with sem_engine_submit and admitted at
+ * the next tick boundary when a slot and enough device memory (the solve's workspace
+ * under memory_cap) are free; each sem_engine_step retires finished solves, admits
+ * queued ones and launches ticks_per_step ticks on the stream.  A solve's results do
+ * not depend on what runs beside it (bitwise).  One thread uses an engine at a time.
+ * ------------------------------------------------------------------------------- */
+typedef struct sem_engine_s sem_engine_t;
+typedef struct {
+  int32_t max_solves;      /* concurrent solves                                        */
+  int64_t memory_cap;      /* device bytes for solve workspaces (allocated at creation) */
+  int32_t ticks_per_step;  /* ticks launched by one sem_engine_step                    */
+  int32_t kernel;          /* 1 tile kernel, 2 strip kernel (fixed for the engine)     */
+  int32_t tile_ex, tile_ez;/* tile kernel tile size                                    */
+} sem_engine_cfg_t;
+
+int sem_engine_create(const sem_engine_cfg_t* cfg, sem_engine_t** out);
+int sem_engine_destroy(sem_engine_t* engine);
+/* queue one solve (same fields as in sem_run; its buffers must stay valid until it is
+ * released) and return a ticket */
+int sem_engine_submit(sem_engine_t* engine, const sem_solve_t* solve, int64_t* ticket);
+/* retire, admit, launch ticks_per_step ticks */
+int sem_engine_step(sem_engine_t* engine, void* stream);
+/* *state: 0 queued, 1 running, 2 done (outputs written), -1 unknown ticket */
+int sem_engine_status(sem_engine_t* engine, int64_t ticket, int32_t* state);
+/* forget a done solve */
+int sem_engine_release(sem_engine_t* engine, int64_t ticket);
+/* out[5]: queued, running, workspace bytes in use, ticks launched, kernel launches */
+int sem_engine_stats(const sem_engine_t* engine, int64_t* out);
+
+/* ---------------------------------------------------------------------------------
+ * Velocity model from a closed cubic B-spline interface (replaces
+ * build_velocity_on_sem_nodes / build_velocity_layered_with_anomaly /
+ * build_velocity_2d_background_with_anomaly: Bspline_Coupling/SEM/sem_waveform/
+ * velocity.py:37-202, layered velocity.py:38-267, gridded velocity.py:54-332).
+ * Per node: nearest curve sample, Newton refinement of the closest parameter, signed
+ * distance (even-odd sign against the sample polygon), sigmoid or hard blend.
+ * ------------------------------------------------------------------------------- */
+typedef struct {
+  int32_t ncoef;             /* coefficients of the closed curve (free points + 3)   */
+  const double* knots;       /* HOST [ncoef + 4]                                     */
+  const double* coef;        /* HOST [ncoef * 2] (x, z) pairs                        */
+  double u_lo, u_hi;         /* valid parameter interval                             */
+  int32_t nsamples;          /* initial-guess samples (<= 4096)                      */
+  const double* u0;          /* DEVICE [nsamples] sample parameters                  */
+  const double* samples;     /* DEVICE [nsamples * 2] C(u0), also the sign polygon    */
+  int32_t newton_steps;
+  double tau;                /* sigmoid width                                        */
+  double v_inside;           /* velocity inside the curve                            */
+  int32_t blend_replace;     /* 0: v_bg + (v_in - v_bg) sigmoid(-sd/tau); 1: v_in inside */
+} sem_curve_t;
+
+/* coords: DEVICE [npoints * 2]; v_background: DEVICE [npoints] or NULL (then v_outside);
+ * outputs DEVICE: velocity [npoints], optional sd [npoints], u_star [npoints],
+ * normal_out [npoints * 2] */
+int sem_velocity_from_curve(const sem_curve_t* curve, int32_t npoints, const double* coords,
+                            const double* v_background, double v_outside, double* velocity_out,
+                            double* sd_out, double* ustar_out, double* normal_out, void* stream);
+const char* sem_velocity_last_error(void);
+
 /* last error message of the calling thread (static storage) */
 const char* sem_last_error(void);
 

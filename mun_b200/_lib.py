@@ -38,10 +38,24 @@ class LaunchCfg(C.Structure):
                 ("graph_chunk", C.c_int32), ("kernel", C.c_int32)]
 
 
+class CurveDesc(C.Structure):
+    _fields_ = [("ncoef", C.c_int32), ("knots", C.POINTER(C.c_double)), ("coef", C.POINTER(C.c_double)),
+                ("u_lo", C.c_double), ("u_hi", C.c_double), ("nsamples", C.c_int32),
+                ("u0", C.c_void_p), ("samples", C.c_void_p), ("newton_steps", C.c_int32),
+                ("tau", C.c_double), ("v_inside", C.c_double), ("blend_replace", C.c_int32)]
+
+
+class EngineCfg(C.Structure):
+    _fields_ = [("max_solves", C.c_int32), ("memory_cap", C.c_int64), ("ticks_per_step", C.c_int32),
+                ("kernel", C.c_int32), ("tile_ex", C.c_int32), ("tile_ez", C.c_int32)]
+
+
 EXPORTS = ["sem_plan_create", "sem_plan_destroy", "sem_plan_workspace_bytes", "sem_batch_create",
            "sem_batch_destroy", "sem_run", "sem_batch_last_launches", "sem_batch_last_kernel",
            "sem_forward",
-           "sem_forward_adjoint", "sem_forward_noalloc", "sem_last_error"]
+           "sem_forward_adjoint", "sem_forward_noalloc", "sem_engine_create", "sem_engine_destroy",
+           "sem_engine_submit", "sem_engine_step", "sem_engine_status", "sem_engine_release",
+           "sem_engine_stats", "sem_velocity_from_curve", "sem_velocity_last_error", "sem_last_error"]
 
 _lib = None
 
@@ -77,10 +91,19 @@ def load(path=None):
     lib.sem_forward.argtypes = [vp, vp, vp, vp, vp]
     lib.sem_forward_adjoint.argtypes = [vp, vp, vp, vp, dbl, i32, i32, vp, vp, vp, vp]
     lib.sem_forward_noalloc.argtypes = [vp, vp, vp, vp, vp]
+    lib.sem_engine_create.argtypes = [C.POINTER(EngineCfg), C.POINTER(vp)]
+    lib.sem_engine_destroy.argtypes = [vp]
+    lib.sem_engine_submit.argtypes = [vp, C.POINTER(Solve), C.POINTER(i64)]
+    lib.sem_engine_step.argtypes = [vp, vp]
+    lib.sem_engine_status.argtypes = [vp, i64, C.POINTER(i32)]
+    lib.sem_engine_release.argtypes = [vp, i64]
+    lib.sem_engine_stats.argtypes = [vp, C.POINTER(i64)]
+    lib.sem_velocity_from_curve.argtypes = [C.POINTER(CurveDesc), i32, vp, vp, dbl, vp, vp, vp, vp, vp]
+    lib.sem_velocity_last_error.restype = C.c_char_p
     lib.sem_last_error.restype = C.c_char_p
     for name in EXPORTS:
         if name not in ("sem_plan_workspace_bytes", "sem_batch_last_launches", "sem_batch_last_kernel",
-                        "sem_last_error"):
+                        "sem_last_error", "sem_velocity_last_error"):
             getattr(lib, name).restype = C.c_int
     _lib = lib
     return lib

@@ -1,0 +1,96 @@
+"""Launch-configuration autotuner.
+
+Picks the kernel variant (tile kernel with a tile shape, or strip kernel), the CUDA-graph
+chunk and the checkpoint interval for a batch by timing candidates on a short proxy of
+the batch: the same meshes, orders, receivers and velocities with a few dozen time steps.
+The choice is cached per batch signature (mesh sizes, orders, solve count, adjoint or
+not).  Results never depend on the choice: every variant computes bitwise the same
+numbers, so tuning only moves time.
+"""
+from __future__ import annotations
+
+import time
+
+import torch
+
+from .plan import SEMPlan
+from .solver import Batch, SolveSpec, choose_ckpt_k
+
+TILE_CANDIDATES = [(8, 8), (16, 8), (8, 4), (16, 4), (4, 4)]
+GRAPH_CANDIDATES = [0, 32]
+
+_cache = {}
+
+
+def signature(specs):
+    shapes = tuple(sorted((s.plan.nelx, s.plan.nelz, s.plan.npol) for s in specs))
+    return (shapes, len(specs), any(s.adjoint for s in specs))
+
+
+def _proxy_plan(plan, nt_proxy):
+    a = plan.arrays
+    kw = dict(plan.kwargs)
+    kw["nt"] = min(int(nt_proxy), plan.nt)
+    return SEMPlan(**kw)
+
+
+def tune(specs, nt_proxy=48, repeats=2, candidates=None, verbose=False):
+    """Return ``dict(kernel=..., tile=..., graph_chunk=..., ckpt_k=...)`` for ``specs``."""
+    key = signature(specs)
+    if key in _cache:
+        return _cache[key]
+    proxies = {}
+    for s in specs:
+        if id(s.plan) not in proxies:
+            proxies[id(s.plan)] = _proxy_plan(s.plan, nt_proxy)
+
+    def proxy_specs():
+        out = []
+        for s in specs:
+            p = proxies[id(s.plan)]
+            y = None if s.y_obs is None else s.y_obs[:p.nt]
+            out.append(SolveSpec(p, s.velocity, adjoint=s.adjoint, exact=s.exact, shift=s.shift,
+                                 misfit=s.misfit, y_obs=y, inv_sigma2=s.inv_sigma2, ckpt_k=p.nt))
+        return out
+
+    cands = candidates or ([(1, t, g) for t in TILE_CANDIDATES for g in GRAPH_CANDIDATES]
+                           + [(2, (0, 0), g) for g in GRAPH_CANDIDATES])
+    best, best_t = None, float("inf")
+    stream = torch.cuda.Stream()
+    for kernel, tile, chunk in cands:
+        b = Batch(tile=tile if kernel == 1 else (8, 8), graph_chunk=chunk, kernel=kernel)
+        try:
+            with torch.cuda.stream(stream):
+                b.run(proxy_specs())  # warm-up (plan lists, graph instantiation)
+            stream.synchronize()
+            times = []
+            for _ in range(repeats):
+                sp = proxy_specs()
+                t0 = time.perf_counter()
+                with torch.cuda.stream(stream):
+                    b.run(sp)
+                stream.synchronize()
+                times.append(time.perf_counter() - t0)
+            el = min(times)
+        except (ValueError, RuntimeError):
+            continue
+        if verbose:
+            print(f"kernel={kernel} tile={tile} graph_chunk={chunk}: {1e3 * el:.2f} ms")
+        if el < best_t:
+            best_t, best = el, (kernel, tile, chunk)
+    kernel, tile, chunk = best
+    k = choose_ckpt_k(specs[0].plan, len(specs)) if any(s.adjoint for s in specs) else 2
+    res = {"kernel": kernel, "tile": tile, "graph_chunk": chunk, "ckpt_k": k, "proxy_ms": 1e3 * best_t}
+    _cache[key] = res
+    return res
+
+
+def tuned_batch(specs, **kw):
+    """A ``Batch`` configured by ``tune`` plus the chosen checkpoint interval applied to
+    the specs."""
+    cfg = tune(specs, **kw)
+    for s in specs:
+        if s.adjoint and not s.ckpt_k:
+            s.ckpt_k = cfg["ckpt_k"]
+    return Batch(tile=cfg["tile"] if cfg["kernel"] == 1 else (8, 8), graph_chunk=cfg["graph_chunk"],
+                 kernel=cfg["kernel"]), cfg

@@ -6,7 +6,7 @@ import subprocess
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 SO = os.path.join(HERE, "_sem.so")
-SOURCES = [os.path.join(HERE, "csrc", "sem_kernels.cu")]
+SOURCES = [os.path.join(HERE, "csrc", "sem_kernels.cu"), os.path.join(HERE, "csrc", "sem_velocity.cu")]
 HEADERS = [os.path.join(ROOT, "include", "mun_sem.h")]
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3", "-std=c++17",
               "-shared", "-Xcompiler", "-fPIC", "-Xptxas", "-v"]

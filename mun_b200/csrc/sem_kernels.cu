@@ -43,6 +43,7 @@
 #include <string.h>
 
 #include <algorithm>
+#include <deque>
 #include <map>
 #include <mutex>
 #include <string>
@@ -537,22 +538,24 @@ __global__ void __launch_bounds__(256) sem_tick_kernel(const SolveDev* __restric
 // strip kernel: one CTA per full-height strip of element columns (large batches)
 //
 // Columns: N left-halo columns, the strip's owned columns and the shared column on its
-// right (kStripCols threads per band row).  The CTA sweeps the strip one element row
-// ("band", N+1 grid rows) at a time; each band of every field the step reads is
-// staged by TMA bulk copies (cp.async.bulk + mbarrier) into a ring of kStages slots,
-// issued kStages bands ahead.  One thread per (band row, column): phase A forms the
-// per-node fluxes beta c^2 (D u) of the x-line and z-line segments through the node,
-// phase B contracts them with D^T and advances the node.  Both directions use the
-// same arithmetic order as the tile kernel (bitwise-equal results).
+// right.  The CTA sweeps the strip one element row ("band", N+1 grid rows) at a time;
+// the band of every field the step reads is staged by TMA bulk copies (cp.async.bulk +
+// mbarrier) into a ring of slots, issued as many bands ahead as there are slots (3 for
+// forward/replay ticks, 2 for the larger adjoint bands so that four CTAs fit per SM).
+// Work per band: one thread per (band row, element segment) for the x-lines, one thread
+// per owned column for the z-line segment of the band, D and beta in registers; then
+// one thread per owned column combines the segment results and advances the band's
+// nodes.  Arithmetic order matches the tile kernel (bitwise-equal results).
 // ----------------------------------------------------------------------------
 constexpr int kStripCols = 128;
-constexpr int kStages = 3;
+constexpr int kStages = 3;        // ring slots of forward/replay ticks
+constexpr int kStagesAdj = 2;     // ring slots of adjoint ticks (bigger bands)
 constexpr int kStripInj = 256;               // receivers per band of one strip (host-checked)
 constexpr long long kWaitNs = 2000000000LL;  // bounded mbarrier waits: 2 s
 
 __host__ __device__ inline int strip_ew_max(int N) { return (kStripCols - N - 1) / N; }
 __host__ __device__ inline int strip_bw(int N) { return (kStripCols + 3 + 3) & ~3; }  // smem row
-__host__ __device__ inline int strip_threads(int N) { return N * kStripCols; }
+__host__ __device__ inline int strip_threads(int N) { return kStripCols; }
 
 __device__ __forceinline__ uint32_t smem_addr(const void* p) {
   return (uint32_t)__cvta_generic_to_shared(p);
@@ -602,26 +605,29 @@ __host__ __device__ inline long long strip_stage_floats(int N, bool adj) {
   const int ndouble = adj ? 1 : 0;  // gradient accumulator
   return ((long long)(nfloat + 2 * ndouble) * (N + 1) * strip_bw(N) + 31) & ~31LL;
 }
-// exchange arrays: Qr, Ql (x) and Qz (z) fluxes [+ Sr, Sl, Sz], z carries, injection rows
+// exchange arrays: x-segment results Xs[rows][segments][N+1] (+ sensitivity), z-segment
+// results Zs[N+1][cols] (+ sensitivity), injection rows and residuals
 __host__ __device__ inline long long strip_xch_floats(int N, bool adj) {
-  const long long row = kStripCols;
-  long long f = 3LL * (N + 1) * row + 2 * row;                    // Qr Ql Qz | zcarry[2]
-  if (adj) f += 3LL * (N + 1) * row + 2 * row + (N + 1) * row + kStripInj;  // S | scarry | inj
+  const long long NP = N + 1, segs = strip_ew_max(N) + 1;
+  long long f = NP * segs * NP + NP * kStripCols;                    // Xs | Zs
+  if (adj) f += NP * segs * NP + NP * kStripCols + NP * kStripCols + kStripInj;  // SXs | SZs | inj | res
   return (f + 31) & ~31LL;
 }
 __host__ __device__ inline long long strip_smem_floats(int N, bool adj) {
-  return 64 + 96 + kStages * strip_stage_floats(N, adj) + strip_xch_floats(N, adj);
+  const long long fwd = kStages * strip_stage_floats(N, false) + strip_xch_floats(N, false);
+  const long long adjf = kStagesAdj * strip_stage_floats(N, true) + strip_xch_floats(N, true);
+  return 64 + 96 + (adj ? (fwd > adjf ? fwd : adjf) : fwd);
 }
 
 template <int N>
-__global__ void __launch_bounds__(N * kStripCols) sem_strip_kernel(const SolveDev* __restrict__ solves,
-                                                                   const int* __restrict__ cta_solve,
-                                                                   const int* __restrict__ tick_ptr,
-                                                                   int unused0, int unused1) {
+__global__ void __launch_bounds__(kStripCols) sem_strip_kernel(const SolveDev* __restrict__ solves,
+                                                               const int* __restrict__ cta_solve,
+                                                               const int* __restrict__ tick_ptr,
+                                                               int unused0, int unused1) {
   constexpr int NP = N + 1;
   constexpr int BW = (kStripCols + 3 + 3) & ~3;
-  constexpr int NT = N * kStripCols;
-  constexpr int R = kStripCols;  // row stride of the exchange arrays
+  constexpr int NT = kStripCols;
+  constexpr int SEGS = (kStripCols - N - 1) / N + 1;  // x-segments per band row (max)
   extern __shared__ __align__(128) float smem[];
   __shared__ SolveDev S;
   __shared__ int s_act, s_t, s_seg, s_abort;
@@ -659,34 +665,30 @@ __global__ void __launch_bounds__(N * kStripCols) sem_strip_kernel(const SolveDe
   const int e0 = strip * EW, e1 = min(e0 + EW, S.nelx);
   const int sx0 = e0 * N;                                   // first owned column
   const int so1 = (e1 == S.nelx) ? S.nxg : e1 * N;          // owned columns [sx0, so1)
-  const int NC = (e1 - e0) * N + N + 1;                     // columns in use
   const int X0 = (sx0 - N) & ~3;                            // 16-byte aligned copy origin
-  const int off = (sx0 - N) - X0;
+  const int off = (sx0 - N) - X0;                           // smem column of column sx0 - N
   const int cs = max(X0, 0), ce = min(X0 + BW, S.pitch);    // copied columns
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const int col = tid % R, row = tid / R;                   // this thread's column and band row
-  const int gx = sx0 - N + col;
-  const bool col_valid = col < NC && gx >= 0 && gx < S.nxg;
-  const bool owned = col_valid && gx >= sx0 && gx < so1;
-  const int sc = col + off;
+  const int nseg = e1 - e0 + 1;                             // segments e0-1 .. e1-1
+  const int seg0 = (e0 == 0) ? 1 : 0;                       // segment -1 does not exist
+  const int gx = sx0 + tid;                                 // this thread's owned column
+  const bool owned = gx < so1;
+  const int sc = tid + N + off;                             // its smem column
 
   // ---------------- shared memory
   unsigned long long* bars = reinterpret_cast<unsigned long long*>(smem);
   float* sD = smem + 64;
   float* sB = sD + 64;
   const int nfloat = (adj ? 4 : 3), ndouble = (adj ? 1 : 0);
-  const long long stage_f = strip_stage_floats(N, adj || final_only ? adj : false);
+  const long long stage_f = strip_stage_floats(N, adj);
+  const int nst = adj ? kStagesAdj : kStages;    // ring slots
   float* stages = smem + 64 + 96;
-  float* Qr = stages + kStages * stage_f;  // [NP][R]
-  float* Ql = Qr + NP * R;                 // [NP][R]
-  float* Qz = Ql + NP * R;                 // [NP][R]
-  float* zcar = Qz + NP * R;               // [2][R]
-  float* Sr = zcar + 2 * R;                // adjoint: [NP][R] x3, [2][R]
-  float* Sl = Sr + NP * R;
-  float* Sz = Sl + NP * R;
-  float* scar = Sz + NP * R;
-  float* sacc = scar + 2 * R;              // [NP][R]
-  float* sres = sacc + NP * R;             // [kStripInj]
+  float* Xs = stages + nst * stage_f;            // [NP][SEGS][NP]
+  float* Zs = Xs + NP * SEGS * NP;                // [NP][NT]
+  float* SXs = Zs + NP * NT;                      // adjoint: [NP][SEGS][NP]
+  float* SZs = SXs + NP * SEGS * NP;              // [NP][NT]
+  float* sacc = SZs + NP * NT;                    // [NP][NT]
+  float* sres = sacc + NP * NT;                   // [kStripInj]
 
   // ---------------- which fields
   const float* cur;
@@ -712,62 +714,76 @@ __global__ void __launch_bounds__(N * kStripCols) sem_strip_kernel(const SolveDe
   const int nload = final_only ? 1 : nfloat;
 
   if (tid == 0) {
-    for (int s = 0; s < kStages; ++s) mbar_init(bars + s, 1);
+    for (int s2 = 0; s2 < nst; ++s2) mbar_init(bars + s2, 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   for (int i = tid; i < NP * NP; i += NT) sD[i] = S.D[i];
   for (int i = tid; i < NP; i += NT) sB[i] = S.beta[i];
   __syncthreads();
 
-  // TMA: element row `ez` of every field into ring slot ez % kStages
+  // TMA: element row `ez` of every field into ring slot ez % nst (warp 0: lane 0
+  // posts the expected bytes, then each lane issues row copies)
   auto issue = [&](int ez) {
-    const int slot = ez % kStages;
+    const int slot = ez % nst;
     float* st = stages + slot * stage_f;
     const unsigned rowb = (unsigned)(ce - cs) * 4u;
-    const unsigned total = (unsigned)nload * NP * rowb +
-                           (final_only ? 0u : (unsigned)ndouble * NP * rowb * 2u);
-    mbar_expect_tx(bars + slot, total);
-    for (int f = 0; f < nload; ++f) {
-      const float* base = (f == 0) ? cur : (f == 1) ? S.c2 : (f == 2) ? vin : fwdu;
-      for (int a = 0; a < NP; ++a)
+    const int nd = (ndouble && !final_only) ? NP : 0;
+    const int ncopy = nload * NP + nd;
+    if (lane == 0) mbar_expect_tx(bars + slot, (unsigned)(nload * NP) * rowb + (unsigned)nd * rowb * 2u);
+    __syncwarp();
+    for (int q = lane; q < ncopy; q += 32) {
+      if (q < nload * NP) {
+        const int f = q / NP, a = q - f * NP;
+        const float* base = (f == 0) ? cur : (f == 1) ? S.c2 : (f == 2) ? vin : fwdu;
         bulk_load(st + (f * NP + a) * BW + (cs - X0), base + (long long)(ez * N + a) * S.pitch + cs,
                   rowb, bars + slot);
-    }
-    if (ndouble && !final_only) {
-      double* gs = reinterpret_cast<double*>(st + nfloat * NP * BW);
-      for (int a = 0; a < NP; ++a)
+      } else {
+        const int a = q - nload * NP;
+        double* gs = reinterpret_cast<double*>(st + nfloat * NP * BW);
         bulk_load(gs + a * BW + (cs - X0), S.grad + (long long)(ez * N + a) * S.pitch + cs,
                   rowb * 2u, bars + slot);
+      }
     }
   };
-  if (tid == 0)
-    for (int ez = 0; ez < min(kStages, S.nelz); ++ez) issue(ez);
+  if (warp == 0)
+    for (int ez = 0; ez < min(nst, S.nelz); ++ez) issue(ez);
 
+  // D and beta in registers (uniform across threads)
+  float Dr[NP][NP], Bt[NP];
+#pragma unroll
+  for (int a = 0; a < NP; ++a) {
+    Bt[a] = sB[a];
+#pragma unroll
+    for (int b = 0; b < NP; ++b) Dr[a][b] = sD[a * NP + b];
+  }
   float ixv = 0.f, Rxv = 0.f, dxv = 0.f;
   if (owned) { ixv = __ldg(S.tx + gx); Rxv = __ldg(S.tx + S.nxg + gx); dxv = __ldg(S.tx + 2 * S.nxg + gx); }
-  const int e_r = col_valid ? gx / N : 0, ia = col_valid ? gx - e_r * N : 0;
+  const int e_r = gx / N, ia = gx - e_r * N;
+  const int s_r = e_r - e0 + 1;                 // x-segment index of this column's right segment
   const bool damp = (act != A_ADJ) || (S.flags & F_EXACT);
   const bool grad_on = adj && t >= S.it0 && t < S.it1;
   const bool in_win = adj && t >= S.it0 && t < S.it1 && ((t - S.it0) % S.decim) == 0;
   const int ms = t - ((S.flags & F_SHIFT) ? 1 : 0);
   const bool rec_on = (act == A_FWD || act == A_FINAL) && ms >= 0 && ms < S.nt;
   if (adj && in_win)
-    for (int i = tid; i < NP * R; i += NT) sacc[i] = 0.f;
+    for (int i = tid; i < NP * NT; i += NT) sacc[i] = 0.f;
+  float zc = 0.f, szc = 0.f;  // z-line carries into the next band's first row
   bool bad = false;
   int abort_ez = -1;
 
   for (int ez = 0; ez < S.nelz; ++ez) {
-    const int slot = ez % kStages;
+    const int slot = ez % nst;
     const float* st = stages + slot * stage_f;
     const float* Bs = st;
     const float* Cs = st + NP * BW;
     const float* Vs = st + 2 * NP * BW;
     const float* Us = st + 3 * NP * BW;
     const double* Gs = reinterpret_cast<const double*>(st + nfloat * NP * BW);
-    if (!mbar_wait(bars + slot, (unsigned)((ez / kStages) & 1))) s_abort = 1;
+    if (!mbar_wait(bars + slot, (unsigned)((ez / nst) & 1))) s_abort = 1;
     __syncthreads();
     if (s_abort) { abort_ez = ez; break; }
-    const bool last = (ez == S.nelz - 1);  // the last band also owns the bottom grid row
+    const bool last = (ez == S.nelz - 1);
+    const int rows = last ? NP : N;
 
     if (rec_on) {  // receivers read out of this band, one warp each
       const int li = strip * S.nelz + ez;
@@ -815,120 +831,116 @@ __global__ void __launch_bounds__(N * kStripCols) sem_strip_kernel(const SolveDe
               for (int e = lane; e < NP * NP; e += 32) {
                 const int j = e / NP, i = e - j * NP;
                 const int gxx = bx + i;
-                if (gxx >= sx0 && gxx < so1) sacc[j * R + (gxx - (sx0 - N))] += wr[e] * rs;
+                if (gxx >= sx0 && gxx < so1) sacc[j * NT + (gxx - sx0)] += wr[e] * rs;
               }
               __syncwarp();
             }
           }
         }
       }
-      // ---- phase A: fluxes at (row, col); rows handled: row, and row N (row 0 threads)
-      if (col_valid) {
-        for (int a = row; a < NP; a += N) {
-          if (a < N || last) {  // x-line fluxes are needed for output rows only
-            const float* br = Bs + a * BW;
-            if (e_r < S.nelx && col < NC - 1) {
-              const float* ub = br + sc - ia;
-              float v = 0.f;
+      // ---- phase A, x-lines: one thread per (band row, element segment)
+      for (int w = tid; w < rows * nseg; w += NT) {
+        const int a = w / nseg, sgi = w - a * nseg;
+        if (sgi < seg0) continue;
+        const float* ub = Bs + a * BW + off + sgi * N;  // column (e0-1+sgi)*N
+        const float* cb = Cs + a * BW + off + sgi * N;
+        float u[NP], du[NP], q[NP];
 #pragma unroll
-              for (int b = 0; b < NP; ++b) v = fmaf(sD[ia * NP + b], ub[b], v);
-              Qr[a * R + col] = sB[ia] * Cs[a * BW + sc] * v;
-              if (adj) {
-                const float* wb = Us + a * BW + sc - ia;
-                float dw = 0.f;
+        for (int b = 0; b < NP; ++b) u[b] = ub[b];
 #pragma unroll
-                for (int b = 0; b < NP; ++b) dw = fmaf(sD[ia * NP + b], wb[b], dw);
-                Sr[a * R + col] = sB[ia] * dw * v;
-              }
-            }
-            if (ia == 0 && e_r >= 1 && col >= N) {
-              const float* ub = br + sc - N;
-              float v = 0.f;
+        for (int a2 = 0; a2 < NP; ++a2) {
+          float v = 0.f;
 #pragma unroll
-              for (int b = 0; b < NP; ++b) v = fmaf(sD[N * NP + b], ub[b], v);
-              Ql[a * R + col] = sB[N] * Cs[a * BW + sc] * v;
-              if (adj) {
-                const float* wb = Us + a * BW + sc - N;
-                float dw = 0.f;
+          for (int b = 0; b < NP; ++b) v = fmaf(Dr[a2][b], u[b], v);
+          du[a2] = v;
+          q[a2] = Bt[a2] * cb[a2] * v;
+        }
+        float* xo = Xs + (a * SEGS + sgi) * NP;
 #pragma unroll
-                for (int b = 0; b < NP; ++b) dw = fmaf(sD[N * NP + b], wb[b], dw);
-                Sl[a * R + col] = sB[N] * dw * v;
-              }
-            }
-          }
-          if (owned) {  // z-line flux at band point a
+        for (int i = 0; i < NP; ++i) {
+          float v = 0.f;
+#pragma unroll
+          for (int a2 = 0; a2 < NP; ++a2) v = fmaf(Dr[a2][i], q[a2], v);
+          xo[i] = v;
+        }
+        if (adj) {
+          const float* wb = Us + a * BW + off + sgi * N;
+#pragma unroll
+          for (int b = 0; b < NP; ++b) u[b] = wb[b];
+          float* so = SXs + (a * SEGS + sgi) * NP;
+#pragma unroll
+          for (int a2 = 0; a2 < NP; ++a2) {
             float v = 0.f;
 #pragma unroll
-            for (int b = 0; b < NP; ++b) v = fmaf(sD[a * NP + b], Bs[b * BW + sc], v);
-            Qz[a * R + col] = sB[a] * Cs[a * BW + sc] * v;
-            if (adj) {
-              float dw = 0.f;
+            for (int b = 0; b < NP; ++b) v = fmaf(Dr[a2][b], u[b], v);
+            so[a2] = Bt[a2] * v * du[a2];
+          }
+        }
+      }
+      // ---- phase A, z-lines: one thread per owned column (the band is the segment)
+      float rz[NP], sz[NP];
+      if (owned) {
+        float u[NP], du[NP], q[NP];
 #pragma unroll
-              for (int b = 0; b < NP; ++b) dw = fmaf(sD[a * NP + b], Us[b * BW + sc], dw);
-              Sz[a * R + col] = sB[a] * dw * v;
-            }
+        for (int b = 0; b < NP; ++b) u[b] = Bs[b * BW + sc];
+#pragma unroll
+        for (int a2 = 0; a2 < NP; ++a2) {
+          float v = 0.f;
+#pragma unroll
+          for (int b = 0; b < NP; ++b) v = fmaf(Dr[a2][b], u[b], v);
+          du[a2] = v;
+          q[a2] = Bt[a2] * Cs[a2 * BW + sc] * v;
+        }
+#pragma unroll
+        for (int j = 0; j < NP; ++j) {
+          float v = 0.f;
+#pragma unroll
+          for (int a2 = 0; a2 < NP; ++a2) v = fmaf(Dr[a2][j], q[a2], v);
+          rz[j] = v;
+        }
+        if (adj) {
+#pragma unroll
+          for (int b = 0; b < NP; ++b) u[b] = Us[b * BW + sc];
+#pragma unroll
+          for (int a2 = 0; a2 < NP; ++a2) {
+            float v = 0.f;
+#pragma unroll
+            for (int b = 0; b < NP; ++b) v = fmaf(Dr[a2][b], u[b], v);
+            sz[a2] = Bt[a2] * v * du[a2];
           }
         }
       }
       __syncthreads();
-      // ---- phase B: contract, combine, advance the node
+      // ---- phase B: combine and advance the owned nodes of the band, row by row
       if (owned) {
-        const float* cin = zcar + (ez & 1) * R;
-        float* cnext = zcar + ((ez + 1) & 1) * R;
-        const float* sin_ = scar + (ez & 1) * R;
-        float* snext = scar + ((ez + 1) & 1) * R;
-        for (int a = row; a < (last ? NP : N); a += N) {
-          const int aq = a;
-          const float* qr = Qr + aq * R;
-          const float* ql = Ql + aq * R;
-          const int cl = col - ia;
+#pragma unroll
+        for (int a = 0; a < NP; ++a) {
+          if (a == N && !last) break;
+          const float* xr = Xs + a * SEGS * NP;
           float X, SX = 0.f;
           if (ia) {
-            float v = 0.f;
-#pragma unroll
-            for (int p = 0; p < N; ++p) v = fmaf(sD[p * NP + ia], qr[cl + p], v);
-            X = fmaf(sD[N * NP + ia], ql[cl + N], v);
-            if (adj) SX = Sr[aq * R + col];
+            X = xr[s_r * NP + ia];
+            if (adj) SX = SXs[a * SEGS * NP + s_r * NP + ia];
           } else {
             X = 0.f;
             if (e_r >= 1) {
-              float v = 0.f;
-#pragma unroll
-              for (int p = 0; p < N; ++p) v = fmaf(sD[p * NP + N], qr[col - N + p], v);
-              X = fmaf(sD[N * NP + N], ql[col], v);
-              if (adj) SX = Sl[aq * R + col];
+              X = xr[(s_r - 1) * NP + N];
+              if (adj) SX = SXs[a * SEGS * NP + (s_r - 1) * NP + N];
             }
             if (e_r < S.nelx) {
-              float v = 0.f;
-#pragma unroll
-              for (int p = 0; p < N; ++p) v = fmaf(sD[p * NP + 0], qr[col + p], v);
-              X += fmaf(sD[N * NP + 0], ql[col + N], v);
-              if (adj) SX += Sr[aq * R + col];
+              X += xr[s_r * NP];
+              if (adj) SX += SXs[a * SEGS * NP + s_r * NP];
             }
           }
           float Z, SZ = 0.f;
-          if (a < N) {
-            float v = 0.f;
-#pragma unroll
-            for (int p = 0; p < NP; ++p) v = fmaf(sD[p * NP + a], Qz[p * R + col], v);
-            if (a == 0) {
-              Z = 0.f;
-              if (ez >= 1) Z = cin[col];
-              Z += v;
-              if (adj) { SZ = 0.f; if (ez >= 1) SZ = sin_[col]; SZ += Sz[col]; }
-              // carry of this element's last point into the next band's first row
-              float w = 0.f;
-#pragma unroll
-              for (int p = 0; p < NP; ++p) w = fmaf(sD[p * NP + N], Qz[p * R + col], w);
-              cnext[col] = w;
-              if (adj) snext[col] = Sz[N * R + col];
-            } else {
-              Z = v;
-              if (adj) SZ = Sz[a * R + col];
-            }
-          } else {  // bottom row of the mesh: only the element above
-            Z = cnext[col];
-            if (adj) SZ = snext[col];
+          if (a == 0) {
+            Z = 0.f;
+            if (ez >= 1) Z = zc;
+            Z += rz[0];
+            if (adj) { if (ez >= 1) SZ = szc; SZ += sz[0]; }
+          } else {
+            Z = rz[a];
+            if (adj) SZ = sz[a];
           }
           const int gz = ez * N + a;
           const float izv = __ldg(S.tz + gz), Rzv = __ldg(S.tz + S.nzg + gz), dzv = __ldg(S.tz + 2 * S.nzg + gz);
@@ -937,7 +949,7 @@ __global__ void __launch_bounds__(N * kStripCols) sem_strip_kernel(const SolveDe
           if (!adj) {
             if (gx == S.src_gx && gz == S.src_gz) extra = S.src_term[t];
           } else {
-            extra = in_win ? sacc[a * R + col] : 0.f;
+            extra = in_win ? sacc[a * NT + tid] : 0.f;
             if (grad_on) S.grad[g] = Gs[a * BW + sc] + (double)(Rzv * SX + Rxv * SZ);
           }
           float res, vres;
@@ -947,21 +959,23 @@ __global__ void __launch_bounds__(N * kStripCols) sem_strip_kernel(const SolveDe
           vout[g] = vres;
           bad |= !isfinite(res);
         }
+        zc = rz[N];
+        if (adj) szc = sz[N];
+        if (adj && in_win) {  // carry the injection row shared with the next band
+          const float carry = sacc[N * NT + tid];
+#pragma unroll
+          for (int a = 1; a < NP; ++a) sacc[a * NT + tid] = 0.f;
+          sacc[tid] = carry;
+        }
       }
     }
-    __syncthreads();  // done with this slot, the flux arrays and the injection rows
-    if (adj && in_win && !final_only && row == 0) {  // carry the injection row shared with the next band
-      const float carry = sacc[N * R + col];
-      for (int a = 1; a < NP; ++a) sacc[a * R + col] = 0.f;
-      sacc[col] = carry;
-    }
-    if (tid == 0 && ez + kStages < S.nelz) issue(ez + kStages);
-    if (adj && in_win) __syncthreads();
+    __syncthreads();  // done with this slot and the exchange arrays
+    if (warp == 0 && ez + nst < S.nelz) issue(ez + nst);
   }
   if (abort_ez >= 0) {
     if (tid == 0) atomicOr(S.status, SEM_ERR_TIMEOUT);
-    for (int b = abort_ez; b < min(abort_ez + kStages, S.nelz); ++b)
-      mbar_wait(bars + b % kStages, (unsigned)((b / kStages) & 1));
+    for (int b = abort_ez; b < min(abort_ez + nst, S.nelz); ++b)
+      mbar_wait(bars + b % nst, (unsigned)((b / nst) & 1));
     return;
   }
   if (__any_sync(0xffffffffu, bad) && lane == 0) atomicOr(S.status, SEM_ERR_NONFINITE);
@@ -1670,6 +1684,339 @@ int sem_forward_adjoint(sem_batch_t* b, const sem_plan_t* plan, const double* ve
   s.ckpt_k = ckpt_k; s.y_obs = y_obs; s.it0 = 0; s.it1 = plan->nt; s.decim = 1;
   s.inv_sigma2 = inv_sigma2; s.rec_out = clean_out; s.loglik_out = loglik_out; s.grad_out = grad_out;
   return sem_run(b, &s, 1, nullptr, stream);
+}
+
+}  // extern "C"
+
+// ============================================================================
+// serving engine: continuous batching over the tick program
+// ============================================================================
+struct EngineJob {
+  sem_solve_t s{};
+  int64_t ticket = 0;
+  int k = 2, nseg = 1, prog = 0, ntiles = 0, state = 0;  // 0 queued, 1 running, 2 retired
+  long long start = 0, off = -1;
+  Workspace ws{};
+  cudaEvent_t ev = nullptr;
+};
+
+struct sem_engine_s {
+  sem_engine_cfg_t cfg{};
+  int device = -1;
+  char* arena = nullptr;
+  long long arena_bytes = 0;
+  std::map<long long, long long> free_;  // offset -> size (first fit, coalesced)
+  long long in_use = 0;
+  int* d_tick = nullptr;
+  long long tick = 0;
+  SolveDev* d_solves = nullptr;
+  int solves_cap = 0;
+  int* d_cta = nullptr;
+  long long cta_cap = 0;
+  std::deque<EngineJob*> queue;
+  std::vector<EngineJob*> running;
+  std::map<int64_t, EngineJob*> jobs;
+  int64_t next_ticket = 1;
+  long long launches = 0;
+  std::vector<SolveDev> h_solves;
+  std::vector<int> h_cta;
+};
+
+namespace {
+
+long long arena_alloc(sem_engine_s* e, long long bytes) {
+  bytes = round_up(bytes, 256);
+  for (auto it = e->free_.begin(); it != e->free_.end(); ++it) {
+    if (it->second >= bytes) {
+      const long long off = it->first, rest = it->second - bytes;
+      e->free_.erase(it);
+      if (rest > 0) e->free_[off + bytes] = rest;
+      e->in_use += bytes;
+      return off;
+    }
+  }
+  return -1;
+}
+
+void arena_free(sem_engine_s* e, long long off, long long bytes) {
+  bytes = round_up(bytes, 256);
+  e->in_use -= bytes;
+  auto it = e->free_.emplace(off, bytes).first;
+  auto nx = std::next(it);
+  if (nx != e->free_.end() && it->first + it->second == nx->first) {
+    it->second += nx->second;
+    e->free_.erase(nx);
+  }
+  if (it != e->free_.begin()) {
+    auto pv = std::prev(it);
+    if (pv->first + pv->second == it->first) {
+      pv->second += it->second;
+      e->free_.erase(it);
+    }
+  }
+}
+
+}  // namespace
+
+extern "C" {
+
+int sem_engine_create(const sem_engine_cfg_t* cfg, sem_engine_t** out) {
+  if (!cfg || !out) return fail(SEM_ERR_ARG, "null argument");
+  if (cfg->max_solves < 1 || cfg->memory_cap < (1 << 20) || cfg->ticks_per_step < 1 ||
+      cfg->kernel < 1 || cfg->kernel > 2 || cfg->tile_ex < 1 || cfg->tile_ez < 1)
+    return fail(SEM_ERR_ARG, "bad engine configuration");
+  auto* e = new sem_engine_s();
+  e->cfg = *cfg;
+  cudaGetDevice(&e->device);
+  cudaError_t err = cudaMalloc((void**)&e->arena, cfg->memory_cap);
+  if (err != cudaSuccess) {
+    delete e;
+    return fail(SEM_ERR_OOM, std::string("engine arena: ") + cudaGetErrorString(err));
+  }
+  e->arena_bytes = cfg->memory_cap;
+  e->free_[0] = cfg->memory_cap;
+  if (cudaMalloc((void**)&e->d_tick, 256) != cudaSuccess ||
+      cudaMemset(e->d_tick, 0, sizeof(int)) != cudaSuccess) {
+    cudaFree(e->arena);
+    delete e;
+    return fail(SEM_ERR_OOM, "engine tick counter");
+  }
+  *out = e;
+  return SEM_OK;
+}
+
+int sem_engine_destroy(sem_engine_t* e) {
+  if (!e) return SEM_OK;
+  cudaDeviceSynchronize();
+  for (auto& kv : e->jobs) {
+    if (kv.second->ev) cudaEventDestroy(kv.second->ev);
+    delete kv.second;
+  }
+  cudaFree(e->arena); cudaFree(e->d_tick); cudaFree(e->d_solves); cudaFree(e->d_cta);
+  delete e;
+  return SEM_OK;
+}
+
+int sem_engine_submit(sem_engine_t* e, const sem_solve_t* s, int64_t* ticket) {
+  if (!e || !s || !ticket) return fail(SEM_ERR_ARG, "null argument");
+  if (!s->plan || !s->velocity || !s->rec_out) return fail(SEM_ERR_ARG, "solve missing plan/velocity/rec_out");
+  const bool adj = s->flags & SEM_F_ADJOINT;
+  if (adj && !(s->flags & SEM_F_SHIFT)) return fail(SEM_ERR_ARG, "adjoint requires the shifted receiver convention");
+  if ((adj || (s->flags & SEM_F_MISFIT)) && !s->y_obs) return fail(SEM_ERR_ARG, "y_obs required");
+  if (s->decim < 1 || s->it0 < 0 || s->it1 > s->plan->nt || s->it0 >= s->it1)
+    return fail(SEM_ERR_ARG, "bad misfit window");
+  if (s->plan->device != e->device) return fail(SEM_ERR_ARG, "plan and engine on different devices");
+  auto* j = new EngineJob();
+  j->s = *s;
+  j->ticket = e->next_ticket++;
+  j->k = adj ? std::max(2, std::min((int)s->ckpt_k, s->plan->nt)) : 2;
+  j->ws = layout(s->plan, s->flags, j->k, &j->nseg);
+  if (j->ws.bytes > e->arena_bytes) {
+    delete j;
+    return fail(SEM_ERR_ARG, "solve needs more device memory than the engine's cap");
+  }
+  const int nt = s->plan->nt;
+  j->prog = nt + ((s->flags & SEM_F_SHIFT) ? 1 : 0) + (adj ? 1 + nt + j->k * (j->nseg - 1) : 0);
+  e->queue.push_back(j);
+  e->jobs[j->ticket] = j;
+  *ticket = j->ticket;
+  return SEM_OK;
+}
+
+int sem_engine_status(sem_engine_t* e, int64_t ticket, int32_t* state) {
+  if (!e || !state) return fail(SEM_ERR_ARG, "null argument");
+  auto it = e->jobs.find(ticket);
+  if (it == e->jobs.end()) { *state = -1; return SEM_OK; }
+  EngineJob* j = it->second;
+  if (j->state < 2) { *state = j->state; return SEM_OK; }
+  const cudaError_t q = cudaEventQuery(j->ev);
+  if (q == cudaErrorNotReady) { *state = 1; return SEM_OK; }
+  CUDA_TRY(q);
+  *state = 2;
+  return SEM_OK;
+}
+
+int sem_engine_release(sem_engine_t* e, int64_t ticket) {
+  if (!e) return fail(SEM_ERR_ARG, "null argument");
+  auto it = e->jobs.find(ticket);
+  if (it == e->jobs.end()) return SEM_OK;
+  EngineJob* j = it->second;
+  if (j->state != 2) return fail(SEM_ERR_ARG, "solve still queued or running");
+  if (j->ev) {
+    CUDA_TRY(cudaEventSynchronize(j->ev));
+    cudaEventDestroy(j->ev);
+  }
+  delete j;
+  e->jobs.erase(it);
+  return SEM_OK;
+}
+
+int sem_engine_stats(const sem_engine_t* e, int64_t* out) {
+  if (!e || !out) return fail(SEM_ERR_ARG, "null argument");
+  out[0] = (int64_t)e->queue.size();
+  out[1] = (int64_t)e->running.size();
+  out[2] = e->in_use;
+  out[3] = e->tick;
+  out[4] = e->launches;
+  return SEM_OK;
+}
+
+int sem_engine_step(sem_engine_t* e, void* stream_v) {
+  if (!e) return fail(SEM_ERR_ARG, "null argument");
+  cudaStream_t stream = (cudaStream_t)stream_v;
+  const bool use_strip = (e->cfg.kernel == 2);
+  // ---- retire solves whose program has ended: outputs, then free the workspace
+  for (size_t i = 0; i < e->running.size();) {
+    EngineJob* j = e->running[i];
+    if (e->tick < j->start + j->prog) { ++i; continue; }
+    const sem_plan_s* p = j->s.plan;
+    char* a = e->arena + j->off;
+    if ((j->s.flags & SEM_F_ADJOINT) && j->s.grad_out) {
+      grad_out_kernel<<<std::min(1024, (p->npoints + 255) / 256), 256, 0, stream>>>(
+          j->s.velocity, p->node_pos, (const double*)(a + j->ws.grad), j->s.inv_sigma2,
+          (const double*)(a + j->ws.misfit) + 2 * p->nrec, j->s.grad_out, p->npoints);
+      e->launches++;
+    }
+    if ((j->s.flags & SEM_F_MISFIT) && j->s.loglik_out) {
+      loglik_kernel<<<1, 32, 0, stream>>>((const double*)(a + j->ws.misfit), p->nrec, j->s.inv_sigma2,
+                                          j->s.loglik_out);
+      e->launches++;
+    }
+    if (j->s.status_out) {
+      copy_status_kernel<<<1, 32, 0, stream>>>((const int*)(a + j->ws.status), j->s.status_out);
+      e->launches++;
+    }
+    CUDA_TRY(cudaEventCreateWithFlags(&j->ev, cudaEventDisableTiming));
+    CUDA_TRY(cudaEventRecord(j->ev, stream));
+    arena_free(e, j->off, j->ws.bytes);
+    j->state = 2;
+    e->running.erase(e->running.begin() + i);
+  }
+  // ---- admit queued solves in arrival order while a slot and memory are free
+  while (!e->queue.empty() && (int)e->running.size() < e->cfg.max_solves) {
+    EngineJob* j = e->queue.front();
+    const long long off = arena_alloc(e, j->ws.bytes);
+    if (off < 0) break;
+    e->queue.pop_front();
+    j->off = off;
+    j->start = e->tick;
+    j->state = 1;
+    const sem_plan_s* p = j->s.plan;
+    char* a = e->arena + off;
+    const long long F = p->fstride * 4;
+    CUDA_TRY(cudaMemsetAsync(a + j->ws.W, 0, F, stream));
+    CUDA_TRY(cudaMemsetAsync(a + j->ws.V, 0, F, stream));
+    if (j->s.flags & SEM_F_ADJOINT) {
+      CUDA_TRY(cudaMemsetAsync(a + j->ws.ckpt, 0, 2 * F, stream));
+      CUDA_TRY(cudaMemsetAsync(a + j->ws.ring, 0, F, stream));
+      CUDA_TRY(cudaMemsetAsync(a + j->ws.L, 0, 3 * F, stream));
+      CUDA_TRY(cudaMemsetAsync(a + j->ws.grad, 0, 2 * F, stream));
+    }
+    CUDA_TRY(cudaMemsetAsync(a + j->ws.misfit, 0, j->ws.status - j->ws.misfit + 256, stream));
+    set_c2_kernel<<<std::min(1024, (p->npoints + 255) / 256), 256, 0, stream>>>(
+        j->s.velocity, p->node_pos, (float*)(a + j->ws.c2), p->npoints);
+    e->launches++;
+    e->running.push_back(j);
+  }
+  if (e->running.empty()) return SEM_OK;
+  // ---- descriptors and CTA maps of the running set, grouped by order
+  std::vector<EngineJob*> order(e->running);
+  std::stable_sort(order.begin(), order.end(),
+                   [](EngineJob* x, EngineJob* y) { return x->s.plan->npol < y->s.plan->npol; });
+  const int n = (int)order.size();
+  e->h_solves.assign(n, SolveDev{});
+  e->h_cta.clear();
+  struct Group { int N; long long cta0, ncta; bool adj; int first; };
+  std::vector<Group> groups;
+  for (int oi = 0; oi < n; ++oi) {
+    EngineJob* j = order[oi];
+    const sem_plan_s* p = j->s.plan;
+    sem_plan_s::Lists L;
+    int ntx, ntz, ntiles, rc;
+    if (use_strip) {
+      const int ewm = strip_ew_max(p->npol);
+      ntx = (p->nelx + ewm - 1) / ewm;
+      ntz = (p->nelx + ntx - 1) / ntx;
+      ntx = (p->nelx + ntz - 1) / ntz;
+      ntiles = ntx;
+      rc = get_strip_lists(p, ntz, &L);
+    } else {
+      ntiles = tiles_of(p, e->cfg.tile_ex, e->cfg.tile_ez, &ntx, &ntz);
+      rc = get_lists(p, e->cfg.tile_ex, e->cfg.tile_ez, &L);
+    }
+    if (rc) return rc;
+    if (groups.empty() || groups.back().N != p->npol)
+      groups.push_back(Group{p->npol, (long long)e->h_cta.size(), 0, false, oi});
+    Group& G = groups.back();
+    G.adj |= (j->s.flags & SEM_F_ADJOINT) != 0;
+    char* a = e->arena + j->off;
+    SolveDev& d = e->h_solves[oi];
+    d.nelx = p->nelx; d.nelz = p->nelz; d.nxg = p->nxg; d.nzg = p->nzg; d.pitch = p->pitch;
+    d.tiles_x = ntx; d.tiles_z = ntz;
+    d.tile_base = (int)(e->h_cta.size() - G.cta0);
+    d.nt = p->nt; d.k = j->k; d.nseg = j->nseg; d.flags = j->s.flags;
+    d.start_tick = (int)j->start;
+    d.it0 = j->s.it0; d.it1 = j->s.it1; d.decim = j->s.decim;
+    d.src_gx = p->src_gx; d.src_gz = p->src_gz; d.nrec = p->nrec;
+    d.fstride = p->fstride;
+    const bool adj = j->s.flags & SEM_F_ADJOINT;
+    d.c2 = (const float*)(a + j->ws.c2);
+    d.W = (float*)(a + j->ws.W);
+    d.V = (float*)(a + j->ws.V);
+    d.ckpt = adj ? (float*)(a + j->ws.ckpt) : nullptr;
+    d.ring = adj ? (float*)(a + j->ws.ring) : nullptr;
+    d.L = adj ? (float*)(a + j->ws.L) : nullptr;
+    d.Mu = adj ? (float*)(a + j->ws.Mu) : nullptr;
+    d.grad = adj ? (double*)(a + j->ws.grad) : nullptr;
+    d.D = p->D; d.beta = p->beta; d.tx = p->tx; d.tz = p->tz; d.src_term = p->src_term;
+    d.rec_base = p->rec_base; d.rec_w = p->rec_w;
+    d.rec_tile_off = L.rec_off; d.rec_tile_ids = L.rec_ids;
+    d.inj_tile_off = L.inj_off; d.inj_tile_ids = L.inj_ids;
+    d.rec_out = j->s.rec_out; d.yobs = j->s.y_obs;
+    d.misfit = (double*)(a + j->ws.misfit);
+    d.rmax = d.misfit + p->nrec;
+    d.adj_scale = d.misfit + 2 * p->nrec;
+    d.status = (int*)(a + j->ws.status);
+    for (int c = 0; c < ntiles; ++c) e->h_cta.push_back(oi - G.first);
+    G.ncta += ntiles;
+  }
+  if (n > e->solves_cap) {
+    cudaFree(e->d_solves);
+    e->d_solves = nullptr;
+    CUDA_TRY(cudaMalloc((void**)&e->d_solves, sizeof(SolveDev) * std::max(n, e->cfg.max_solves)));
+    e->solves_cap = std::max(n, e->cfg.max_solves);
+  }
+  if ((long long)e->h_cta.size() > e->cta_cap) {
+    cudaFree(e->d_cta);
+    e->d_cta = nullptr;
+    const long long cap = std::max<long long>((long long)e->h_cta.size() * 2, 1024);
+    CUDA_TRY(cudaMalloc((void**)&e->d_cta, sizeof(int) * cap));
+    e->cta_cap = cap;
+  }
+  CUDA_TRY(cudaMemcpyAsync(e->d_solves, e->h_solves.data(), sizeof(SolveDev) * n,
+                           cudaMemcpyHostToDevice, stream));
+  CUDA_TRY(cudaMemcpyAsync(e->d_cta, e->h_cta.data(), sizeof(int) * e->h_cta.size(),
+                           cudaMemcpyHostToDevice, stream));
+  // ---- ticks
+  for (int c = 0; c < e->cfg.ticks_per_step; ++c) {
+    for (auto& G : groups) {
+      KernelFn fn = use_strip ? strip_kernel_for(G.N) : kernel_for(G.N);
+      if (!fn) return fail(SEM_ERR_UNSUPPORTED, "polynomial order");
+      const size_t smem = (size_t)(use_strip ? strip_smem_floats(G.N, G.adj)
+                                             : smem_floats(G.N, e->cfg.tile_ex, e->cfg.tile_ez, G.adj)) *
+                          sizeof(float);
+      if (c == 0)
+        CUDA_TRY(cudaFuncSetAttribute((const void*)fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      fn<<<(unsigned)G.ncta, use_strip ? strip_threads(G.N) : 256, smem, stream>>>(
+          e->d_solves + G.first, e->d_cta + G.cta0, e->d_tick, e->cfg.tile_ex, e->cfg.tile_ez);
+      e->launches++;
+    }
+    tick_advance_kernel<<<1, 1, 0, stream>>>(e->d_tick);
+    e->launches++;
+  }
+  e->tick += e->cfg.ticks_per_step;
+  CUDA_TRY(cudaGetLastError());
+  return SEM_OK;
 }
 
 }  // extern "C"

@@ -116,6 +116,7 @@ class SEMPlan:
         if not torch.cuda.is_available():
             raise RuntimeError("mun_b200 needs a CUDA device (no CPU fallback)")
         torch.cuda.init()
+        self.kwargs = dict(kw)
         a = build_plan_arrays(**kw)
         self.arrays = a
         self.nt, self.npoints, self.nrec, self.npol = a["nt"], a["npoints"], a["nrec"], a["npol"]

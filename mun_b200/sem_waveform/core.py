@@ -220,22 +220,34 @@ class SEMSimulation:
 
     # ------------------------------------------------------------------ model building
     def _build_velocity(self, ctrl_abs):
-        """Velocity (and signed distance, extras) for absolute control points."""
+        """Velocity (and signed distance, extras) for absolute control points.  On a CUDA
+        device the model is built there (``sem_velocity_from_curve``); the host builders
+        compute the same numbers (``method.velocity_on_device = False`` selects them)."""
         vp = self.config["velocity"]
         tau, samples = float(vp["tau"]), int(vp["spline_samples"])
         anom = vp.get("anomaly", {}) if isinstance(vp.get("anomaly", {}), dict) else {}
+        ctrl = np.reshape(ctrl_abs, (6, 2) if self.variant == "canonical" else (-1, 2))
+        v_in = self.vmin if self.variant == "canonical" else float(anom.get("v_inside", self.vmin))
+        blend = "smooth" if self.variant == "canonical" else str(anom.get("blend", "smooth"))
+        if self.device.type == "cuda" and self.config["method"].get("velocity_on_device", True):
+            if not hasattr(self, "_coords_dev"):
+                self._coords_dev = torch.as_tensor(self.global_coords, device=self.device)
+                bg = self._background()
+                self._bg_dev = None if bg is None else torch.as_tensor(bg, device=self.device)
+            vel_d, sd_d, us_d, nr_d = vel.build_velocity_device(
+                self._coords_dev, ctrl, tau, samples, v_in, v_outside=self.vmax,
+                v_background_dev=self._bg_dev, periodic=(self.variant == "grid2d"), blend=blend)
+            return (vel_d.cpu().numpy(), sd_d.cpu().numpy(),
+                    {"u_star": us_d.cpu().numpy(), "normal_out": nr_d.cpu().numpy()})
         if self.variant == "canonical":
-            return vel.build_velocity_on_sem_nodes(self.global_coords, np.reshape(ctrl_abs, (6, 2)),
-                                                   self.vmin, self.vmax, tau, samples, 7)
-        v_in = float(anom.get("v_inside", self.vmin))
-        blend = str(anom.get("blend", "smooth"))
+            return vel.build_velocity_on_sem_nodes(self.global_coords, ctrl, self.vmin, self.vmax, tau,
+                                                   samples, 7)
         if self.variant == "layered":
             return vel.build_velocity_layered_with_anomaly(
-                self.global_coords, self.interfaces_z, self.layer_velocities,
-                np.reshape(ctrl_abs, (-1, 2)), v_in, tau, samples, 7, blend)
+                self.global_coords, self.interfaces_z, self.layer_velocities, ctrl, v_in, tau, samples, 7,
+                blend)
         return vel.build_velocity_2d_background_with_anomaly(
-            self.global_coords, self.v_background, np.reshape(ctrl_abs, (-1, 2)), v_in, tau,
-            samples, 7, blend)
+            self.global_coords, self.v_background, ctrl, v_in, tau, samples, 7, blend)
 
     def _background(self):
         if self.variant == "layered":

@@ -274,3 +274,52 @@ def build_velocity_2d_background_with_anomaly(nodes_xy, v_background, ctrl6_xy=N
     else:
         v = v_bg + (float(v_inside) - v_bg) * _sigmoid_blend(sd, tau)
     return v, sd, {"u_star": us, "closest": cb, "tangent": th, "normal_out": no}
+
+
+# ------------------------------------------------------------------ device builder
+
+
+def build_velocity_device(coords_dev, ctrl, tau, samples, v_inside, v_outside=None, v_background_dev=None,
+                          newton_steps=7, periodic=False, blend="smooth", stream=None):
+    """Same result as the host builders above, computed on the GPU
+    (``sem_velocity_from_curve``).  ``coords_dev``: (P,2) float64 CUDA tensor; the
+    background is either ``v_outside`` (constant) or ``v_background_dev`` (P,).
+    Returns CUDA tensors (velocity, sd, u_star, normal_out)."""
+    import ctypes as C
+
+    import torch
+
+    from .. import _lib
+    sp = closed_spline_periodic(ctrl) if periodic else closed_spline_clamped(ctrl)
+    if periodic:
+        u0 = np.linspace(sp.lo, sp.hi, int(samples), endpoint=False)
+    else:
+        u0 = np.linspace(sp.lo, sp.hi, int(samples))
+    C0 = sp.eval(u0)
+    dev = coords_dev.device
+    u0_d = torch.as_tensor(u0, device=dev)
+    s_d = torch.as_tensor(np.ascontiguousarray(C0), device=dev)
+    n = coords_dev.shape[0]
+    vel = torch.empty(n, dtype=torch.float64, device=dev)
+    sd = torch.empty(n, dtype=torch.float64, device=dev)
+    us = torch.empty(n, dtype=torch.float64, device=dev)
+    nr = torch.empty((n, 2), dtype=torch.float64, device=dev)
+    knots = np.ascontiguousarray(sp.t, dtype=np.float64)
+    coef = np.ascontiguousarray(sp.c, dtype=np.float64)
+    cd = _lib.CurveDesc(len(coef), knots.ctypes.data_as(C.POINTER(C.c_double)),
+                        coef.ctypes.data_as(C.POINTER(C.c_double)), float(sp.lo), float(sp.hi),
+                        len(u0), u0_d.data_ptr(), s_d.data_ptr(), int(newton_steps), float(tau),
+                        float(v_inside), 1 if blend == "replace" else 0)
+    lib = _lib.load()
+    cs = coords_dev.contiguous()
+    strm = stream if stream is not None else torch.cuda.current_stream().cuda_stream
+    rc = lib.sem_velocity_from_curve(
+        C.byref(cd), int(n), C.c_void_p(cs.data_ptr()),
+        C.c_void_p(v_background_dev.data_ptr()) if v_background_dev is not None else None,
+        float(v_outside if v_outside is not None else 0.0), C.c_void_p(vel.data_ptr()),
+        C.c_void_p(sd.data_ptr()), C.c_void_p(us.data_ptr()), C.c_void_p(nr.data_ptr()), C.c_void_p(strm))
+    if rc != 0:
+        raise ValueError("sem_velocity_from_curve: " + lib.sem_velocity_last_error().decode())
+    torch.cuda.current_stream().synchronize() if stream is None else None
+    del u0_d, s_d, cs
+    return vel, sd, us, nr

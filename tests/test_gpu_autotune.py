@@ -1,0 +1,31 @@
+"""The autotuner picks a configuration and the tuned run gives bitwise the default result."""
+import numpy as np
+import pytest
+import torch
+
+from mun_b200 import Batch, SolveSpec
+from mun_b200.autotune import tune, tuned_batch
+from tests.goldens import load
+from tests.gpu_cases import aligned_obs, dev, plan_for
+
+pytestmark = pytest.mark.gpu
+
+
+def test_tuned_configuration_gives_the_same_numbers():
+    g = load("inject_n3")
+    plan = plan_for(g["config"], g["dt"], g["nt"])
+    y = dev(aligned_obs(g))
+    inv = 1.0 / float(g["sigma"]) ** 2
+
+    def specs():
+        return [SolveSpec(plan, dev(np.asarray(g["velocity"]) * (1 + 0.01 * i)), adjoint=True, y_obs=y,
+                          inv_sigma2=inv, ckpt_k=9) for i in range(6)]
+    cfg = tune(specs(), nt_proxy=24, repeats=1)
+    assert cfg["kernel"] in (1, 2) and cfg["graph_chunk"] in (0, 32)
+    ref = specs()
+    Batch().run(ref)
+    sp = specs()
+    b, _ = tuned_batch(sp)
+    b.run(sp)
+    for a, c in zip(ref, sp):
+        assert torch.equal(a.grad, c.grad) and torch.equal(a.rec, c.rec)

@@ -33,14 +33,13 @@ def audit(N, nelx, nelz):
     pitch = pitch_of(nxg)
     ns, EW = strips_of(nelx, N)
     BW = bw(N)
+    SEGS = (THREADS - N - 1) // N + 1
     owner = np.zeros(nxg, dtype=int)
     for strip in range(ns):
         e0, e1 = strip * EW, min(strip * EW + EW, nelx)
         assert e1 > e0
         sx0 = e0 * N
         so1 = nxg if e1 == nelx else e1 * N
-        NC = (e1 - e0) * N + N + 1
-        assert NC <= THREADS
         X0 = (sx0 - N) & ~3
         off = (sx0 - N) - X0
         assert 0 <= off <= 3 and X0 % 4 == 0
@@ -48,45 +47,28 @@ def audit(N, nelx, nelz):
         assert cs % 4 == 0 and ce % 4 == 0 and ce > cs      # 16-byte aligned bulk copies
         assert (cs - X0) % 4 == 0 and ((ce - cs) * 4) % 16 == 0
         copied = set(range(cs, ce))
-        qr_written, ql_written = set(), set()
+        nseg = e1 - e0 + 1
+        seg0 = 1 if e0 == 0 else 0
+        assert nseg <= SEGS
+        written = set()
+        for sgi in range(seg0, nseg):        # phase A x-items read the segment's columns
+            for b in range(NP):
+                sm_col = off + sgi * N + b
+                assert 0 <= sm_col < BW
+                assert X0 + sm_col in copied
+            written.add(sgi)
+        assert so1 - sx0 <= THREADS
         for tid in range(THREADS):
-            gx = sx0 - N + tid
-            valid = tid < NC and 0 <= gx < nxg
-            if not valid:
-                continue
-            sc = tid + off
-            assert 0 <= sc < BW
-            er, ia = divmod(gx, N)
-            if er < nelx and tid < NC - 1:
-                for b in range(NP):
-                    col = gx - ia + b
-                    assert col in copied and 0 <= sc - ia + b < BW
-                qr_written.add(tid)
-            if ia == 0 and er >= 1 and tid >= N:
-                for b in range(NP):
-                    assert gx - N + b in copied
-                ql_written.add(tid)
-        for tid in range(THREADS):
-            gx = sx0 - N + tid
-            if not (tid < NC and 0 <= gx < nxg and sx0 <= gx < so1):
+            gx = sx0 + tid
+            if gx >= so1:
                 continue
             owner[gx] += 1
-            assert gx in copied
+            sc = tid + N + off
+            assert 0 <= sc < BW and X0 + sc == gx and gx in copied   # z-column and node reads
             er, ia = divmod(gx, N)
-            cl = tid - ia
-            if ia:
-                need_r = [cl + p for p in range(N)]
-                need_l = [cl + N]
-            else:
-                need_r, need_l = [], []
-                if er >= 1:
-                    need_r += [tid - N + p for p in range(N)]
-                    need_l += [tid]
-                if er < nelx:
-                    need_r += [tid + p for p in range(N)]
-                    need_l += [tid + N]
-            assert all(c in qr_written for c in need_r), (strip, gx)
-            assert all(c in ql_written for c in need_l), (strip, gx)
+            s_r = er - e0 + 1
+            need = [s_r] if ia else ([s_r - 1] if er >= 1 else []) + ([s_r] if er < nelx else [])
+            assert need and all(x in written for x in need), (strip, gx)
     assert (owner == 1).all()
 
 
@@ -110,6 +92,7 @@ def test_strip_receiver_lists_cover():
             X0 = (sx0 - N) & ~3
             # recording strip has the whole element in its copied columns
             assert bx - X0 >= 0 and bx + N - X0 < bw(N)
+            assert bx + N <= min(X0 + bw(N), -(-nxg // 32) * 32) - 1
             # injection: every node owned by exactly one listed strip
             listed = []
             for s in range(ns):
