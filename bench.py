@@ -163,6 +163,219 @@ def run_reference(args):
     print(json.dumps(out), flush=True)
 
 
+def _layered_plume(coords, cx, cz, ax, az, drop=0.08):
+    from mun_b200.bspline import layered_velocity
+    base = layered_velocity(coords[:, 1], [300.0, 650.0], [1500.0, 2200.0, 3000.0])
+    r2 = ((coords[:, 0] - cx) / ax) ** 2 + ((coords[:, 1] - cz) / az) ** 2
+    w = 1.0 / (1.0 + np.exp((r2 - 1.0) * 8.0))   # smooth ellipse indicator
+    return base * (1.0 - drop * w)
+
+
+def run_uneven(args):
+    """Uneven batch: 64 solves, meshes 40x20..200x100 (2:1), orders {3,4,5}, 8-20 Hz,
+    nt from each mesh's CFL for T=0.5 s clamped to [1500, 6000], layered base with a
+    seeded elliptical -8% plume; one batched launch sequence vs one solve at a time."""
+    import torch
+    from mun_b200 import Batch, SEMPlan, SolveSpec
+    from mun_b200.mesh import create_global_mesh
+    rng = np.random.default_rng(3)
+    specs_args = []
+    for i in range(args.models if args.models != 256 else 64):
+        nelx = int(rng.integers(40, 201))
+        nelz = max(1, nelx // 2)
+        N = int(rng.choice([3, 4, 5]))
+        f0 = float(rng.uniform(8.0, 20.0))
+        coords, _, ng = create_global_mesh(0.0, 2000.0, 0.0, 1000.0, nelx, nelz, N)
+        v = _layered_plume(coords, rng.uniform(600, 1400), rng.uniform(400, 700), rng.uniform(150, 400),
+                           rng.uniform(150, 400))
+        h = min(2000.0 / nelx, 1000.0 / nelz)
+        dt = 0.35 * (h / (N + 1)) / (float(v.max()) * (N + 1) * np.sqrt(2.0))
+        nt = int(min(6000, max(1500, np.ceil(0.5 / dt))))
+        rec = np.stack([np.linspace(0.0, 2000.0, 100), np.full(100, 10.0)], 1)
+        specs_args.append(dict(plan=dict(xmin=0.0, xmax=2000.0, zmin=0.0, zmax=1000.0, nelx=nelx, nelz=nelz,
+                                         npol=N, dt=dt, nt=nt, src_xz=(1000.0, 20.0), f0=f0, amp=1.0,
+                                         receivers=rec, pml_thickness=200.0, sponge_cmax=3000.0,
+                                         coords=coords, node_grid=ng), v=v))
+    plans = [SEMPlan(**a["plan"]) for a in specs_args]
+    dev = torch.device("cuda")
+    stream = torch.cuda.Stream()
+    # observations: each model's own forward with a 2% slower velocity
+    ys = []
+    for p, a in zip(plans, specs_args):
+        s = SolveSpec(p, torch.as_tensor(a["v"] * 0.98, device=dev), shift=True)
+        with torch.cuda.stream(stream):
+            Batch().run([s])
+        ys.append(s.rec.double())
+    stream.synchronize()
+    node_steps = sum(p.npoints * p.nt for p in plans)
+
+    def specs():
+        return [SolveSpec(p, torch.as_tensor(a["v"], device=dev), adjoint=True, y_obs=y, inv_sigma2=1e6,
+                          ckpt_k=0) for p, a, y in zip(plans, specs_args, ys)]
+    b = Batch(kernel=args.kernel, graph_chunk=args.graph_chunk)
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ms = []
+    for it in range(args.warmup + args.steps):
+        sp = specs()
+        with torch.cuda.stream(stream):
+            ev0.record(stream)
+            b.run(sp)
+            ev1.record(stream)
+        ev1.synchronize()
+        if it >= args.warmup:
+            ms.append(ev0.elapsed_time(ev1))
+    batched = len(plans) / (np.mean(ms) / 1e3)
+    plain_ms = []
+    pb = Batch()
+    for sp in specs()[: max(4, args.plain)]:
+        with torch.cuda.stream(stream):
+            ev0.record(stream)
+            pb.run([sp])
+            ev1.record(stream)
+        ev1.synchronize()
+        plain_ms.append(ev0.elapsed_time(ev1))
+    # plain time of the whole set, scaled by node-steps of the timed subset
+    sub = plans[: len(plain_ms)]
+    plain_total = sum(plain_ms) * node_steps / sum(p.npoints * p.nt for p in sub)
+    print(json.dumps({"workload": "uneven batch: 64 solves, 40x20..200x100 el, N in {3,4,5}, nt 1500-6000",
+                      "metric": "SEM fwd+adjoint solves/s", "batched": batched, "unit": "solves/s",
+                      "batched_ms": float(np.mean(ms)), "kernel": b.last_kernel,
+                      "plain_estimated": len(plans) / (plain_total / 1e3), "plain_solves_timed": len(plain_ms),
+                      "mnode_steps_per_s": node_steps / (np.mean(ms) / 1e3) / 1e6,
+                      "orders": sorted(set(p.npol for p in plans)), "nt_range": [min(p.nt for p in plans),
+                                                                                   max(p.nt for p in plans)]}),
+          flush=True)
+
+
+def run_serving(args):
+    """Serving: Poisson request stream of forward-only likelihoods from 16 random-walk MCMC
+    chains (meshes 60x30..120x60, order 4) mixed with flow-trainer batches of 32
+    forward+adjoint solves (100x50, order 4, 10x6 B-spline perturbations); continuous
+    batching in the engine; p50/p99 latency and solves/s vs the same requests served one
+    at a time."""
+    import torch
+    from mun_b200 import Batch, SEMPlan, SolveSpec
+    from mun_b200.mesh import create_global_mesh
+    from mun_b200.serving import Engine, Request, serve
+    rng = np.random.default_rng(4)
+    dev = torch.device("cuda")
+    T = args.serve_T
+    chains = []
+    for c in range(16):
+        nelx = int(rng.integers(60, 121))
+        nelz = nelx // 2
+        coords, _, ng = create_global_mesh(0.0, 2000.0, 0.0, 1000.0, nelx, nelz, 4)
+        v0 = _layered_plume(coords, rng.uniform(800, 1200), 550.0, 250.0, 150.0)
+        h = 2000.0 / nelx
+        dt = 0.35 * (h / 5) / (3300.0 * 5 * np.sqrt(2.0))
+        nt = int(np.ceil(T / dt))
+        rec = np.stack([np.linspace(0.0, 2000.0, 50), np.full(50, 10.0)], 1)
+        p = SEMPlan(xmin=0.0, xmax=2000.0, zmin=0.0, zmax=1000.0, nelx=nelx, nelz=nelz, npol=4, dt=dt, nt=nt,
+                    src_xz=(1000.0, 20.0), f0=10.0, amp=1.0, receivers=rec, pml_thickness=200.0,
+                    sponge_cmax=3000.0, coords=coords, node_grid=ng)
+        s = SolveSpec(p, torch.as_tensor(v0, device=dev))
+        Batch().run([s])
+        chains.append((p, v0, s.rec.double(), coords))
+    W = workload(nmodels=32, nt=int(np.ceil(T / workload(nmodels=1, nt=10)["dt"])))
+    fplan = SEMPlan(**W["plan_kw"])
+    obs = SolveSpec(fplan, torch.as_tensor(W["v_true"], device=dev), shift=True)
+    Batch().run([obs])
+    fy = obs.rec.double()
+    reqs = []
+    t = 0.0
+    rate = args.serve_rate
+    n_req = args.serve_requests
+    k_flow = 0
+    while len(reqs) < n_req:
+        t += rng.exponential(1.0 / rate)
+        if rng.uniform() < 0.8:   # MCMC proposal
+            c = int(rng.integers(16))
+            p, v0, y, coords = chains[c]
+            v = v0 + rng.normal(0, 20.0) * np.exp(-((coords[:, 0] - 1000) ** 2 + (coords[:, 1] - 550) ** 2) / 2e5)
+            reqs.append(Request(t, SolveSpec(p, torch.as_tensor(v, device=dev), misfit=True, y_obs=y,
+                                             inv_sigma2=1e6), "mcmc"))
+        else:                      # flow-trainer batch of 32 samples
+            for i in range(32):
+                reqs.append(Request(t, SolveSpec(fplan, torch.as_tensor(W["vels"][(32 * k_flow + i) % 32], device=dev),
+                                                 adjoint=True, y_obs=fy, inv_sigma2=1e6, ckpt_k=fplan.nt),
+                                    "flow"))
+            k_flow += 1
+    eng = Engine(max_solves=args.serve_slots, memory_cap_bytes=int(args.serve_cap_gb * (1 << 30)),
+                 ticks_per_step=args.serve_ticks, kernel=1)
+    done, lat, wall = serve(eng, reqs)
+    # serialized reference: the same requests one at a time, back to back
+    b = Batch()
+    t0 = time.perf_counter()
+    for r in reqs:
+        s = r.spec
+        s2 = SolveSpec(s.plan, s.velocity, adjoint=s.adjoint, misfit=s.misfit, shift=s.shift,
+                       y_obs=s.y_obs, inv_sigma2=s.inv_sigma2, ckpt_k=s.ckpt_k)
+        b.run([s2])
+    torch.cuda.synchronize()
+    serial = time.perf_counter() - t0
+    kinds = np.array([r.kind for r in done])
+    out = {"workload": f"serving: Poisson {rate:.0f} req/s, 16 MCMC chains (fwd likelihood, 60x30..120x60) "
+                       f"+ flow batches of 32 fwd+adj (100x50), T={T} s",
+           "requests": len(done), "wall_s": wall, "solves_per_s": len(done) / wall,
+           "p50_ms": 1e3 * float(np.percentile(lat, 50)), "p99_ms": 1e3 * float(np.percentile(lat, 99)),
+           "p50_ms_mcmc": 1e3 * float(np.percentile(lat[kinds == "mcmc"], 50)),
+           "p99_ms_mcmc": 1e3 * float(np.percentile(lat[kinds == "mcmc"], 99)),
+           "p50_ms_flow": 1e3 * float(np.percentile(lat[kinds == "flow"], 50)) if (kinds == "flow").any() else None,
+           "serialized_solves_per_s": len(reqs) / serial, "engine": eng.stats()}
+    print(json.dumps(out), flush=True)
+
+
+def run_single(args):
+    """Single large solve: 8000x4000 m, 400x200 elements, order 4 (1601x801 nodes), GRF
+    velocity (mean 2500, std 300, correlation 200 m, clipped [1500,4000], seed 1), Ricker
+    15 Hz at the surface centre, 400 surface receivers, 5000 steps, checkpoint every 250."""
+    import torch
+    from mun_b200 import Batch, SEMPlan, SolveSpec
+    from mun_b200.mesh import create_global_mesh
+    nelx, nelz, N = 400, 200, 4
+    coords, _, ng = create_global_mesh(0.0, 8000.0, 0.0, 4000.0, nelx, nelz, N)
+    rng = np.random.default_rng(1)
+    nx, nz = 801, 401
+    w = rng.standard_normal((nz, nx))
+    kx = np.fft.fftfreq(nx, d=10.0)
+    kz = np.fft.fftfreq(nz, d=10.0)
+    K2 = kx[None, :] ** 2 + kz[:, None] ** 2
+    f = np.real(np.fft.ifft2(np.fft.fft2(w) * np.exp(-2 * (np.pi ** 2) * (200.0 ** 2) * K2)))
+    f = (f - f.mean()) / f.std() * 300.0 + 2500.0
+    grid = np.clip(f, 1500.0, 4000.0)
+    from mun_b200.sem_waveform.velocity import build_background_from_grid
+    v = build_background_from_grid(coords, np.linspace(0, 8000, nx), np.linspace(0, 4000, nz), grid)
+    dt = 0.35 * (20.0 / 5) / (float(v.max()) * 5 * np.sqrt(2.0))
+    nt = args.nt if args.nt != 3000 else 5000
+    rec = np.stack([np.linspace(0.0, 8000.0, 400), np.full(400, 1e-3)], 1)
+    plan = SEMPlan(xmin=0.0, xmax=8000.0, zmin=0.0, zmax=4000.0, nelx=nelx, nelz=nelz, npol=N, dt=dt, nt=nt,
+                   src_xz=(4000.0, 1e-3), f0=15.0, amp=1.0, receivers=rec, pml_thickness=400.0,
+                   sponge_cmax=4000.0, coords=coords, node_grid=ng)
+    dev = torch.device("cuda")
+    obs = SolveSpec(plan, torch.as_tensor(v * 1.01, device=dev), shift=True)
+    Batch().run([obs])
+    stream = torch.cuda.Stream()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ms = []
+    b = Batch(kernel=args.kernel)
+    for it in range(args.warmup + args.steps):
+        s = SolveSpec(plan, torch.as_tensor(v, device=dev), adjoint=True, y_obs=obs.rec.double(), inv_sigma2=1e6,
+                      ckpt_k=250)
+        with torch.cuda.stream(stream):
+            ev0.record(stream)
+            b.run([s])
+            ev1.record(stream)
+        ev1.synchronize()
+        if it >= args.warmup:
+            ms.append(ev0.elapsed_time(ev1))
+    m = float(np.mean(ms))
+    print(json.dumps({"workload": "single large solve: 400x200 el, N=4, 1,282,401 nodes, 5000 steps, k=250",
+                      "nt": nt, "ms_per_solve": m, "solves_per_s": 1e3 / m, "kernel": b.last_kernel,
+                      "mnode_steps_per_s": plan.npoints * nt / (m / 1e3) / 1e6,
+                      "achieved_gbs_56B": 56 * plan.npoints * nt / (m / 1e3) / 1e9,
+                      "status": int(s.status.item())}), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -179,9 +392,22 @@ def main():
     ap.add_argument("--ref-nt", type=int, default=200)
     ap.add_argument("--cpu-nt", type=int, default=200)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--workload", default="elbo", choices=["elbo", "uneven", "serving", "single"])
+    ap.add_argument("--serve-rate", type=float, default=200.0)
+    ap.add_argument("--serve-requests", type=int, default=400)
+    ap.add_argument("--serve-T", type=float, default=0.25)
+    ap.add_argument("--serve-slots", type=int, default=256)
+    ap.add_argument("--serve-cap-gb", type=float, default=150.0)
+    ap.add_argument("--serve-ticks", type=int, default=32)
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
+    if args.workload == "uneven":
+        return run_uneven(args)
+    if args.workload == "serving":
+        return run_serving(args)
+    if args.workload == "single":
+        return run_single(args)
 
     import torch
     import torch.distributed as dist
