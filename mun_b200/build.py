@@ -26,18 +26,20 @@ def needs_build():
     return any(os.path.getmtime(p) > t for p in SOURCES + HEADERS)
 
 
-def build(force=False, verbose=False):
-    """Compile the library if a source is newer than the .so (or ``force``)."""
-    if not force and not needs_build():
+def build(force=False, verbose=False, out=None, defines=()):
+    """Compile the library if a source is newer than the .so (or ``force``).  ``out`` and
+    ``defines`` build a variant elsewhere (kernel tuning experiments)."""
+    target = out or SO
+    if out is None and not force and not needs_build():
         return SO
-    cmd = [nvcc_path()] + NVCC_FLAGS + ["-o", SO + ".tmp"] + SOURCES
+    cmd = [nvcc_path()] + NVCC_FLAGS + [f"-D{d}" for d in defines] + ["-o", target + ".tmp"] + SOURCES
     res = subprocess.run(cmd, capture_output=True, text=True)
     if res.returncode != 0:
         raise RuntimeError("nvcc failed:\n" + res.stderr)
     if verbose:
         print(res.stderr)
-    os.replace(SO + ".tmp", SO)
-    return SO
+    os.replace(target + ".tmp", target)
+    return target
 
 
 if __name__ == "__main__":

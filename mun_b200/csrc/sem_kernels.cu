@@ -547,11 +547,25 @@ __global__ void __launch_bounds__(256) sem_tick_kernel(const SolveDev* __restric
 // one thread per owned column combines the segment results and advances the band's
 // nodes.  Arithmetic order matches the tile kernel (bitwise-equal results).
 // ----------------------------------------------------------------------------
+#ifndef SEM_STAGES_ADJ
+#define SEM_STAGES_ADJ 2
+#endif
+#ifndef SEM_STRIP_MIN_BLOCKS
+#define SEM_STRIP_MIN_BLOCKS 4
+#endif
+#ifndef SEM_ONE_BARRIER
+#define SEM_ONE_BARRIER 1
+#endif
+#ifndef SEM_WAIT_HINT_NS
+#define SEM_WAIT_HINT_NS 20000
+#endif
 constexpr int kStripCols = 128;
-constexpr int kStages = 3;        // ring slots of forward/replay ticks
-constexpr int kStagesAdj = 2;     // ring slots of adjoint ticks (bigger bands)
+constexpr int kStages = 3;                   // ring slots of forward/replay ticks
+constexpr int kStagesAdj = SEM_STAGES_ADJ;   // ring slots of adjoint ticks (bigger bands)
 constexpr int kStripInj = 256;               // receivers per band of one strip (host-checked)
 constexpr long long kWaitNs = 2000000000LL;  // bounded mbarrier waits: 2 s
+// floats ahead of the ring: mbarriers (64), D (64), beta (16), the band's z-table rows (48)
+constexpr int kStripHdr = 192;
 
 __host__ __device__ inline int strip_ew_max(int N) { return (kStripCols - N - 1) / N; }
 __host__ __device__ inline int strip_bw(int N) { return (kStripCols + 3 + 3) & ~3; }  // smem row
@@ -570,12 +584,22 @@ __device__ __forceinline__ void mbar_expect_tx(unsigned long long* bar, unsigned
 }
 __device__ __forceinline__ bool mbar_try_wait(unsigned long long* bar, unsigned parity) {
   unsigned ok;
+#if SEM_WAIT_HINT_NS > 0
+  // suspend until the phase completes (or the hint elapses) instead of spinning
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
+      "selp.u32 %0, 1, 0, p;\n}"
+      : "=r"(ok)
+      : "r"(smem_addr(bar)), "r"(parity), "r"((unsigned)SEM_WAIT_HINT_NS)
+      : "memory");
+#else
   asm volatile(
       "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
       "selp.u32 %0, 1, 0, p;\n}"
       : "=r"(ok)
       : "r"(smem_addr(bar)), "r"(parity)
       : "memory");
+#endif
   return ok != 0;
 }
 __device__ __forceinline__ long long global_ns() {
@@ -606,68 +630,58 @@ __host__ __device__ inline long long strip_stage_floats(int N, bool adj) {
   return ((long long)(nfloat + 2 * ndouble) * (N + 1) * strip_bw(N) + 31) & ~31LL;
 }
 // exchange arrays: x-segment results Xs[rows][segments][N+1] (+ sensitivity), z-segment
-// results Zs[N+1][cols] (+ sensitivity), injection rows and residuals
+// results stay in registers; injection rows and residuals
 __host__ __device__ inline long long strip_xch_floats(int N, bool adj) {
   const long long NP = N + 1, segs = strip_ew_max(N) + 1;
-  long long f = NP * segs * NP + NP * kStripCols;                    // Xs | Zs
-  if (adj) f += NP * segs * NP + NP * kStripCols + NP * kStripCols + kStripInj;  // SXs | SZs | inj | res
+  const long long nb = SEM_ONE_BARRIER ? 2 : 1;                      // exchange buffers
+  long long f = nb * (adj ? 2 : 1) * NP * segs * NP;                 // Xs | SXs (per buffer)
+  if (adj) f += NP * kStripCols + kStripInj;                         // inj | res
   return (f + 31) & ~31LL;
 }
 __host__ __device__ inline long long strip_smem_floats(int N, bool adj) {
   const long long fwd = kStages * strip_stage_floats(N, false) + strip_xch_floats(N, false);
   const long long adjf = kStagesAdj * strip_stage_floats(N, true) + strip_xch_floats(N, true);
-  return 64 + 96 + (adj ? (fwd > adjf ? fwd : adjf) : fwd);
+  return kStripHdr + (adj ? (fwd > adjf ? fwd : adjf) : fwd);
 }
 
+// Loads the N+1 consecutive floats of one x-line segment (16-byte aligned for N = 4,
+// where the strip's copy origin puts every element edge on a 4-float boundary).
 template <int N>
-__global__ void __launch_bounds__(kStripCols) sem_strip_kernel(const SolveDev* __restrict__ solves,
-                                                               const int* __restrict__ cta_solve,
-                                                               const int* __restrict__ tick_ptr,
-                                                               int unused0, int unused1) {
+__device__ __forceinline__ void load_seg(const float* p, float (&u)[N + 1]) {
+  if constexpr (N == 4) {
+    const float4 q = *reinterpret_cast<const float4*>(p);
+    u[0] = q.x; u[1] = q.y; u[2] = q.z; u[3] = q.w; u[4] = p[4];
+  } else {
+#pragma unroll
+    for (int b = 0; b <= N; ++b) u[b] = p[b];
+  }
+}
+
+// One tick of one strip, instantiated for forward-like ticks (FWD, FINAL, REPLAY) and for
+// adjoint ticks so that neither carries the other's branches.
+template <int N, bool ADJ>
+__device__ __forceinline__ void strip_tick(const SolveDev& S, const int act, const int t,
+                                           const int seg, float* smem, int* s_abort) {
   constexpr int NP = N + 1;
   constexpr int BW = (kStripCols + 3 + 3) & ~3;
   constexpr int NT = kStripCols;
   constexpr int SEGS = (kStripCols - N - 1) / N + 1;  // x-segments per band row (max)
-  extern __shared__ __align__(128) float smem[];
-  __shared__ SolveDev S;
-  __shared__ int s_act, s_t, s_seg, s_abort;
+  constexpr int NF = ADJ ? 4 : 3;                      // staged float fields
+  constexpr int NST = ADJ ? kStagesAdj : kStages;      // ring slots
+  constexpr int NBUF = SEM_ONE_BARRIER ? 2 : 1;        // exchange buffers
+  constexpr int XSZ = (ADJ ? 2 : 1) * NP * SEGS * NP;  // floats of one exchange buffer
+  const bool final_only = !ADJ && act == A_FINAL;
 
-  const int sid = cta_solve[blockIdx.x];
-  {
-    const unsigned long long* src = reinterpret_cast<const unsigned long long*>(solves + sid);
-    unsigned long long* dst = reinterpret_cast<unsigned long long*>(&S);
-    for (int i = threadIdx.x; i < (int)(sizeof(SolveDev) / 8); i += NT) dst[i] = src[i];
-  }
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    int act, t, seg;
-    decode(S, *tick_ptr - S.start_tick, act, t, seg);
-    s_act = act; s_t = t; s_seg = seg; s_abort = 0;
-  }
-  __syncthreads();
-  const int act = s_act;
-  if (act == A_NONE) return;
-  const int t = s_t, seg = s_seg;
-  if (act == A_SCALE) {
-    if (blockIdx.x == S.tile_base && threadIdx.x == 0) {
-      double m = 0.0;
-      for (int r = 0; r < S.nrec; ++r) m = fmax(m, S.rmax[r]);
-      *S.adj_scale = (m > 0.0 && isfinite(m)) ? ldexp(1.0, -ilogb(m)) : 1.0;
-    }
-    return;
-  }
-  const bool adj = (act == A_ADJ);
-  const bool final_only = (act == A_FINAL);
-
-  // ---------------- strip geometry (tiles_x = number of strips, tiles_z = elements/strip)
+  // ---------------- strip geometry (tiles_z = elements per strip)
+  const int nelx = S.nelx, nelz = S.nelz, nxg = S.nxg, nzg = S.nzg, pitch = S.pitch;
   const int strip = blockIdx.x - S.tile_base;
   const int EW = S.tiles_z;
-  const int e0 = strip * EW, e1 = min(e0 + EW, S.nelx);
+  const int e0 = strip * EW, e1 = min(e0 + EW, nelx);
   const int sx0 = e0 * N;                                   // first owned column
-  const int so1 = (e1 == S.nelx) ? S.nxg : e1 * N;          // owned columns [sx0, so1)
+  const int so1 = (e1 == nelx) ? nxg : e1 * N;              // owned columns [sx0, so1)
   const int X0 = (sx0 - N) & ~3;                            // 16-byte aligned copy origin
   const int off = (sx0 - N) - X0;                           // smem column of column sx0 - N
-  const int cs = max(X0, 0), ce = min(X0 + BW, S.pitch);    // copied columns
+  const int cs = max(X0, 0), ce = min(X0 + BW, pitch);      // copied columns
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int nseg = e1 - e0 + 1;                             // segments e0-1 .. e1-1
   const int seg0 = (e0 == 0) ? 1 : 0;                       // segment -1 does not exist
@@ -677,18 +691,14 @@ __global__ void __launch_bounds__(kStripCols) sem_strip_kernel(const SolveDev* _
 
   // ---------------- shared memory
   unsigned long long* bars = reinterpret_cast<unsigned long long*>(smem);
-  float* sD = smem + 64;
-  float* sB = sD + 64;
-  const int nfloat = (adj ? 4 : 3), ndouble = (adj ? 1 : 0);
-  const long long stage_f = strip_stage_floats(N, adj);
-  const int nst = adj ? kStagesAdj : kStages;    // ring slots
-  float* stages = smem + 64 + 96;
-  float* Xs = stages + nst * stage_f;            // [NP][SEGS][NP]
-  float* Zs = Xs + NP * SEGS * NP;                // [NP][NT]
-  float* SXs = Zs + NP * NT;                      // adjoint: [NP][SEGS][NP]
-  float* SZs = SXs + NP * SEGS * NP;              // [NP][NT]
-  float* sacc = SZs + NP * NT;                    // [NP][NT]
-  float* sres = sacc + NP * NT;                   // [kStripInj]
+  float* const sD = smem + 64;
+  float* const sB = sD + 64;
+  float* const sTz = sB + 16;                     // [2][3][8] band rows of 1/mz, Rz, dz
+  const long long stage_f = strip_stage_floats(N, ADJ);
+  float* const stages = smem + kStripHdr;
+  float* const xs0 = stages + NST * stage_f;      // exchange: Xs [NP][SEGS][NP] (+ SXs)
+  float* const sacc = xs0 + NBUF * XSZ;           // adjoint: injection rows [NP][NT]
+  float* const sres = sacc + NP * NT;             // adjoint: band residuals [kStripInj]
 
   // ---------------- which fields
   const float* cur;
@@ -696,57 +706,61 @@ __global__ void __launch_bounds__(kStripCols) sem_strip_kernel(const SolveDev* _
   float* out = nullptr;
   float* vout = nullptr;
   const float* fwdu = nullptr;
-  if (act == A_FWD) {
-    cur = fwd_b(S, t); vin = fwd_v(S, t);
-    out = (float*)fwd_b(S, t + 1); vout = (float*)fwd_v(S, t + 1);
-  } else if (act == A_FINAL) {
-    cur = fwd_b(S, t);
-  } else if (act == A_REPLAY) {
-    cur = rep_b(S, seg, t); vin = rep_v(S, seg, t);
-    out = (float*)rep_b(S, seg, t + 1); vout = (float*)rep_v(S, seg, t + 1);
-  } else {
+  if (ADJ) {
     cur = S.L + (long long)((t + 1) & 1) * S.fstride;
     out = S.L + (long long)(t & 1) * S.fstride;
     vin = S.Mu;
     vout = S.Mu;
     fwdu = S.ring + (long long)(t + 1 - seg * S.k) * S.fstride;
+  } else if (act == A_FWD) {
+    cur = fwd_b(S, t); vin = fwd_v(S, t);
+    out = (float*)fwd_b(S, t + 1); vout = (float*)fwd_v(S, t + 1);
+  } else if (act == A_FINAL) {
+    cur = fwd_b(S, t);
+  } else {
+    cur = rep_b(S, seg, t); vin = rep_v(S, seg, t);
+    out = (float*)rep_b(S, seg, t + 1); vout = (float*)rep_v(S, seg, t + 1);
   }
-  const int nload = final_only ? 1 : nfloat;
+  const float* const c2p = S.c2;
+  double* const gradp = S.grad;
+  const float* const tzp = S.tz;
+  const int nload = final_only ? 1 : NF;
 
   if (tid == 0) {
-    for (int s2 = 0; s2 < nst; ++s2) mbar_init(bars + s2, 1);
+    for (int s2 = 0; s2 < NST; ++s2) mbar_init(bars + s2, 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   for (int i = tid; i < NP * NP; i += NT) sD[i] = S.D[i];
-  for (int i = tid; i < NP; i += NT) sB[i] = S.beta[i];
+  if (tid < NP) sB[tid] = S.beta[tid];
   __syncthreads();
 
-  // TMA: element row `ez` of every field into ring slot ez % nst (warp 0: lane 0
-  // posts the expected bytes, then each lane issues row copies)
+  // TMA: element row `ez` of every field into ring slot ez % NST (warp 0: lane 0 posts
+  // the expected bytes, then each lane issues row copies)
   auto issue = [&](int ez) {
-    const int slot = ez % nst;
+    const int slot = ez % NST;
     float* st = stages + slot * stage_f;
     const unsigned rowb = (unsigned)(ce - cs) * 4u;
-    const int nd = (ndouble && !final_only) ? NP : 0;
+    const int nd = ADJ ? NP : 0;
     const int ncopy = nload * NP + nd;
     if (lane == 0) mbar_expect_tx(bars + slot, (unsigned)(nload * NP) * rowb + (unsigned)nd * rowb * 2u);
     __syncwarp();
     for (int q = lane; q < ncopy; q += 32) {
       if (q < nload * NP) {
         const int f = q / NP, a = q - f * NP;
-        const float* base = (f == 0) ? cur : (f == 1) ? S.c2 : (f == 2) ? vin : fwdu;
-        bulk_load(st + (f * NP + a) * BW + (cs - X0), base + (long long)(ez * N + a) * S.pitch + cs,
+        const float* base = (f == 0) ? cur : (f == 1) ? c2p : (f == 2) ? vin : fwdu;
+        bulk_load(st + (f * NP + a) * BW + (cs - X0), base + (long long)(ez * N + a) * pitch + cs,
                   rowb, bars + slot);
       } else {
         const int a = q - nload * NP;
-        double* gs = reinterpret_cast<double*>(st + nfloat * NP * BW);
-        bulk_load(gs + a * BW + (cs - X0), S.grad + (long long)(ez * N + a) * S.pitch + cs,
+        double* gs = reinterpret_cast<double*>(st + NF * NP * BW);
+        bulk_load(gs + a * BW + (cs - X0), gradp + (long long)(ez * N + a) * pitch + cs,
                   rowb * 2u, bars + slot);
       }
     }
   };
+  int issued = min(NST, nelz);  // bands whose copies have been issued (same in every thread)
   if (warp == 0)
-    for (int ez = 0; ez < min(nst, S.nelz); ++ez) issue(ez);
+    for (int ez = 0; ez < issued; ++ez) issue(ez);
 
   // D and beta in registers (uniform across threads)
   float Dr[NP][NP], Bt[NP];
@@ -757,39 +771,72 @@ __global__ void __launch_bounds__(kStripCols) sem_strip_kernel(const SolveDev* _
     for (int b = 0; b < NP; ++b) Dr[a][b] = sD[a * NP + b];
   }
   float ixv = 0.f, Rxv = 0.f, dxv = 0.f;
-  if (owned) { ixv = __ldg(S.tx + gx); Rxv = __ldg(S.tx + S.nxg + gx); dxv = __ldg(S.tx + 2 * S.nxg + gx); }
+  if (owned) { ixv = __ldg(S.tx + gx); Rxv = __ldg(S.tx + nxg + gx); dxv = __ldg(S.tx + 2 * nxg + gx); }
+  // this column's x-segment results: its element's segment at local index ia, or on an
+  // element edge the left segment's last and the right segment's first entries
   const int e_r = gx / N, ia = gx - e_r * N;
-  const int s_r = e_r - e0 + 1;                 // x-segment index of this column's right segment
-  const bool damp = (act != A_ADJ) || (S.flags & F_EXACT);
-  const bool grad_on = adj && t >= S.it0 && t < S.it1;
-  const bool in_win = adj && t >= S.it0 && t < S.it1 && ((t - S.it0) % S.decim) == 0;
+  const int s_r = e_r - e0 + 1;
+  const bool edge = (ia == 0);
+  const bool hasL = edge && e_r >= 1;
+  const bool hasR0 = e_r < nelx;
+  const int xoR = s_r * NP + ia;
+  const int xoL = (s_r - 1) * NP + N;
+  // x-line items: rows 0..N-1 of each band as (row tid / nseg, segment tid % nseg), which
+  // fits one item per thread; row N of the last band by threads tid < nseg
+  const int xa = tid / nseg, xsg = tid - xa * nseg;
+  const bool xitem = (xa < N) && (xsg >= seg0);
+  const bool xitem_last = (tid < nseg) && (tid >= seg0);
+
+  const bool damp = !ADJ || (S.flags & F_EXACT);
+  const bool grad_on = ADJ && t >= S.it0 && t < S.it1;
+  const bool in_win = ADJ && t >= S.it0 && t < S.it1 && ((t - S.it0) % S.decim) == 0;
   const int ms = t - ((S.flags & F_SHIFT) ? 1 : 0);
-  const bool rec_on = (act == A_FWD || act == A_FINAL) && ms >= 0 && ms < S.nt;
-  if (adj && in_win)
+  const bool rec_on = !ADJ && (act == A_FWD || act == A_FINAL) && ms >= 0 && ms < S.nt;
+  // the source column's thread adds the source term on the source row
+  const int src_row = (!ADJ && !final_only && owned && gx == S.src_gx) ? S.src_gz : -1;
+  const float src_val = (src_row >= 0) ? S.src_term[t] : 0.f;
+  if (ADJ && in_win)
     for (int i = tid; i < NP * NT; i += NT) sacc[i] = 0.f;
+  // receiver / injection list bounds of the current band, fetched one band ahead
+  const int li0 = strip * nelz;
+  int rec_lo = 0, rec_hi = 0, inj_lo = 0, inj_hi = 0;
+  if (rec_on) { rec_lo = S.rec_tile_off[li0]; rec_hi = S.rec_tile_off[li0 + 1]; }
+  if (ADJ && in_win) { inj_lo = S.inj_tile_off[li0]; inj_hi = S.inj_tile_off[li0 + 1]; }
+
   float zc = 0.f, szc = 0.f;  // z-line carries into the next band's first row
   bool bad = false;
   int abort_ez = -1;
+  int gb = gx;                // offset of (row ez * N, column gx) in a field
 
-  for (int ez = 0; ez < S.nelz; ++ez) {
-    const int slot = ez % nst;
+  for (int ez = 0; ez < nelz; ++ez, gb += N * pitch) {
+    const int slot = ez % NST;
     const float* st = stages + slot * stage_f;
     const float* Bs = st;
     const float* Cs = st + NP * BW;
     const float* Vs = st + 2 * NP * BW;
     const float* Us = st + 3 * NP * BW;
-    const double* Gs = reinterpret_cast<const double*>(st + nfloat * NP * BW);
-    if (!mbar_wait(bars + slot, (unsigned)((ez / nst) & 1))) s_abort = 1;
-    __syncthreads();
-    if (s_abort) { abort_ez = ez; break; }
-    const bool last = (ez == S.nelz - 1);
-    const int rows = last ? NP : N;
+    const double* Gs = reinterpret_cast<const double*>(st + NF * NP * BW);
+    float* const Xs = xs0 + (SEM_ONE_BARRIER ? (ez & 1) : 0) * XSZ;
+    float* const SXs = Xs + NP * SEGS * NP;
+    float* const tzb = sTz + (ez & 1) * 24;
+    const int r0 = rec_lo, r1 = rec_hi, j0 = inj_lo, j1 = inj_hi;
+    if (ez + 1 < nelz) {
+      if (rec_on) { rec_lo = rec_hi; rec_hi = S.rec_tile_off[li0 + ez + 2]; }
+      if (ADJ && in_win) { inj_lo = inj_hi; inj_hi = S.inj_tile_off[li0 + ez + 2]; }
+    }
+    if (!final_only && tid < 3 * NP) {  // the band's rows of the z tables
+      const int k = tid / NP, a = tid - k * NP;
+      tzb[k * 8 + a] = __ldg(tzp + k * nzg + ez * N + a);
+    }
+    // a failed wait records the first band that failed; every thread tests "failed at or
+    // before this band" after the band's barrier, so all threads leave at the same band
+    if (!mbar_wait(bars + slot, (unsigned)((ez / NST) & 1))) atomicMin(s_abort, ez);
+    const bool last = (ez == nelz - 1);
 
     if (rec_on) {  // receivers read out of this band, one warp each
-      const int li = strip * S.nelz + ez;
-      const int off0 = S.rec_tile_off[li], cnt = S.rec_tile_off[li + 1] - off0;
+      const int cnt = r1 - r0;
       for (int q = warp; q < cnt; q += NT / 32) {
-        const int r = S.rec_tile_ids[off0 + q];
+        const int r = S.rec_tile_ids[r0 + q];
         const int bx = S.rec_base[2 * r];
         const float* wr = S.rec_w + (long long)r * NP * NP;
         float acc = 0.f;
@@ -810,50 +857,44 @@ __global__ void __launch_bounds__(kStripCols) sem_strip_kernel(const SolveDev* _
       }
     }
     if (!final_only) {
-      if (in_win) {  // adjoint source of receivers in this element row
-        const int li = strip * S.nelz + ez;
-        const int off0 = S.inj_tile_off[li], cnt = S.inj_tile_off[li + 1] - off0;
-        if (cnt > 0) {
-          const double ascale = *S.adj_scale;
-          const long long yrow = (long long)((t - S.it0) / S.decim) * S.nrec;
-          for (int q = tid; q < cnt; q += NT) {
-            const int r = S.inj_tile_ids[off0 + q];
-            const double res = (double)S.rec_out[(long long)t * S.nrec + r] - S.yobs[yrow + r];
-            sres[q] = (float)(res * ascale);
-          }
-          __syncthreads();
-          if (warp == 0) {
-            for (int q = 0; q < cnt; ++q) {
-              const int r = S.inj_tile_ids[off0 + q];
-              const float rs = sres[q];
-              const int bx = S.rec_base[2 * r];
-              const float* wr = S.rec_w + (long long)r * NP * NP;
-              for (int e = lane; e < NP * NP; e += 32) {
-                const int j = e / NP, i = e - j * NP;
-                const int gxx = bx + i;
-                if (gxx >= sx0 && gxx < so1) sacc[j * NT + (gxx - sx0)] += wr[e] * rs;
-              }
-              __syncwarp();
+      if (ADJ && in_win && j1 > j0) {  // adjoint source of receivers in this element row
+        const int cnt = j1 - j0;
+        const double ascale = *S.adj_scale;
+        const long long yrow = (long long)((t - S.it0) / S.decim) * S.nrec;
+        for (int q = tid; q < cnt; q += NT) {
+          const int r = S.inj_tile_ids[j0 + q];
+          const double res = (double)S.rec_out[(long long)t * S.nrec + r] - S.yobs[yrow + r];
+          sres[q] = (float)(res * ascale);
+        }
+        __syncthreads();
+        if (warp == 0) {
+          for (int q = 0; q < cnt; ++q) {
+            const int r = S.inj_tile_ids[j0 + q];
+            const float rs = sres[q];
+            const int bx = S.rec_base[2 * r];
+            const float* wr = S.rec_w + (long long)r * NP * NP;
+            for (int e = lane; e < NP * NP; e += 32) {
+              const int j = e / NP, i = e - j * NP;
+              const int gxx = bx + i;
+              if (gxx >= sx0 && gxx < so1) sacc[j * NT + (gxx - sx0)] += wr[e] * rs;
             }
+            __syncwarp();
           }
         }
       }
       // ---- phase A, x-lines: one thread per (band row, element segment)
-      for (int w = tid; w < rows * nseg; w += NT) {
-        const int a = w / nseg, sgi = w - a * nseg;
-        if (sgi < seg0) continue;
-        const float* ub = Bs + a * BW + off + sgi * N;  // column (e0-1+sgi)*N
-        const float* cb = Cs + a * BW + off + sgi * N;
-        float u[NP], du[NP], q[NP];
-#pragma unroll
-        for (int b = 0; b < NP; ++b) u[b] = ub[b];
+      auto xline = [&](int a, int sgi) {
+        const int o = a * BW + off + sgi * N;  // column (e0 - 1 + sgi) * N of row a
+        float u[NP], c[NP], du[NP], q[NP];
+        load_seg<N>(Bs + o, u);
+        load_seg<N>(Cs + o, c);
 #pragma unroll
         for (int a2 = 0; a2 < NP; ++a2) {
           float v = 0.f;
 #pragma unroll
           for (int b = 0; b < NP; ++b) v = fmaf(Dr[a2][b], u[b], v);
           du[a2] = v;
-          q[a2] = Bt[a2] * cb[a2] * v;
+          q[a2] = Bt[a2] * c[a2] * v;
         }
         float* xo = Xs + (a * SEGS + sgi) * NP;
 #pragma unroll
@@ -863,10 +904,8 @@ __global__ void __launch_bounds__(kStripCols) sem_strip_kernel(const SolveDev* _
           for (int a2 = 0; a2 < NP; ++a2) v = fmaf(Dr[a2][i], q[a2], v);
           xo[i] = v;
         }
-        if (adj) {
-          const float* wb = Us + a * BW + off + sgi * N;
-#pragma unroll
-          for (int b = 0; b < NP; ++b) u[b] = wb[b];
+        if (ADJ) {
+          load_seg<N>(Us + o, u);
           float* so = SXs + (a * SEGS + sgi) * NP;
 #pragma unroll
           for (int a2 = 0; a2 < NP; ++a2) {
@@ -876,7 +915,9 @@ __global__ void __launch_bounds__(kStripCols) sem_strip_kernel(const SolveDev* _
             so[a2] = Bt[a2] * v * du[a2];
           }
         }
-      }
+      };
+      if (xitem) xline(xa, xsg);
+      if (last && xitem_last) xline(N, tid);
       // ---- phase A, z-lines: one thread per owned column (the band is the segment)
       float rz[NP], sz[NP];
       if (owned) {
@@ -898,7 +939,7 @@ __global__ void __launch_bounds__(kStripCols) sem_strip_kernel(const SolveDev* _
           for (int a2 = 0; a2 < NP; ++a2) v = fmaf(Dr[a2][j], q[a2], v);
           rz[j] = v;
         }
-        if (adj) {
+        if (ADJ) {
 #pragma unroll
           for (int b = 0; b < NP; ++b) u[b] = Us[b * BW + sc];
 #pragma unroll
@@ -911,25 +952,34 @@ __global__ void __launch_bounds__(kStripCols) sem_strip_kernel(const SolveDev* _
         }
       }
       __syncthreads();
+      if (*s_abort <= ez) { abort_ez = ez; break; }
+#if SEM_ONE_BARRIER
+      // every thread is past phase B of band ez - 1: its ring slot is free
+      if (ez >= 1 && ez - 1 + NST < nelz) {
+        if (warp == 0) issue(ez - 1 + NST);
+        ++issued;
+      }
+#endif
       // ---- phase B: combine and advance the owned nodes of the band, row by row
       if (owned) {
 #pragma unroll
         for (int a = 0; a < NP; ++a) {
           if (a == N && !last) break;
           const float* xr = Xs + a * SEGS * NP;
+          const float* sxr = SXs + a * SEGS * NP;
           float X, SX = 0.f;
-          if (ia) {
-            X = xr[s_r * NP + ia];
-            if (adj) SX = SXs[a * SEGS * NP + s_r * NP + ia];
+          if (!edge) {
+            X = xr[xoR];
+            if (ADJ) SX = sxr[xoR];
           } else {
             X = 0.f;
-            if (e_r >= 1) {
-              X = xr[(s_r - 1) * NP + N];
-              if (adj) SX = SXs[a * SEGS * NP + (s_r - 1) * NP + N];
+            if (hasL) {
+              X = xr[xoL];
+              if (ADJ) SX = sxr[xoL];
             }
-            if (e_r < S.nelx) {
-              X += xr[s_r * NP];
-              if (adj) SX += SXs[a * SEGS * NP + s_r * NP];
+            if (hasR0) {
+              X += xr[xoR];
+              if (ADJ) SX += sxr[xoR];
             }
           }
           float Z, SZ = 0.f;
@@ -937,31 +987,30 @@ __global__ void __launch_bounds__(kStripCols) sem_strip_kernel(const SolveDev* _
             Z = 0.f;
             if (ez >= 1) Z = zc;
             Z += rz[0];
-            if (adj) { if (ez >= 1) SZ = szc; SZ += sz[0]; }
+            if (ADJ) { if (ez >= 1) SZ = szc; SZ += sz[0]; }
           } else {
             Z = rz[a];
-            if (adj) SZ = sz[a];
+            if (ADJ) SZ = sz[a];
           }
-          const int gz = ez * N + a;
-          const float izv = __ldg(S.tz + gz), Rzv = __ldg(S.tz + S.nzg + gz), dzv = __ldg(S.tz + 2 * S.nzg + gz);
-          const long long g = (long long)gz * S.pitch + gx;
-          float extra = 0.f;
-          if (!adj) {
-            if (gx == S.src_gx && gz == S.src_gz) extra = S.src_term[t];
+          const float izv = tzb[a], Rzv = tzb[8 + a], dzv = tzb[16 + a];
+          const int g = gb + a * pitch;
+          float extra;
+          if (!ADJ) {
+            extra = (ez * N + a == src_row) ? src_val : 0.f;
           } else {
             extra = in_win ? sacc[a * NT + tid] : 0.f;
-            if (grad_on) S.grad[g] = Gs[a * BW + sc] + (double)(Rzv * SX + Rxv * SZ);
+            if (grad_on) gradp[g] = Gs[a * BW + sc] + (double)(Rzv * SX + Rxv * SZ);
           }
           float res, vres;
-          advance_node(adj, damp, Bs[a * BW + sc], Vs[a * BW + sc], X, Z, ixv, Rxv, dxv, izv, Rzv,
+          advance_node(ADJ, damp, Bs[a * BW + sc], Vs[a * BW + sc], X, Z, ixv, Rxv, dxv, izv, Rzv,
                        dzv, extra, res, vres);
           out[g] = res;
           vout[g] = vres;
           bad |= !isfinite(res);
         }
         zc = rz[N];
-        if (adj) szc = sz[N];
-        if (adj && in_win) {  // carry the injection row shared with the next band
+        if (ADJ) szc = sz[N];
+        if (ADJ && in_win) {  // carry the injection row shared with the next band
           const float carry = sacc[N * NT + tid];
 #pragma unroll
           for (int a = 1; a < NP; ++a) sacc[a * NT + tid] = 0.f;
@@ -969,16 +1018,60 @@ __global__ void __launch_bounds__(kStripCols) sem_strip_kernel(const SolveDev* _
         }
       }
     }
-    __syncthreads();  // done with this slot and the exchange arrays
-    if (warp == 0 && ez + nst < S.nelz) issue(ez + nst);
+    if (!SEM_ONE_BARRIER || final_only) {
+      __syncthreads();  // done with this slot and the exchange arrays
+      if (final_only && *s_abort <= ez) { abort_ez = ez; break; }
+      if (ez + NST < nelz) {
+        if (warp == 0) issue(ez + NST);
+        ++issued;
+      }
+    }
   }
   if (abort_ez >= 0) {
+    // drain the copies still in flight (bands abort_ez .. issued - 1) before leaving
     if (tid == 0) atomicOr(S.status, SEM_ERR_TIMEOUT);
-    for (int b = abort_ez; b < min(abort_ez + nst, S.nelz); ++b)
-      mbar_wait(bars + b % nst, (unsigned)((b / nst) & 1));
+    for (int b = abort_ez; b < issued; ++b) mbar_wait(bars + b % NST, (unsigned)((b / NST) & 1));
     return;
   }
   if (__any_sync(0xffffffffu, bad) && lane == 0) atomicOr(S.status, SEM_ERR_NONFINITE);
+}
+
+template <int N>
+__global__ void __launch_bounds__(kStripCols, (N <= 4) ? SEM_STRIP_MIN_BLOCKS : 4)
+    sem_strip_kernel(const SolveDev* __restrict__ solves, const int* __restrict__ cta_solve,
+                     const int* __restrict__ tick_ptr, int unused0, int unused1) {
+  extern __shared__ __align__(128) float smem[];
+  __shared__ SolveDev S;
+  __shared__ int s_act, s_t, s_seg, s_abort;
+
+  const int sid = cta_solve[blockIdx.x];
+  {
+    const unsigned long long* src = reinterpret_cast<const unsigned long long*>(solves + sid);
+    unsigned long long* dst = reinterpret_cast<unsigned long long*>(&S);
+    for (int i = threadIdx.x; i < (int)(sizeof(SolveDev) / 8); i += kStripCols) dst[i] = src[i];
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int act, t, seg;
+    decode(S, *tick_ptr - S.start_tick, act, t, seg);
+    s_act = act; s_t = t; s_seg = seg; s_abort = 0x7fffffff;
+  }
+  __syncthreads();
+  const int act = s_act;
+  if (act == A_NONE) return;
+  const int t = s_t, seg = s_seg;
+  if (act == A_SCALE) {
+    if (blockIdx.x == S.tile_base && threadIdx.x == 0) {
+      double m = 0.0;
+      for (int r = 0; r < S.nrec; ++r) m = fmax(m, S.rmax[r]);
+      *S.adj_scale = (m > 0.0 && isfinite(m)) ? ldexp(1.0, -ilogb(m)) : 1.0;
+    }
+    return;
+  }
+  if (act == A_ADJ)
+    strip_tick<N, true>(S, act, t, seg, smem, &s_abort);
+  else
+    strip_tick<N, false>(S, act, t, seg, smem, &s_abort);
 }
 
 __global__ void tick_advance_kernel(int* tick) { *tick += 1; }
@@ -1242,6 +1335,9 @@ int sem_plan_create(const sem_plan_desc_t* d, sem_plan_t** out) {
     return fail(SEM_ERR_ARG, "bad mesh / nt / nrec");
   const int nxg = d->nelx * d->npol + 1, nzg = d->nelz * d->npol + 1;
   if ((long long)nxg * nzg != d->npoints) return fail(SEM_ERR_ARG, "npoints != nxg*nzg");
+  // node offsets within a field are 32-bit in the kernels
+  if ((long long)round_up(nxg, 32) * nzg >= (1LL << 31) - 64)
+    return fail(SEM_ERR_UNSUPPORTED, "mesh too large: a field must hold fewer than 2^31 nodes");
   if (d->src_gx < 0 || d->src_gx >= nxg || d->src_gz < 0 || d->src_gz >= nzg)
     return fail(SEM_ERR_ARG, "source node outside the mesh");
   auto* p = new sem_plan_s();

@@ -1,7 +1,9 @@
-"""CPU audit of the strip kernel's index arithmetic (mirrors sem_strip_kernel in
+"""CPU audit of the strip kernel's index arithmetic (mirrors strip_tick in
 sem_kernels.cu): TMA copy ranges and alignment, shared-memory reads inside the copied
-columns, phase-B flux reads only where phase A wrote, exact partition of the owned
-columns, and coverage of the per-band receiver lists."""
+columns, the thread-to-x-item map (every (row, segment) item exactly once), 16-byte
+aligned segment loads for N = 4, phase-B flux reads only where phase A wrote, exact
+partition of the owned columns, shared-memory totals, and coverage of the per-band
+receiver lists."""
 import numpy as np
 import pytest
 
@@ -50,12 +52,28 @@ def audit(N, nelx, nelz):
         nseg = e1 - e0 + 1
         seg0 = 1 if e0 == 0 else 0
         assert nseg <= SEGS
+        if N == 4:
+            assert off == 0                  # segment starts on 4-float boundaries (float4)
+        # x-items: thread tid -> (row tid // nseg, segment tid % nseg) for rows 0..N-1;
+        # row N of the last band by threads tid < nseg
+        items = []
+        for tid in range(THREADS):
+            xa, xsg = divmod(tid, nseg)
+            if xa < N and xsg >= seg0:
+                items.append((xa, xsg))
+            if tid < nseg and tid >= seg0:
+                items.append((N, tid))
+        assert sorted(items) == [(a, g) for a in range(NP) for g in range(seg0, nseg)]
         written = set()
-        for sgi in range(seg0, nseg):        # phase A x-items read the segment's columns
+        for a, sgi in items:                 # phase A x-items read the segment's columns
+            o = a * BW + off + sgi * N
+            if N == 4:
+                assert o % 4 == 0
             for b in range(NP):
                 sm_col = off + sgi * N + b
                 assert 0 <= sm_col < BW
                 assert X0 + sm_col in copied
+            assert (a * SEGS + sgi) * NP + N < NP * SEGS * NP   # exchange buffer bound
             written.add(sgi)
         assert so1 - sx0 <= THREADS
         for tid in range(THREADS):
@@ -70,6 +88,47 @@ def audit(N, nelx, nelz):
             need = [s_r] if ia else ([s_r - 1] if er >= 1 else []) + ([s_r] if er < nelx else [])
             assert need and all(x in written for x in need), (strip, gx)
     assert (owner == 1).all()
+
+
+STAGES, STAGES_ADJ, INJ, HDR, NBUF = 3, 2, 256, 192, 2
+
+
+def smem_bytes(N, adj):
+    """strip_smem_floats(N, adj) * 4: header, ring slots, exchange buffers, injection."""
+    NP, segs = N + 1, ew_max(N) + 1
+
+    def stage(a):
+        return (((4 if a else 3) + (2 if a else 0)) * NP * bw(N) + 31) & ~31
+
+    def xch(a):
+        f = NBUF * (2 if a else 1) * NP * segs * NP + ((NP * THREADS + INJ) if a else 0)
+        return (f + 31) & ~31
+
+    fwd = STAGES * stage(False) + xch(False)
+    adjf = STAGES_ADJ * stage(True) + xch(True)
+    return 4 * (HDR + (max(fwd, adjf) if adj else fwd))
+
+
+@pytest.mark.parametrize("N", [1, 2, 3, 4, 5, 6, 7])
+def test_strip_shared_memory_layout(N):
+    # header: 64 floats of mbarriers (>= ring slots), D (NP^2 <= 64), beta (<= 16),
+    # z-table rows [2][3][8] (NP <= 8); ring starts 128-byte aligned
+    assert max(STAGES, STAGES_ADJ) * 2 <= 64 and (N + 1) ** 2 <= 64 and N + 1 <= 8
+    assert 64 + 64 + 16 + 48 == HDR and (HDR * 4) % 128 == 0
+    assert 3 * (N + 1) <= THREADS          # threads staging the z-table rows
+    for adj in (False, True):
+        assert smem_bytes(N, adj) + 1024 <= 227 * 1024
+    if N <= 4:                             # four CTAs per SM on the 228 KB SM
+        assert 4 * (smem_bytes(N, True) + 1024 + 1024) <= 228 * 1024
+
+
+def test_field_offsets_fit_int32():
+    # plans whose padded field reaches 2^31 floats are refused (kernels use int offsets)
+    for N, nelx, nelz in ((4, 100, 50), (7, 2000, 2000), (4, 8000, 8000)):
+        nxg, nzg = nelx * N + 1, nelz * N + 1
+        ok = pitch_of(nxg) * nzg < (1 << 31) - 64
+        if ok:
+            assert (nzg - 1) * pitch_of(nxg) + nxg < 2 ** 31
 
 
 @pytest.mark.parametrize("N", [1, 2, 3, 4, 5, 6, 7])
