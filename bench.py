@@ -454,6 +454,7 @@ def main():
     stream.synchronize()
     launches_per_step = batch.last_launches
     kernel_used = batch.last_kernel
+    groups_used = batch.last_groups
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     step_ms = []
     clocks = Clocks(os.path.join(HERE, "gpurun_out", f"clocks_r{rank}.csv") if os.path.isdir(
@@ -543,6 +544,7 @@ def main():
                                    "3000 steps, 100 receivers)",
                        "models_per_gpu": n, "nodes": W["npoints"], "nt": W["nt"],
                        "kernel": kernel_used, "tile": args.tile, "graph_chunk": args.graph_chunk,
+                       "ckpt_k": args.ckpt_k or "auto", "groups": groups_used,
                        "l2": "inputs larger than L2 (state+c2 of 256 models ~250 MB per field set)",
                        "parallelism": f"replicas x{world}"},
             "plain": {"value": plain_value, "unit": "solves/s", "kernel": plain_kernel,

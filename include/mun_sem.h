@@ -78,7 +78,8 @@ typedef struct {
   const sem_plan_t* plan;
   const double* velocity;   /* [npoints] nodal velocity, reference node order         */
   int32_t flags;            /* SEM_F_*                                                */
-  int32_t ckpt_k;           /* checkpoint interval for the adjoint replay (>=2)       */
+  int32_t ckpt_k;           /* checkpoint interval for the adjoint replay (>=2); 0 =
+                               automatic (see sem_launch_cfg_t.memory_budget)          */
   const double* y_obs;      /* [n_obs*nrec] observations on the misfit grid or NULL   */
   int32_t it0, it1, decim;  /* misfit window [it0,it1) and decimation (0,nt,1 = all)  */
   double inv_sigma2;        /* 1/(sigma^2 + 1e-24)                                    */
@@ -98,6 +99,13 @@ typedef struct {
                                  2 strip kernel (one CTA per full-height strip, TMA-
                                  staged element-row bands); auto picks strips when the
                                  batch has at least one strip per SM                   */
+  int32_t reserved;           /* must be 0                                             */
+  int64_t memory_budget;      /* device bytes the workspaces of solves with ckpt_k = 0
+                                 may use; 0 = 85% of (free + this batch's arena) less
+                                 512 MiB.  Such batches run as consecutive groups, each
+                                 with the largest checkpoint interval that fits (no
+                                 replay when k = nt), the split chosen by a tick-cost
+                                 model; results do not depend on the split            */
 } sem_launch_cfg_t;
 
 int sem_plan_create(const sem_plan_desc_t* desc, sem_plan_t** out);
@@ -113,6 +121,9 @@ int sem_run(sem_batch_t* batch, const sem_solve_t* solves, int32_t n,
             const sem_launch_cfg_t* cfg, void* stream);
 /* number of kernel launches issued by the last sem_run (for accounting) */
 int64_t sem_batch_last_launches(const sem_batch_t* batch);
+/* number of consecutive groups the last sem_run ran (1 unless ckpt_k = 0 solves were
+ * split under the memory budget) */
+int32_t sem_batch_last_groups(const sem_batch_t* batch);
 /* kernel variant used by the last sem_run: 1 tile, 2 strip */
 int32_t sem_batch_last_kernel(const sem_batch_t* batch);
 

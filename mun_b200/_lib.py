@@ -35,7 +35,8 @@ class Solve(C.Structure):
 
 class LaunchCfg(C.Structure):
     _fields_ = [("tile_ex", C.c_int32), ("tile_ez", C.c_int32), ("threads", C.c_int32),
-                ("graph_chunk", C.c_int32), ("kernel", C.c_int32)]
+                ("graph_chunk", C.c_int32), ("kernel", C.c_int32), ("reserved", C.c_int32),
+                ("memory_budget", C.c_int64)]
 
 
 class CurveDesc(C.Structure):
@@ -52,7 +53,7 @@ class EngineCfg(C.Structure):
 
 EXPORTS = ["sem_plan_create", "sem_plan_destroy", "sem_plan_workspace_bytes", "sem_batch_create",
            "sem_batch_destroy", "sem_run", "sem_batch_last_launches", "sem_batch_last_kernel",
-           "sem_forward",
+           "sem_batch_last_groups", "sem_forward",
            "sem_forward_adjoint", "sem_forward_noalloc", "sem_engine_create", "sem_engine_destroy",
            "sem_engine_submit", "sem_engine_step", "sem_engine_status", "sem_engine_release",
            "sem_engine_stats", "sem_velocity_from_curve", "sem_velocity_last_error", "sem_last_error"]
@@ -88,6 +89,8 @@ def load(path=None):
     lib.sem_batch_last_launches.restype = i64
     lib.sem_batch_last_kernel.argtypes = [vp]
     lib.sem_batch_last_kernel.restype = i32
+    lib.sem_batch_last_groups.argtypes = [vp]
+    lib.sem_batch_last_groups.restype = i32
     lib.sem_forward.argtypes = [vp, vp, vp, vp, vp]
     lib.sem_forward_adjoint.argtypes = [vp, vp, vp, vp, dbl, i32, i32, vp, vp, vp, vp]
     lib.sem_forward_noalloc.argtypes = [vp, vp, vp, vp, vp]
@@ -103,7 +106,7 @@ def load(path=None):
     lib.sem_last_error.restype = C.c_char_p
     for name in EXPORTS:
         if name not in ("sem_plan_workspace_bytes", "sem_batch_last_launches", "sem_batch_last_kernel",
-                        "sem_last_error", "sem_velocity_last_error"):
+                        "sem_batch_last_groups", "sem_last_error", "sem_velocity_last_error"):
             getattr(lib, name).restype = C.c_int
     _lib = lib
     return lib

@@ -16,7 +16,7 @@ import numpy as np
 import torch
 
 from .bspline import grid_basis
-from .solver import Batch, SolveSpec, choose_ckpt_k
+from .solver import Batch, SolveSpec
 
 
 class SEMLikelihoodAdjointFn(torch.autograd.Function):
@@ -73,9 +73,8 @@ class GridLikelihood(torch.autograd.Function):
         v = model.velocity(theta)
         inv_s2 = 1.0 / (float(sigma) ** 2 + 1e-24)
         n = theta.shape[0]
-        k = ckpt_k or choose_ckpt_k(model.plan, n)
         specs = [SolveSpec(model.plan, v[i], adjoint=True, exact=exact, y_obs=y_obs,
-                           inv_sigma2=inv_s2, ckpt_k=k) for i in range(n)]
+                           inv_sigma2=inv_s2, ckpt_k=ckpt_k) for i in range(n)]
         (batch or Batch()).run(specs)
         st = torch.cat([s.status for s in specs])
         if bool((st != 0).any()):

@@ -1,8 +1,8 @@
 """Launch-configuration autotuner.
 
-Picks the kernel variant (tile kernel with a tile shape, or strip kernel), the CUDA-graph
-chunk and the checkpoint interval for a batch by timing candidates on a short proxy of
-the batch: the same meshes, orders, receivers and velocities with a few dozen time steps.
+Picks the kernel variant (tile kernel with a tile shape, or strip kernel) and the
+CUDA-graph chunk for a batch by timing candidates on a short proxy of the batch (the
+checkpoint interval and group split stay with the library's memory-budget schedule): the same meshes, orders, receivers and velocities with a few dozen time steps.
 The choice is cached per batch signature (mesh sizes, orders, solve count, adjoint or
 not).  Results never depend on the choice: every variant computes bitwise the same
 numbers, so tuning only moves time.
@@ -14,7 +14,7 @@ import time
 import torch
 
 from .plan import SEMPlan
-from .solver import Batch, SolveSpec, choose_ckpt_k
+from .solver import Batch, SolveSpec
 
 TILE_CANDIDATES = [(8, 8), (16, 8), (8, 4), (16, 4), (4, 4)]
 GRAPH_CANDIDATES = [0, 32]
@@ -79,18 +79,14 @@ def tune(specs, nt_proxy=48, repeats=2, candidates=None, verbose=False):
         if el < best_t:
             best_t, best = el, (kernel, tile, chunk)
     kernel, tile, chunk = best
-    k = choose_ckpt_k(specs[0].plan, len(specs)) if any(s.adjoint for s in specs) else 2
-    res = {"kernel": kernel, "tile": tile, "graph_chunk": chunk, "ckpt_k": k, "proxy_ms": 1e3 * best_t}
+    # ckpt_k 0: the library picks the checkpoint interval and group split at run time
+    res = {"kernel": kernel, "tile": tile, "graph_chunk": chunk, "ckpt_k": 0, "proxy_ms": 1e3 * best_t}
     _cache[key] = res
     return res
 
 
 def tuned_batch(specs, **kw):
-    """A ``Batch`` configured by ``tune`` plus the chosen checkpoint interval applied to
-    the specs."""
+    """A ``Batch`` configured by ``tune`` (checkpointing stays automatic)."""
     cfg = tune(specs, **kw)
-    for s in specs:
-        if s.adjoint and not s.ckpt_k:
-            s.ckpt_k = cfg["ckpt_k"]
     return Batch(tile=cfg["tile"] if cfg["kernel"] == 1 else (8, 8), graph_chunk=cfg["graph_chunk"],
                  kernel=cfg["kernel"]), cfg

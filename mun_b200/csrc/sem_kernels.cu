@@ -43,6 +43,7 @@
 #include <string.h>
 
 #include <algorithm>
+#include <cmath>
 #include <deque>
 #include <map>
 #include <mutex>
@@ -1320,6 +1321,7 @@ struct sem_batch_s {
   long long cta_cap = 0;
   long long last_launches = 0;
   int last_kernel = 0;
+  int last_groups = 0;
   std::vector<SolveDev> h_solves;
   std::vector<int> h_cta;
 };
@@ -1424,15 +1426,12 @@ int64_t sem_batch_last_launches(const sem_batch_t* b) { return b ? b->last_launc
 
 int32_t sem_batch_last_kernel(const sem_batch_t* b) { return b ? b->last_kernel : -1; }
 
-int sem_run(sem_batch_t* b, const sem_solve_t* solves, int32_t n, const sem_launch_cfg_t* cfg_in,
-            void* stream_v) {
-  if (!b || (!solves && n) || n < 0) return fail(SEM_ERR_ARG, "null argument");
-  cudaStream_t stream = (cudaStream_t)stream_v;
-  sem_launch_cfg_t cfg = cfg_in ? *cfg_in : sem_launch_cfg_t{8, 8, 256, 0, 0};
-  if (cfg.tile_ex < 1 || cfg.tile_ez < 1) return fail(SEM_ERR_ARG, "tile size must be >= 1");
-  if (cfg.kernel < 0 || cfg.kernel > 2) return fail(SEM_ERR_ARG, "kernel must be 0 (auto), 1 (tile), 2 (strip)");
-  if (cfg.threads < 32 || cfg.threads > 256 || cfg.threads % 32) cfg.threads = 256;
-  b->last_launches = 0;
+}  // extern "C"
+
+// One group of solves run to completion: the whole batch, or one group of an automatic
+// schedule (solves then carry the group's checkpoint interval).
+static int run_group(sem_batch_t* b, const sem_solve_t* solves, int32_t n,
+                     const sem_launch_cfg_t& cfg, cudaStream_t stream) {
   if (n == 0) return SEM_OK;
 
   // ---- validate and lay out workspaces
@@ -1673,6 +1672,171 @@ int sem_run(sem_batch_t* b, const sem_solve_t* solves, int32_t n, const sem_laun
   CUDA_TRY(cudaGetLastError());
   return SEM_OK;
 }
+
+namespace {
+
+// Time of one tick in units of the per-CTA work: CTAs beyond one resident wave queue
+// behind it, and each round costs a fixed latency part plus a part growing with the
+// CTAs resident per SM (the strip kernel's tick times fit 6.4 + CTAs/SM).
+double tick_rounds(long long ctas, long long slots, int sms) {
+  double c = 0.0;
+  for (long long left = ctas; left > 0; left -= slots)
+    c += 6.4 + (double)std::min(left, slots) / sms;
+  return c;
+}
+
+struct GroupPlan { int begin, end, k; };
+
+// Automatic schedule for solves with ckpt_k = 0: split the batch (in the caller's order)
+// into g consecutive groups of equal size run one after another, each with the largest
+// checkpoint interval whose workspace fits the memory budget (k = nt: no replay), and
+// pick the g with the smallest modelled time.  Explicit ckpt_k values are kept.
+int auto_schedule(const sem_solve_t* sv, int n, const sem_launch_cfg_t& cfg, long long budget,
+                  std::vector<GroupPlan>* out) {
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  // per-solve CTAs of either kernel and resident CTAs per SM (first solve's order)
+  std::vector<long long> strips(n), tiles(n);
+  for (int i = 0; i < n; ++i) {
+    const sem_plan_s* p = sv[i].plan;
+    const int ewm = strip_ew_max(p->npol);
+    strips[i] = (p->nelx + ewm - 1) / ewm;
+    int tx, tz;
+    tiles[i] = tiles_of(p, cfg.tile_ex, cfg.tile_ez, &tx, &tz);
+  }
+  bool any_adj = false;
+  for (int i = 0; i < n; ++i) any_adj |= (sv[i].flags & SEM_F_ADJOINT) != 0;
+  const int N0 = sv[0].plan->npol;
+  auto occupancy = [&](bool strip) -> long long {
+    KernelFn fn = strip ? strip_kernel_for(N0) : kernel_for(N0);
+    const size_t smem = (size_t)(strip ? strip_smem_floats(N0, any_adj)
+                                       : smem_floats(N0, cfg.tile_ex, cfg.tile_ez, any_adj)) * 4;
+    int nb = 1;
+    if (smem <= 227 * 1024 &&
+        cudaFuncSetAttribute((const void*)fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) == cudaSuccess &&
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, fn, strip ? strip_threads(N0) : cfg.threads, smem) ==
+            cudaSuccess)
+      nb = std::max(nb, 1);
+    else
+      nb = 1;
+    cudaGetLastError();
+    return (long long)nb * sms;
+  };
+  const long long slots_strip = occupancy(true), slots_tile = occupancy(false);
+
+  double best = -1.0;
+  std::vector<GroupPlan> best_plan;
+  const int gmax = std::min(n, 64);
+  for (int g = 1; g <= gmax; ++g) {
+    const int m = (n + g - 1) / g;
+    std::vector<GroupPlan> plan;
+    double cost = 0.0;
+    bool ok = true;
+    for (int b0 = 0; b0 < n && ok; b0 += m) {
+      const int b1 = std::min(n, b0 + m);
+      // largest common k for the automatic solves whose workspaces fit the budget
+      int nt_max = 2, k_floor = 2;
+      for (int i = b0; i < b1; ++i)
+        if ((sv[i].flags & SEM_F_ADJOINT) && sv[i].ckpt_k <= 0) {
+          nt_max = std::max(nt_max, sv[i].plan->nt);
+          k_floor = std::max(k_floor, std::min(sv[i].plan->nt, (int)std::sqrt(2.0 * sv[i].plan->nt)));
+        }
+      auto bytes_at = [&](int k) {
+        long long tot = 0;
+        int ns;
+        for (int i = b0; i < b1; ++i) {
+          const bool adj = sv[i].flags & SEM_F_ADJOINT;
+          const int ki = !adj ? 2 : (sv[i].ckpt_k > 0 ? sv[i].ckpt_k : std::min(k, sv[i].plan->nt));
+          tot += layout(sv[i].plan, sv[i].flags, std::max(2, std::min(ki, sv[i].plan->nt)), &ns).bytes;
+        }
+        return tot;
+      };
+      if (bytes_at(k_floor) > budget) { ok = false; break; }
+      int lo = k_floor, hi = nt_max;
+      while (lo < hi) {
+        const int mid = lo + (hi - lo + 1) / 2;
+        if (bytes_at(mid) <= budget) lo = mid; else hi = mid - 1;
+      }
+      const int k = lo;
+      // modelled time: forward-like ticks (forward + replay) and adjoint ticks (x1.5)
+      long long fwd_ticks = 0, adj_ticks = 0, nstrip = 0, ntile = 0;
+      for (int i = b0; i < b1; ++i) {
+        const sem_solve_t& s = sv[i];
+        const int nt = s.plan->nt;
+        const bool adj = s.flags & SEM_F_ADJOINT;
+        const int ki = std::max(2, std::min(adj ? (s.ckpt_k > 0 ? s.ckpt_k : k) : 2, nt));
+        const int nseg = (nt + ki - 1) / ki;
+        fwd_ticks = std::max(fwd_ticks, (long long)nt + 1 + (adj ? (long long)ki * (nseg - 1) : 0));
+        if (adj) adj_ticks = std::max(adj_ticks, (long long)nt);
+        nstrip += strips[i];
+        ntile += tiles[i];
+      }
+      const bool strip = cfg.kernel == 2 || (cfg.kernel == 0 && nstrip >= sms);
+      const double per_tick = strip ? tick_rounds(nstrip, slots_strip, sms) : tick_rounds(ntile, slots_tile, sms);
+      cost += per_tick * ((double)fwd_ticks + 1.5 * (double)adj_ticks);
+      plan.push_back(GroupPlan{b0, b1, k});
+    }
+    if (!ok) continue;
+    if (best < 0.0 || cost < 0.98 * best) { best = cost; best_plan = plan; }
+  }
+  if (best < 0.0) {  // nothing fits: one solve at a time with the smallest workspace
+    for (int i = 0; i < n; ++i) {
+      const int nt = sv[i].plan->nt;
+      best_plan.push_back(GroupPlan{i, i + 1, std::max(2, std::min(nt, (int)std::sqrt(2.0 * nt)))});
+    }
+  }
+  *out = best_plan;
+  return SEM_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int sem_run(sem_batch_t* b, const sem_solve_t* solves, int32_t n, const sem_launch_cfg_t* cfg_in,
+            void* stream_v) {
+  if (!b || (!solves && n) || n < 0) return fail(SEM_ERR_ARG, "null argument");
+  cudaStream_t stream = (cudaStream_t)stream_v;
+  sem_launch_cfg_t cfg = cfg_in ? *cfg_in : sem_launch_cfg_t{8, 8, 256, 0, 0, 0, 0};
+  if (cfg.tile_ex < 1 || cfg.tile_ez < 1) return fail(SEM_ERR_ARG, "tile size must be >= 1");
+  if (cfg.kernel < 0 || cfg.kernel > 2) return fail(SEM_ERR_ARG, "kernel must be 0 (auto), 1 (tile), 2 (strip)");
+  if (cfg.threads < 32 || cfg.threads > 256 || cfg.threads % 32) cfg.threads = 256;
+  if (cfg.memory_budget < 0) return fail(SEM_ERR_ARG, "memory_budget must be >= 0");
+  b->last_launches = 0;
+  b->last_groups = 0;
+  if (n == 0) return SEM_OK;
+  bool any_auto = false;
+  for (int i = 0; i < n; ++i) {
+    if (!solves[i].plan) return fail(SEM_ERR_ARG, "solve missing plan/velocity/rec_out");
+    any_auto |= (solves[i].flags & SEM_F_ADJOINT) && solves[i].ckpt_k <= 0;
+  }
+  if (!any_auto) {
+    b->last_groups = 1;
+    return run_group(b, solves, n, cfg, stream);
+  }
+  long long budget = cfg.memory_budget;
+  if (budget == 0) {
+    size_t fr = 0, tot = 0;
+    CUDA_TRY(cudaMemGetInfo(&fr, &tot));
+    budget = (long long)(0.85 * (double)((long long)fr + b->arena_bytes)) - (512LL << 20);
+    budget = std::max(budget, 1LL << 20);
+  }
+  std::vector<GroupPlan> groups;
+  int rc = auto_schedule(solves, n, cfg, budget, &groups);
+  if (rc) return rc;
+  std::vector<sem_solve_t> sv(solves, solves + n);
+  for (const GroupPlan& g : groups) {
+    for (int i = g.begin; i < g.end; ++i)
+      if ((sv[i].flags & SEM_F_ADJOINT) && sv[i].ckpt_k <= 0) sv[i].ckpt_k = g.k;
+    rc = run_group(b, sv.data() + g.begin, g.end - g.begin, cfg, stream);
+    if (rc) return rc;
+    b->last_groups++;
+  }
+  return SEM_OK;
+}
+
+int32_t sem_batch_last_groups(const sem_batch_t* b) { return b ? b->last_groups : -1; }
 
 int sem_forward_noalloc(const sem_plan_t* p, const double* velocity, float* rec_out,
                         int32_t* status_out, void* stream_v) {

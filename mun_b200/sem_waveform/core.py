@@ -26,7 +26,7 @@ import torch
 from .. import _lib
 from ..obs import align_observation, misfit_window
 from ..plan import SEMPlan
-from ..solver import Batch, SolveSpec, choose_ckpt_k
+from ..solver import Batch, SolveSpec
 from . import velocity as vel
 from .mesh import create_global_mesh, find_closest_node
 from .operators import precompute_sem_operators
@@ -424,10 +424,6 @@ class SEMSimulation:
                                        sigma * sigma + 1e-24, ckpt_k=ckpt_k)
             specs.append(sp)
             wins.append(win)
-        if ckpt_k == 0:
-            k = choose_ckpt_k(specs[0].plan, len(specs))
-            for sp in specs:
-                sp.ckpt_k = k
         self._get_batch().run(specs)
         self._check_status(specs)
         outs = []

@@ -24,7 +24,7 @@ class SolveSpec:
     y_obs: torch.Tensor = None   # (n_obs, nrec) float64 on the device, misfit grid
     window: tuple = None         # (it0, it1, decim)
     inv_sigma2: float = 1.0
-    ckpt_k: int = 0              # 0: choose from the memory budget
+    ckpt_k: int = 0              # 0: the library picks k and the group split (memory budget)
     rec: torch.Tensor = None     # outputs
     loglik: torch.Tensor = None
     grad: torch.Tensor = None
@@ -94,6 +94,12 @@ class Batch:
         return int(self._lib.sem_batch_last_launches(self.handle))
 
     @property
+    def last_groups(self):
+        """Consecutive groups the last run used (automatic checkpointing may split a
+        batch so that each group's forward history fits the memory budget)."""
+        return int(self._lib.sem_batch_last_groups(self.handle))
+
+    @property
     def last_kernel(self):
         return {1: "tile", 2: "strip"}.get(int(self._lib.sem_batch_last_kernel(self.handle)), "none")
 
@@ -135,7 +141,8 @@ class Batch:
                 s.grad = torch.empty(p.npoints, dtype=torch.float64, device=dev)
             if s.status is None:
                 s.status = torch.zeros(1, dtype=torch.int32, device=dev)
-            k = s.ckpt_k if s.ckpt_k else (choose_ckpt_k(p, n, memory_budget) if s.adjoint else 2)
+            # 0: the library picks the checkpoint interval and the group split
+            k = s.ckpt_k if s.ckpt_k else (0 if s.adjoint else 2)
             a = arr[i]
             a.plan = p.handle.value
             a.velocity = v.data_ptr()
@@ -151,7 +158,8 @@ class Batch:
         t = tile or self.tile
         cfg = _lib.LaunchCfg(int(t[0]), int(t[1]), self.threads,
                              int(self.graph_chunk if graph_chunk is None else graph_chunk),
-                             int(self.kernel if kernel is None else kernel))
+                             int(self.kernel if kernel is None else kernel), 0,
+                             int(memory_budget or 0))
         cur = torch.cuda.current_stream()
         if cfg.graph_chunk > 0 and cur.cuda_stream == 0:
             # graphs cannot be captured on the legacy default stream: use a side stream
