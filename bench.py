@@ -29,6 +29,13 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, HERE)
 
 BYTES_PER_NODE_STEP_FWDADJ = 56  # algorithmic bytes (float32 state, float64 gradient RMW)
+# bytes one tick moves per node in the strip kernel: forward / replay tick reads b, v, c^2
+# and writes b, v; adjoint tick reads lambda, mu, c^2, the forward b and the float64
+# gradient and writes lambda, mu and the gradient
+BYTES_PER_NODE_FWD_TICK = 20
+BYTES_PER_NODE_ADJ_TICK = 40
+# DRAM bytes per node measured by ncu for each tick kind (None: not measured)
+TRAFFIC_B_PER_NODE = None
 
 
 def workload(nmodels=256, nelx=100, nelz=50, nt=3000, nrec=100, seed0=0):
@@ -456,7 +463,7 @@ def main():
     kernel_used = batch.last_kernel
     groups_used = batch.last_groups
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    step_ms = []
+    step_ms, tick_ms = [], []
     clocks = Clocks(os.path.join(HERE, "gpurun_out", f"clocks_r{rank}.csv") if os.path.isdir(
         os.path.join(HERE, "gpurun_out")) else f"/tmp/clocks_r{rank}.csv")
     barrier()
@@ -469,9 +476,17 @@ def main():
                 ev1.record(stream)
             ev1.synchronize()
             step_ms.append(ev0.elapsed_time(ev1))
+            tick_ms.append(batch.last_tick_ms())
     torch.cuda.synchronize()
     barrier()
     ms = float(np.mean(step_ms))
+    ticks_per_step = batch.last_ticks
+    # node-ticks of each kind per step: every group runs nt adjoint ticks, a read-out and
+    # a scale tick; its remaining ticks are forward or replay ticks
+    fwd_like = ticks_per_step - groups_used * (W["nt"] + 2)
+    kern_bytes = W["npoints"] * (n // groups_used) * (
+        BYTES_PER_NODE_FWD_TICK * fwd_like + BYTES_PER_NODE_ADJ_TICK * groups_used * W["nt"])
+    tick_loop_ms = float(np.mean(tick_ms))
     if world > 1:
         t = torch.tensor([ms], device=dev)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
@@ -521,11 +536,19 @@ def main():
     plain_ms = np.array(plain_ms)
     plain_value = 1e3 / plain_ms.mean()
 
-    # ---------------- roofline of the dominant kernel (sem_tick_kernel<4>)
+    # ---------------- roofline of the dominant kernel (the tick kernel, one launch per tick)
     pk, pk_kind = peaks()
     alg_bytes = BYTES_PER_NODE_STEP_FWDADJ * W["npoints"] * W["nt"] * n
-    achieved = alg_bytes / (ms / 1e3) / 1e9
+    step_achieved = alg_bytes / (ms / 1e3) / 1e9
+    achieved = kern_bytes / (tick_loop_ms / 1e3) / 1e9
     peak = float(pk.get("hbm_gbs", 6650.0))
+    # DRAM traffic per node of each tick kind from the ncu capture of the strip kernel
+    # (16 models, scaled per node), averaged like the algorithmic bytes
+    traffic = None
+    if kernel_used == "strip" and TRAFFIC_B_PER_NODE:
+        traffic = W["npoints"] * (n // groups_used) * (
+            TRAFFIC_B_PER_NODE["fwd"] * fwd_like + TRAFFIC_B_PER_NODE["adj"] * groups_used * W["nt"]
+        ) / ticks_per_step
 
     cpu = None
     if rank == 0 and not args.no_cpu:
@@ -556,8 +579,18 @@ def main():
             "e2e": {"value": n * world / (e2e / 1e3), "unit": "solves/s", "h2d_bytes_per_step": int(h2d),
                     "d2h_bytes_per_step": int(d2h)},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": None, "peak_kind": pk_kind,
-                         "note": "56 B/node-step algorithmic over the whole step time (all launches)"},
+                         "frac": achieved / peak, "traffic": traffic, "peak_kind": pk_kind,
+                         "kernel": f"sem_{kernel_used}_kernel<4>",
+                         "bytes_per_node": {"forward_tick": BYTES_PER_NODE_FWD_TICK,
+                                            "adjoint_tick": BYTES_PER_NODE_ADJ_TICK},
+                         "launch_us_avg": 1e3 * tick_loop_ms / ticks_per_step,
+                         "ticks_per_step": ticks_per_step, "forward_like_ticks": fwd_like,
+                         "note": "algorithmic bytes of the step's tick launches over the CUDA-"
+                                 "event time of the tick loops (tick kernel + 1-thread tick "
+                                 "counter kernel per tick); traffic = ncu DRAM bytes per launch",
+                         "step_level": {"bytes_per_node_step": BYTES_PER_NODE_STEP_FWDADJ,
+                                        "achieved": step_achieved,
+                                        "frac": step_achieved / peak}},
             "cpu_baseline": cpu,
             "gpu_launches": int(launches_per_step * args.steps),
             "status": int(status),

@@ -124,6 +124,13 @@ int64_t sem_batch_last_launches(const sem_batch_t* batch);
 /* number of consecutive groups the last sem_run ran (1 unless ckpt_k = 0 solves were
  * split under the memory budget) */
 int32_t sem_batch_last_groups(const sem_batch_t* batch);
+/* tick rounds the last sem_run launched, summed over its groups (each round launches the
+ * tick kernel once per polynomial order, then the tick counter kernel) */
+int64_t sem_batch_last_ticks(const sem_batch_t* batch);
+/* device time of the last sem_run's tick loops (CUDA events recorded on its stream
+ * around each group's tick launches; set-up and output kernels excluded), in ms.
+ * Waits for those events. */
+int sem_batch_last_tick_ms(const sem_batch_t* batch, double* ms_out);
 /* kernel variant used by the last sem_run: 1 tile, 2 strip */
 int32_t sem_batch_last_kernel(const sem_batch_t* batch);
 

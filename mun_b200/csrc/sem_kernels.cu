@@ -554,9 +554,6 @@ __global__ void __launch_bounds__(256) sem_tick_kernel(const SolveDev* __restric
 #ifndef SEM_STRIP_MIN_BLOCKS
 #define SEM_STRIP_MIN_BLOCKS 4
 #endif
-#ifndef SEM_ONE_BARRIER
-#define SEM_ONE_BARRIER 1
-#endif
 #ifndef SEM_WAIT_HINT_NS
 #define SEM_WAIT_HINT_NS 20000
 #endif
@@ -625,6 +622,30 @@ __device__ __forceinline__ void bulk_load(void* dst, const void* src, unsigned b
       : "memory");
 }
 
+#ifndef SEM_TMA_STORE
+#define SEM_TMA_STORE 0
+#endif
+#ifndef SEM_ISSUE_LAST
+#define SEM_ISSUE_LAST 0
+#endif
+// shared -> global bulk copy (16-byte aligned addresses, size a multiple of 16)
+__device__ __forceinline__ void bulk_store(void* dst, const void* src, unsigned bytes) {
+  asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;" ::"l"(dst),
+               "r"(smem_addr(src)), "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
+// this thread's bulk stores have finished reading shared memory
+__device__ __forceinline__ void bulk_wait_read() {
+  asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
+}
+// this thread's bulk stores are complete
+__device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
+// generic-proxy shared-memory writes become visible to the async (bulk copy) proxy
+__device__ __forceinline__ void fence_proxy_async_smem() {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
 __host__ __device__ inline long long strip_stage_floats(int N, bool adj) {
   const int nfloat = adj ? 4 : 3;  // cur, c2, v (+ forward field)
   const int ndouble = adj ? 1 : 0;  // gradient accumulator
@@ -634,7 +655,7 @@ __host__ __device__ inline long long strip_stage_floats(int N, bool adj) {
 // results stay in registers; injection rows and residuals
 __host__ __device__ inline long long strip_xch_floats(int N, bool adj) {
   const long long NP = N + 1, segs = strip_ew_max(N) + 1;
-  const long long nb = SEM_ONE_BARRIER ? 2 : 1;                      // exchange buffers
+  const long long nb = 2;                                            // exchange buffers
   long long f = nb * (adj ? 2 : 1) * NP * segs * NP;                 // Xs | SXs (per buffer)
   if (adj) f += NP * kStripCols + kStripInj;                         // inj | res
   return (f + 31) & ~31LL;
@@ -645,13 +666,18 @@ __host__ __device__ inline long long strip_smem_floats(int N, bool adj) {
   return kStripHdr + (adj ? (fwd > adjf ? fwd : adjf) : fwd);
 }
 
-// Loads the N+1 consecutive floats of one x-line segment (16-byte aligned for N = 4,
-// where the strip's copy origin puts every element edge on a 4-float boundary).
+// Loads the N+1 consecutive floats of one x-line segment.  For N = 4 the strip's copy
+// origin puts every element edge on a 4-float boundary: one float4, and the shared edge
+// node comes from the next lane's first value when that lane holds the next segment of
+// the same row (`from_next`), else from shared memory.
 template <int N>
-__device__ __forceinline__ void load_seg(const float* p, float (&u)[N + 1]) {
+__device__ __forceinline__ void load_seg(const float* p, float (&u)[N + 1], unsigned mask,
+                                         bool from_next) {
   if constexpr (N == 4) {
     const float4 q = *reinterpret_cast<const float4*>(p);
-    u[0] = q.x; u[1] = q.y; u[2] = q.z; u[3] = q.w; u[4] = p[4];
+    u[0] = q.x; u[1] = q.y; u[2] = q.z; u[3] = q.w;
+    const float nx = __shfl_down_sync(mask, q.x, 1);
+    u[4] = from_next ? nx : p[4];
   } else {
 #pragma unroll
     for (int b = 0; b <= N; ++b) u[b] = p[b];
@@ -666,10 +692,10 @@ __device__ __forceinline__ void strip_tick(const SolveDev& S, const int act, con
   constexpr int NP = N + 1;
   constexpr int BW = (kStripCols + 3 + 3) & ~3;
   constexpr int NT = kStripCols;
+  constexpr int NW = NT / 32;
   constexpr int SEGS = (kStripCols - N - 1) / N + 1;  // x-segments per band row (max)
   constexpr int NF = ADJ ? 4 : 3;                      // staged float fields
   constexpr int NST = ADJ ? kStagesAdj : kStages;      // ring slots
-  constexpr int NBUF = SEM_ONE_BARRIER ? 2 : 1;        // exchange buffers
   constexpr int XSZ = (ADJ ? 2 : 1) * NP * SEGS * NP;  // floats of one exchange buffer
   const bool final_only = !ADJ && act == A_FINAL;
 
@@ -689,16 +715,21 @@ __device__ __forceinline__ void strip_tick(const SolveDev& S, const int act, con
   const int gx = sx0 + tid;                                 // this thread's owned column
   const bool owned = gx < so1;
   const int sc = tid + N + off;                             // its smem column
+  // owned columns [h0, h1) leave by bulk stores of whole rows from the ring slot (16-byte
+  // aligned on both sides); the rest by plain stores from the owner thread
+  const int h0 = SEM_TMA_STORE ? ((sx0 + 3) & ~3) : so1, h1 = SEM_TMA_STORE ? (so1 & ~3) : so1;
+  const bool by_bulk = SEM_TMA_STORE && h1 > h0 && gx >= h0 && gx < h1;
 
   // ---------------- shared memory
   unsigned long long* bars = reinterpret_cast<unsigned long long*>(smem);
+  int* const done = reinterpret_cast<int*>(smem + 32);      // per slot: warps past phase B
   float* const sD = smem + 64;
   float* const sB = sD + 64;
   float* const sTz = sB + 16;                     // [2][3][8] band rows of 1/mz, Rz, dz
   const long long stage_f = strip_stage_floats(N, ADJ);
   float* const stages = smem + kStripHdr;
-  float* const xs0 = stages + NST * stage_f;      // exchange: Xs [NP][SEGS][NP] (+ SXs)
-  float* const sacc = xs0 + NBUF * XSZ;           // adjoint: injection rows [NP][NT]
+  float* const xs0 = stages + NST * stage_f;      // 2 exchange buffers: Xs [NP][SEGS][NP] (+ SXs)
+  float* const sacc = xs0 + 2 * XSZ;              // adjoint: injection rows [NP][NT]
   float* const sres = sacc + NP * NT;             // adjoint: band residuals [kStripInj]
 
   // ---------------- which fields
@@ -728,14 +759,14 @@ __device__ __forceinline__ void strip_tick(const SolveDev& S, const int act, con
   const int nload = final_only ? 1 : NF;
 
   if (tid == 0) {
-    for (int s2 = 0; s2 < NST; ++s2) mbar_init(bars + s2, 1);
+    for (int s2 = 0; s2 < NST; ++s2) { mbar_init(bars + s2, 1); done[s2] = 0; }
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   for (int i = tid; i < NP * NP; i += NT) sD[i] = S.D[i];
   if (tid < NP) sB[tid] = S.beta[tid];
   __syncthreads();
 
-  // TMA: element row `ez` of every field into ring slot ez % NST (warp 0: lane 0 posts
+  // TMA: element row `ez` of every field into ring slot ez % NST (one warp: lane 0 posts
   // the expected bytes, then each lane issues row copies)
   auto issue = [&](int ez) {
     const int slot = ez % NST;
@@ -759,9 +790,8 @@ __device__ __forceinline__ void strip_tick(const SolveDev& S, const int act, con
       }
     }
   };
-  int issued = min(NST, nelz);  // bands whose copies have been issued (same in every thread)
   if (warp == 0)
-    for (int ez = 0; ez < issued; ++ez) issue(ez);
+    for (int ez = 0; ez < min(NST, nelz); ++ez) issue(ez);
 
   // D and beta in registers (uniform across threads)
   float Dr[NP][NP], Bt[NP];
@@ -779,14 +809,19 @@ __device__ __forceinline__ void strip_tick(const SolveDev& S, const int act, con
   const int s_r = e_r - e0 + 1;
   const bool edge = (ia == 0);
   const bool hasL = edge && e_r >= 1;
-  const bool hasR0 = e_r < nelx;
+  const bool hasR = !edge || e_r < nelx;
   const int xoR = s_r * NP + ia;
   const int xoL = (s_r - 1) * NP + N;
   // x-line items: rows 0..N-1 of each band as (row tid / nseg, segment tid % nseg), which
-  // fits one item per thread; row N of the last band by threads tid < nseg
+  // fits one item per thread; row N of the last band by threads tid < nseg.  The next
+  // lane holds the next segment of the same row when its item is valid and sgi + 1 < nseg.
   const int xa = tid / nseg, xsg = tid - xa * nseg;
   const bool xitem = (xa < N) && (xsg >= seg0);
   const bool xitem_last = (tid < nseg) && (tid >= seg0);
+  const unsigned mA = __ballot_sync(0xffffffffu, xitem);
+  const unsigned mL = __ballot_sync(0xffffffffu, xitem_last);
+  const bool nextA = lane < 31 && ((mA >> (lane + 1)) & 1u) && xsg + 1 < nseg;
+  const bool nextL = lane < 31 && ((mL >> (lane + 1)) & 1u) && tid + 1 < nseg;
 
   const bool damp = !ADJ || (S.flags & F_EXACT);
   const bool grad_on = ADJ && t >= S.it0 && t < S.it1;
@@ -803,6 +838,10 @@ __device__ __forceinline__ void strip_tick(const SolveDev& S, const int act, con
   int rec_lo = 0, rec_hi = 0, inj_lo = 0, inj_hi = 0;
   if (rec_on) { rec_lo = S.rec_tile_off[li0]; rec_hi = S.rec_tile_off[li0 + 1]; }
   if (ADJ && in_win) { inj_lo = S.inj_tile_off[li0]; inj_hi = S.inj_tile_off[li0 + 1]; }
+  // z-table rows: threads tid < 3 NP stage entry (tk, ta) of each band, fetched a band ahead
+  const bool tz_thr = !final_only && tid < 3 * NP;
+  const int tk = tid / NP, ta = tid - tk * NP;
+  float tz_next = tz_thr ? __ldg(tzp + tk * nzg + ta) : 0.f;
 
   float zc = 0.f, szc = 0.f;  // z-line carries into the next band's first row
   bool bad = false;
@@ -817,7 +856,7 @@ __device__ __forceinline__ void strip_tick(const SolveDev& S, const int act, con
     const float* Vs = st + 2 * NP * BW;
     const float* Us = st + 3 * NP * BW;
     const double* Gs = reinterpret_cast<const double*>(st + NF * NP * BW);
-    float* const Xs = xs0 + (SEM_ONE_BARRIER ? (ez & 1) : 0) * XSZ;
+    float* const Xs = xs0 + (ez & 1) * XSZ;
     float* const SXs = Xs + NP * SEGS * NP;
     float* const tzb = sTz + (ez & 1) * 24;
     const int r0 = rec_lo, r1 = rec_hi, j0 = inj_lo, j1 = inj_hi;
@@ -825,9 +864,9 @@ __device__ __forceinline__ void strip_tick(const SolveDev& S, const int act, con
       if (rec_on) { rec_lo = rec_hi; rec_hi = S.rec_tile_off[li0 + ez + 2]; }
       if (ADJ && in_win) { inj_lo = inj_hi; inj_hi = S.inj_tile_off[li0 + ez + 2]; }
     }
-    if (!final_only && tid < 3 * NP) {  // the band's rows of the z tables
-      const int k = tid / NP, a = tid - k * NP;
-      tzb[k * 8 + a] = __ldg(tzp + k * nzg + ez * N + a);
+    if (tz_thr) {
+      tzb[tk * 8 + ta] = tz_next;
+      if (ez + 1 < nelz) tz_next = __ldg(tzp + tk * nzg + (ez + 1) * N + ta);
     }
     // a failed wait records the first band that failed; every thread tests "failed at or
     // before this band" after the band's barrier, so all threads leave at the same band
@@ -836,7 +875,7 @@ __device__ __forceinline__ void strip_tick(const SolveDev& S, const int act, con
 
     if (rec_on) {  // receivers read out of this band, one warp each
       const int cnt = r1 - r0;
-      for (int q = warp; q < cnt; q += NT / 32) {
+      for (int q = warp; q < cnt; q += NW) {
         const int r = S.rec_tile_ids[r0 + q];
         const int bx = S.rec_base[2 * r];
         const float* wr = S.rec_w + (long long)r * NP * NP;
@@ -857,188 +896,217 @@ __device__ __forceinline__ void strip_tick(const SolveDev& S, const int act, con
         }
       }
     }
-    if (!final_only) {
-      if (ADJ && in_win && j1 > j0) {  // adjoint source of receivers in this element row
-        const int cnt = j1 - j0;
-        const double ascale = *S.adj_scale;
-        const long long yrow = (long long)((t - S.it0) / S.decim) * S.nrec;
-        for (int q = tid; q < cnt; q += NT) {
-          const int r = S.inj_tile_ids[j0 + q];
-          const double res = (double)S.rec_out[(long long)t * S.nrec + r] - S.yobs[yrow + r];
-          sres[q] = (float)(res * ascale);
-        }
-        __syncthreads();
-        if (warp == 0) {
-          for (int q = 0; q < cnt; ++q) {
-            const int r = S.inj_tile_ids[j0 + q];
-            const float rs = sres[q];
-            const int bx = S.rec_base[2 * r];
-            const float* wr = S.rec_w + (long long)r * NP * NP;
-            for (int e = lane; e < NP * NP; e += 32) {
-              const int j = e / NP, i = e - j * NP;
-              const int gxx = bx + i;
-              if (gxx >= sx0 && gxx < so1) sacc[j * NT + (gxx - sx0)] += wr[e] * rs;
-            }
-            __syncwarp();
-          }
-        }
-      }
-      // ---- phase A, x-lines: one thread per (band row, element segment)
-      auto xline = [&](int a, int sgi) {
-        const int o = a * BW + off + sgi * N;  // column (e0 - 1 + sgi) * N of row a
-        float u[NP], c[NP], du[NP], q[NP];
-        load_seg<N>(Bs + o, u);
-        load_seg<N>(Cs + o, c);
-#pragma unroll
-        for (int a2 = 0; a2 < NP; ++a2) {
-          float v = 0.f;
-#pragma unroll
-          for (int b = 0; b < NP; ++b) v = fmaf(Dr[a2][b], u[b], v);
-          du[a2] = v;
-          q[a2] = Bt[a2] * c[a2] * v;
-        }
-        float* xo = Xs + (a * SEGS + sgi) * NP;
-#pragma unroll
-        for (int i = 0; i < NP; ++i) {
-          float v = 0.f;
-#pragma unroll
-          for (int a2 = 0; a2 < NP; ++a2) v = fmaf(Dr[a2][i], q[a2], v);
-          xo[i] = v;
-        }
-        if (ADJ) {
-          load_seg<N>(Us + o, u);
-          float* so = SXs + (a * SEGS + sgi) * NP;
-#pragma unroll
-          for (int a2 = 0; a2 < NP; ++a2) {
-            float v = 0.f;
-#pragma unroll
-            for (int b = 0; b < NP; ++b) v = fmaf(Dr[a2][b], u[b], v);
-            so[a2] = Bt[a2] * v * du[a2];
-          }
-        }
-      };
-      if (xitem) xline(xa, xsg);
-      if (last && xitem_last) xline(N, tid);
-      // ---- phase A, z-lines: one thread per owned column (the band is the segment)
-      float rz[NP], sz[NP];
-      if (owned) {
-        float u[NP], du[NP], q[NP];
-#pragma unroll
-        for (int b = 0; b < NP; ++b) u[b] = Bs[b * BW + sc];
-#pragma unroll
-        for (int a2 = 0; a2 < NP; ++a2) {
-          float v = 0.f;
-#pragma unroll
-          for (int b = 0; b < NP; ++b) v = fmaf(Dr[a2][b], u[b], v);
-          du[a2] = v;
-          q[a2] = Bt[a2] * Cs[a2 * BW + sc] * v;
-        }
-#pragma unroll
-        for (int j = 0; j < NP; ++j) {
-          float v = 0.f;
-#pragma unroll
-          for (int a2 = 0; a2 < NP; ++a2) v = fmaf(Dr[a2][j], q[a2], v);
-          rz[j] = v;
-        }
-        if (ADJ) {
-#pragma unroll
-          for (int b = 0; b < NP; ++b) u[b] = Us[b * BW + sc];
-#pragma unroll
-          for (int a2 = 0; a2 < NP; ++a2) {
-            float v = 0.f;
-#pragma unroll
-            for (int b = 0; b < NP; ++b) v = fmaf(Dr[a2][b], u[b], v);
-            sz[a2] = Bt[a2] * v * du[a2];
-          }
-        }
+    if (final_only) {
+      __syncthreads();  // done with this slot
+      if (*s_abort <= ez) { abort_ez = ez; break; }
+      if (warp == 0 && ez + NST < nelz) issue(ez + NST);
+      continue;
+    }
+    if (ADJ && in_win && j1 > j0) {  // adjoint source of receivers in this element row
+      const int cnt = j1 - j0;
+      const double ascale = *S.adj_scale;
+      const long long yrow = (long long)((t - S.it0) / S.decim) * S.nrec;
+      for (int q = tid; q < cnt; q += NT) {
+        const int r = S.inj_tile_ids[j0 + q];
+        const double res = (double)S.rec_out[(long long)t * S.nrec + r] - S.yobs[yrow + r];
+        sres[q] = (float)(res * ascale);
       }
       __syncthreads();
-      if (*s_abort <= ez) { abort_ez = ez; break; }
-#if SEM_ONE_BARRIER
-      // every thread is past phase B of band ez - 1: its ring slot is free
-      if (ez >= 1 && ez - 1 + NST < nelz) {
-        if (warp == 0) issue(ez - 1 + NST);
-        ++issued;
-      }
-#endif
-      // ---- phase B: combine and advance the owned nodes of the band, row by row
-      if (owned) {
-#pragma unroll
-        for (int a = 0; a < NP; ++a) {
-          if (a == N && !last) break;
-          const float* xr = Xs + a * SEGS * NP;
-          const float* sxr = SXs + a * SEGS * NP;
-          float X, SX = 0.f;
-          if (!edge) {
-            X = xr[xoR];
-            if (ADJ) SX = sxr[xoR];
-          } else {
-            X = 0.f;
-            if (hasL) {
-              X = xr[xoL];
-              if (ADJ) SX = sxr[xoL];
-            }
-            if (hasR0) {
-              X += xr[xoR];
-              if (ADJ) SX += sxr[xoR];
-            }
+      if (warp == 0) {
+        for (int q = 0; q < cnt; ++q) {
+          const int r = S.inj_tile_ids[j0 + q];
+          const float rs = sres[q];
+          const int bx = S.rec_base[2 * r];
+          const float* wr = S.rec_w + (long long)r * NP * NP;
+          for (int e = lane; e < NP * NP; e += 32) {
+            const int j = e / NP, i = e - j * NP;
+            const int gxx = bx + i;
+            if (gxx >= sx0 && gxx < so1) sacc[j * NT + (gxx - sx0)] += wr[e] * rs;
           }
-          float Z, SZ = 0.f;
-          if (a == 0) {
-            Z = 0.f;
-            if (ez >= 1) Z = zc;
-            Z += rz[0];
-            if (ADJ) { if (ez >= 1) SZ = szc; SZ += sz[0]; }
-          } else {
-            Z = rz[a];
-            if (ADJ) SZ = sz[a];
-          }
-          const float izv = tzb[a], Rzv = tzb[8 + a], dzv = tzb[16 + a];
-          const int g = gb + a * pitch;
-          float extra;
-          if (!ADJ) {
-            extra = (ez * N + a == src_row) ? src_val : 0.f;
-          } else {
-            extra = in_win ? sacc[a * NT + tid] : 0.f;
-            if (grad_on) gradp[g] = Gs[a * BW + sc] + (double)(Rzv * SX + Rxv * SZ);
-          }
-          float res, vres;
-          advance_node(ADJ, damp, Bs[a * BW + sc], Vs[a * BW + sc], X, Z, ixv, Rxv, dxv, izv, Rzv,
-                       dzv, extra, res, vres);
-          out[g] = res;
-          vout[g] = vres;
-          bad |= !isfinite(res);
-        }
-        zc = rz[N];
-        if (ADJ) szc = sz[N];
-        if (ADJ && in_win) {  // carry the injection row shared with the next band
-          const float carry = sacc[N * NT + tid];
-#pragma unroll
-          for (int a = 1; a < NP; ++a) sacc[a * NT + tid] = 0.f;
-          sacc[tid] = carry;
+          __syncwarp();
         }
       }
     }
-    if (!SEM_ONE_BARRIER || final_only) {
-      __syncthreads();  // done with this slot and the exchange arrays
-      if (final_only && *s_abort <= ez) { abort_ez = ez; break; }
-      if (ez + NST < nelz) {
-        if (warp == 0) issue(ez + NST);
-        ++issued;
+    // ---- phase A, x-lines: one thread per (band row, element segment)
+    auto xline = [&](int a, int sgi, unsigned m, bool nxt) {
+      const int o = a * BW + off + sgi * N;  // column (e0 - 1 + sgi) * N of row a
+      float u[NP], c[NP], du[NP], q[NP];
+      load_seg<N>(Bs + o, u, m, nxt);
+      load_seg<N>(Cs + o, c, m, nxt);
+#pragma unroll
+      for (int a2 = 0; a2 < NP; ++a2) {
+        float v = 0.f;
+#pragma unroll
+        for (int b = 0; b < NP; ++b) v = fmaf(Dr[a2][b], u[b], v);
+        du[a2] = v;
+        q[a2] = Bt[a2] * c[a2] * v;
+      }
+      float* xo = Xs + (a * SEGS + sgi) * NP;
+#pragma unroll
+      for (int i = 0; i < NP; ++i) {
+        float v = 0.f;
+#pragma unroll
+        for (int a2 = 0; a2 < NP; ++a2) v = fmaf(Dr[a2][i], q[a2], v);
+        xo[i] = v;
+      }
+      if (ADJ) {
+        load_seg<N>(Us + o, u, m, nxt);
+        float* so = SXs + (a * SEGS + sgi) * NP;
+#pragma unroll
+        for (int a2 = 0; a2 < NP; ++a2) {
+          float v = 0.f;
+#pragma unroll
+          for (int b = 0; b < NP; ++b) v = fmaf(Dr[a2][b], u[b], v);
+          so[a2] = Bt[a2] * v * du[a2];
+        }
+      }
+    };
+    if (xitem) xline(xa, xsg, mA, nextA);
+    if (last && xitem_last) xline(N, tid, mL, nextL);
+    // ---- phase A, z-lines: one thread per owned column (the band is the segment)
+    float rz[NP], sz[NP];
+    if (owned) {
+      float u[NP], du[NP], q[NP];
+#pragma unroll
+      for (int b = 0; b < NP; ++b) u[b] = Bs[b * BW + sc];
+#pragma unroll
+      for (int a2 = 0; a2 < NP; ++a2) {
+        float v = 0.f;
+#pragma unroll
+        for (int b = 0; b < NP; ++b) v = fmaf(Dr[a2][b], u[b], v);
+        du[a2] = v;
+        q[a2] = Bt[a2] * Cs[a2 * BW + sc] * v;
+      }
+#pragma unroll
+      for (int j = 0; j < NP; ++j) {
+        float v = 0.f;
+#pragma unroll
+        for (int a2 = 0; a2 < NP; ++a2) v = fmaf(Dr[a2][j], q[a2], v);
+        rz[j] = v;
+      }
+      if (ADJ) {
+#pragma unroll
+        for (int b = 0; b < NP; ++b) u[b] = Us[b * BW + sc];
+#pragma unroll
+        for (int a2 = 0; a2 < NP; ++a2) {
+          float v = 0.f;
+#pragma unroll
+          for (int b = 0; b < NP; ++b) v = fmaf(Dr[a2][b], u[b], v);
+          sz[a2] = Bt[a2] * v * du[a2];
+        }
+      }
+    }
+    __syncthreads();
+    if (*s_abort <= ez) { abort_ez = ez; break; }
+#if !SEM_ISSUE_LAST && !SEM_TMA_STORE
+    // every thread is past phase B of band ez - 1: warp 0 refills its slot
+    if (warp == 0 && ez >= 1 && ez - 1 + NST < nelz) issue(ez - 1 + NST);
+#endif
+    // ---- phase B: combine and advance the owned nodes of the band, row by row
+    if (owned) {
+#pragma unroll
+      for (int a = 0; a < NP; ++a) {
+        if (a == N && !last) break;
+        const float* xr = Xs + a * SEGS * NP;
+        const float* sxr = SXs + a * SEGS * NP;
+        // interior column: its segment's entry; edge column: left + right (or one of them)
+        const float xL = hasL ? xr[xoL] : 0.f;
+        const float xR = hasR ? xr[xoR] : 0.f;
+        const float X = !edge ? xR : (hasR ? xL + xR : xL);
+        float SX = 0.f;
+        if (ADJ) {
+          const float sL = hasL ? sxr[xoL] : 0.f;
+          const float sR = hasR ? sxr[xoR] : 0.f;
+          SX = !edge ? sR : (hasR ? sL + sR : sL);
+        }
+        float Z, SZ = 0.f;
+        if (a == 0) {
+          Z = (ez >= 1 ? zc : 0.f) + rz[0];
+          if (ADJ) SZ = (ez >= 1 ? szc : 0.f) + sz[0];
+        } else {
+          Z = rz[a];
+          if (ADJ) SZ = sz[a];
+        }
+        const float izv = tzb[a], Rzv = tzb[8 + a], dzv = tzb[16 + a];
+        const int g = gb + a * pitch;
+        float extra;
+        double gnew = 0.0;
+        if (!ADJ) {
+          extra = (ez * N + a == src_row) ? src_val : 0.f;
+        } else {
+          extra = in_win ? sacc[a * NT + tid] : 0.f;
+          if (grad_on) gnew = Gs[a * BW + sc] + (double)(Rzv * SX + Rxv * SZ);
+        }
+        float res, vres;
+        advance_node(ADJ, damp, Bs[a * BW + sc], Vs[a * BW + sc], X, Z, ixv, Rxv, dxv, izv, Rzv,
+                     dzv, extra, res, vres);
+        if (by_bulk) {  // in place: only this thread reads its column of the slot in phase B
+          const_cast<float*>(Bs)[a * BW + sc] = res;
+          const_cast<float*>(Vs)[a * BW + sc] = vres;
+          if (ADJ && grad_on) const_cast<double*>(Gs)[a * BW + sc] = gnew;
+        } else {
+          out[g] = res;
+          vout[g] = vres;
+          if (ADJ && grad_on) gradp[g] = gnew;
+        }
+        bad |= !isfinite(res);
+      }
+      zc = rz[N];
+      if (ADJ) szc = sz[N];
+      if (ADJ && in_win) {  // carry the injection row shared with the next band
+        const float carry = sacc[N * NT + tid];
+#pragma unroll
+        for (int a = 1; a < NP; ++a) sacc[a * NT + tid] = 0.f;
+        sacc[tid] = carry;
+      }
+    }
+    // the last warp past phase B of band ez writes the band's rows out of the slot (bulk
+    // stores) and refills the slot with band ez + NST
+    if (SEM_TMA_STORE || (SEM_ISSUE_LAST && ez + NST < nelz)) {
+      if (SEM_TMA_STORE) fence_proxy_async_smem();
+      __syncwarp();
+      int mine = 0;
+      if (lane == 0) mine = (atomicAdd(done + slot, 1) == NW - 1);
+      if (__shfl_sync(0xffffffffu, mine, 0)) {
+        if (SEM_TMA_STORE && h1 > h0) {
+          const int rows = last ? NP : N;
+          const int nf = (ADJ && grad_on) ? 3 : 2;
+          const unsigned nb = (unsigned)(h1 - h0) * 4u;
+          for (int q = lane; q < rows * nf; q += 32) {
+            const int f = q / rows, a = q - f * rows;
+            const long long grow = (long long)(ez * N + a) * pitch + h0;
+            const int srow = a * BW + (h0 - X0);
+            if (f == 0) bulk_store(out + grow, Bs + srow, nb);
+            else if (f == 1) bulk_store(vout + grow, Vs + srow, nb);
+            else bulk_store(gradp + grow, Gs + srow, 2u * nb);
+          }
+          bulk_commit();
+          bulk_wait_read();
+          __syncwarp();
+        }
+        if (lane == 0) done[slot] = 0;
+        if (ez + NST < nelz) issue(ez + NST);
       }
     }
   }
+  if (SEM_TMA_STORE) bulk_wait_all();
   if (abort_ez >= 0) {
-    // drain the copies still in flight (bands abort_ez .. issued - 1) before leaving
+    // drain the copies still in flight (bands abort_ez .. abort_ez + NST - 1) before leaving
     if (tid == 0) atomicOr(S.status, SEM_ERR_TIMEOUT);
-    for (int b = abort_ez; b < issued; ++b) mbar_wait(bars + b % NST, (unsigned)((b / NST) & 1));
+    // refills issued so far: bands < NST, and band ez' - 1 + NST at each mid barrier ez' <
+    // abort_ez (or band ez' + NST after phase B of each band ez' < abort_ez)
+    const int issued = (SEM_ISSUE_LAST || SEM_TMA_STORE) ? abort_ez + NST
+                                                         : max(NST, abort_ez + NST - 1);
+    for (int b = abort_ez; b < min(issued, nelz); ++b)
+      mbar_wait(bars + b % NST, (unsigned)((b / NST) & 1));
+    if (SEM_TMA_STORE) bulk_wait_all();  // bulk stores of earlier bands still read the ring
     return;
   }
   if (__any_sync(0xffffffffu, bad) && lane == 0) atomicOr(S.status, SEM_ERR_NONFINITE);
 }
 
 template <int N>
-__global__ void __launch_bounds__(kStripCols, (N <= 4) ? SEM_STRIP_MIN_BLOCKS : 4)
+__global__ void __launch_bounds__(kStripCols, (N <= 4) ? SEM_STRIP_MIN_BLOCKS : 3)
     sem_strip_kernel(const SolveDev* __restrict__ solves, const int* __restrict__ cta_solve,
                      const int* __restrict__ tick_ptr, int unused0, int unused1) {
   extern __shared__ __align__(128) float smem[];
@@ -1322,6 +1390,9 @@ struct sem_batch_s {
   long long last_launches = 0;
   int last_kernel = 0;
   int last_groups = 0;
+  long long last_ticks = 0;             // tick rounds of the last sem_run (all groups)
+  std::vector<cudaEvent_t> tick_ev;     // per group: before / after its tick loop
+  int tick_ev_used = 0;
   std::vector<SolveDev> h_solves;
   std::vector<int> h_cta;
 };
@@ -1417,6 +1488,7 @@ int sem_batch_create(sem_batch_t** out) {
 
 int sem_batch_destroy(sem_batch_t* b) {
   if (!b) return SEM_OK;
+  for (cudaEvent_t e : b->tick_ev) cudaEventDestroy(e);
   cudaFree(b->arena); cudaFree(b->d_tick); cudaFree(b->d_solves); cudaFree(b->d_cta);
   delete b;
   return SEM_OK;
@@ -1619,7 +1691,14 @@ static int run_group(sem_batch_t* b, const sem_solve_t* solves, int32_t n,
     return SEM_OK;
   };
 
-  // ---- the tick loop: plain launches or captured chunks
+  // ---- the tick loop: plain launches or captured chunks, bracketed by events
+  while ((int)b->tick_ev.size() < b->tick_ev_used + 2) {
+    cudaEvent_t e;
+    CUDA_TRY(cudaEventCreate(&e));
+    b->tick_ev.push_back(e);
+  }
+  cudaEvent_t ev_begin = b->tick_ev[b->tick_ev_used], ev_end = b->tick_ev[b->tick_ev_used + 1];
+  CUDA_TRY(cudaEventRecord(ev_begin, stream));
   const long long per_tick = (long long)launches.size() + 1;
   bool graphed = false;
   if (cfg.graph_chunk > 0 && stream != nullptr && stream != cudaStreamLegacy &&
@@ -1646,6 +1725,9 @@ static int run_group(sem_batch_t* b, const sem_solve_t* solves, int32_t n,
     b->last_launches += (long long)max_prog * per_tick;
   }
   CUDA_TRY(cudaGetLastError());
+  CUDA_TRY(cudaEventRecord(ev_end, stream));
+  b->tick_ev_used += 2;
+  b->last_ticks += max_prog;
 
   // ---- outputs
   for (int oi = 0; oi < n; ++oi) {
@@ -1805,6 +1887,8 @@ int sem_run(sem_batch_t* b, const sem_solve_t* solves, int32_t n, const sem_laun
   if (cfg.memory_budget < 0) return fail(SEM_ERR_ARG, "memory_budget must be >= 0");
   b->last_launches = 0;
   b->last_groups = 0;
+  b->last_ticks = 0;
+  b->tick_ev_used = 0;
   if (n == 0) return SEM_OK;
   bool any_auto = false;
   for (int i = 0; i < n; ++i) {
@@ -1837,6 +1921,21 @@ int sem_run(sem_batch_t* b, const sem_solve_t* solves, int32_t n, const sem_laun
 }
 
 int32_t sem_batch_last_groups(const sem_batch_t* b) { return b ? b->last_groups : -1; }
+
+int64_t sem_batch_last_ticks(const sem_batch_t* b) { return b ? b->last_ticks : -1; }
+
+int sem_batch_last_tick_ms(const sem_batch_t* b, double* ms_out) {
+  if (!b || !ms_out) return fail(SEM_ERR_ARG, "null argument");
+  double tot = 0.0;
+  for (int i = 0; i + 1 < b->tick_ev_used; i += 2) {
+    CUDA_TRY(cudaEventSynchronize(b->tick_ev[i + 1]));
+    float ms = 0.f;
+    CUDA_TRY(cudaEventElapsedTime(&ms, b->tick_ev[i], b->tick_ev[i + 1]));
+    tot += ms;
+  }
+  *ms_out = tot;
+  return SEM_OK;
+}
 
 int sem_forward_noalloc(const sem_plan_t* p, const double* velocity, float* rec_out,
                         int32_t* status_out, void* stream_v) {

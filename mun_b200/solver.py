@@ -100,6 +100,18 @@ class Batch:
         return int(self._lib.sem_batch_last_groups(self.handle))
 
     @property
+    def last_ticks(self):
+        """Tick rounds the last run launched (summed over its groups)."""
+        return int(self._lib.sem_batch_last_ticks(self.handle))
+
+    def last_tick_ms(self):
+        """Device time (ms) of the last run's tick loops, from CUDA events the library
+        records on the run's stream around them; waits for those events."""
+        ms = C.c_double()
+        _lib.check(self._lib.sem_batch_last_tick_ms(self.handle, C.byref(ms)))
+        return float(ms.value)
+
+    @property
     def last_kernel(self):
         return {1: "tile", 2: "strip"}.get(int(self._lib.sem_batch_last_kernel(self.handle)), "none")
 
