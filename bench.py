@@ -34,8 +34,10 @@ BYTES_PER_NODE_STEP_FWDADJ = 56  # algorithmic bytes (float32 state, float64 gra
 # gradient and writes lambda, mu and the gradient
 BYTES_PER_NODE_FWD_TICK = 20
 BYTES_PER_NODE_ADJ_TICK = 40
-# DRAM bytes per node measured by ncu for each tick kind (None: not measured)
-TRAFFIC_B_PER_NODE = None
+# DRAM bytes per node and tick of the strip kernel from one ncu capture (dram__bytes_read +
+# dram__bytes_write of one forward and one adjoint tick over 128 models, 10.3 M nodes;
+# profiles/sem_strip_kernel_N4_128models.md), scaled to a launch by its nodes
+TRAFFIC_B_PER_NODE = {"fwd": 16.6, "adj": 36.7}
 
 
 def workload(nmodels=256, nelx=100, nelz=50, nt=3000, nrec=100, seed0=0):
@@ -543,7 +545,7 @@ def main():
     achieved = kern_bytes / (tick_loop_ms / 1e3) / 1e9
     peak = float(pk.get("hbm_gbs", 6650.0))
     # DRAM traffic per node of each tick kind from the ncu capture of the strip kernel
-    # (16 models, scaled per node), averaged like the algorithmic bytes
+    # (128 models, per node), averaged over the step's ticks like the algorithmic bytes
     traffic = None
     if kernel_used == "strip" and TRAFFIC_B_PER_NODE:
         traffic = W["npoints"] * (n // groups_used) * (

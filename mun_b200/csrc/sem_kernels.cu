@@ -1178,6 +1178,62 @@ __global__ void copy_status_kernel(const int* __restrict__ st, int* __restrict__
   if (threadIdx.x == 0 && blockIdx.x == 0) *out = *st;
 }
 
+// Per-solve inputs and outputs of one sem_run group, for the batched set-up and output
+// kernels (one grid row per solve).
+struct SolveIo {
+  const double* vel;      // [npoints] velocity, reference node order
+  const int* pos;         // [npoints] grid offset of each node
+  float* c2;              // c^2 field
+  int npoints, nzero;
+  char* zp[8];            // workspace ranges that must start at zero (256-byte aligned,
+  long long zb[8];        //   lengths multiples of 16 bytes)
+  double* grad_out;       // or null
+  const double* gacc;     // float64 dJ/dc^2 accumulator
+  const double* adj_scale;
+  double inv_sigma2;
+  const double* misfit;   // [nrec]
+  int nrec;
+  double* loglik_out;     // or null
+  const int* st;          // workspace status word
+  int* status_out;        // or null
+};
+
+// clears every solve's zero-start state and stages c^2 (row blockIdx.y = solve)
+__global__ void batch_setup_kernel(const SolveIo* __restrict__ io, int s0) {
+  const SolveIo& s = io[s0 + blockIdx.y];
+  const long long t0 = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  for (int r = 0; r < s.nzero; ++r) {
+    uint4* p = reinterpret_cast<uint4*>(s.zp[r]);
+    const long long n16 = s.zb[r] >> 4;
+    for (long long i = t0; i < n16; i += stride) p[i] = make_uint4(0u, 0u, 0u, 0u);
+  }
+  for (long long i = t0; i < s.npoints; i += stride) {
+    const double v = s.vel[i];
+    s.c2[s.pos[i]] = (float)(v * v);
+  }
+}
+
+// gradient in reference node order, log-likelihood and status of every solve
+// (same arithmetic as grad_out_kernel / loglik_kernel / copy_status_kernel)
+__global__ void batch_output_kernel(const SolveIo* __restrict__ io, int s0) {
+  const SolveIo& s = io[s0 + blockIdx.y];
+  if (s.grad_out) {
+    const double scale = s.inv_sigma2 / *s.adj_scale;  // exact: adj_scale is a power of two
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < s.npoints;
+         i += (long long)gridDim.x * blockDim.x)
+      s.grad_out[i] = 2.0 * s.vel[i] * s.gacc[s.pos[i]] * scale;
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    if (s.loglik_out) {
+      double m = 0.0;
+      for (int r = 0; r < s.nrec; ++r) m += s.misfit[r];
+      *s.loglik_out = -0.5 * m * s.inv_sigma2;
+    }
+    if (s.status_out) *s.status_out = *s.st;
+  }
+}
+
 // ----------------------------------------------------------------------------
 // Scratch of the allocation-free forward entry point (sem_forward_noalloc).  Every
 // GPU that loads this library holds it until the process exits.  Host code must not
@@ -1392,6 +1448,9 @@ struct sem_batch_s {
   int last_groups = 0;
   long long last_ticks = 0;             // tick rounds of the last sem_run (all groups)
   std::vector<cudaEvent_t> tick_ev;     // per group: before / after its tick loop
+  SolveIo* d_io = nullptr;              // per-solve set-up / output table of a group
+  int io_cap = 0;
+  std::vector<SolveIo> h_io;
   int tick_ev_used = 0;
   std::vector<SolveDev> h_solves;
   std::vector<int> h_cta;
@@ -1489,6 +1548,7 @@ int sem_batch_create(sem_batch_t** out) {
 int sem_batch_destroy(sem_batch_t* b) {
   if (!b) return SEM_OK;
   for (cudaEvent_t e : b->tick_ev) cudaEventDestroy(e);
+  cudaFree(b->d_io);
   cudaFree(b->arena); cudaFree(b->d_tick); cudaFree(b->d_solves); cudaFree(b->d_cta);
   delete b;
   return SEM_OK;
@@ -1635,25 +1695,51 @@ static int run_group(sem_batch_t* b, const sem_solve_t* solves, int32_t n,
   CUDA_TRY(cudaMemcpyAsync(b->d_cta, b->h_cta.data(), sizeof(int) * b->h_cta.size(),
                            cudaMemcpyHostToDevice, stream));
 
-  // ---- zero the state that must start at zero, stage c^2
+  // ---- per-solve inputs/outputs: one set-up launch (zero-start state, c^2) and one
+  // output launch (gradient, log-likelihood, status) for the whole group
+  b->h_io.assign(n, SolveIo{});
+  long long max_pts = 1;
   for (int oi = 0; oi < n; ++oi) {
     const int i = order[oi];
     const sem_solve_t& s = solves[i];
     const sem_plan_s* p = s.plan;
     char* a = b->arena + base[i];
     const long long F = p->fstride * 4;
+    SolveIo& io = b->h_io[oi];
+    io.vel = s.velocity; io.pos = p->node_pos; io.c2 = (float*)(a + ws[i].c2);
+    io.npoints = p->npoints;
+    max_pts = std::max(max_pts, (long long)p->npoints);
     // zero initial state: b_0 (ckpt 0 or ring 0 or W 0), v_0 (ckpt 1 or V), adjoint state
-    CUDA_TRY(cudaMemsetAsync(a + ws[i].W, 0, F, stream));
-    CUDA_TRY(cudaMemsetAsync(a + ws[i].V, 0, F, stream));
+    auto zero = [&](long long o, long long bytes) { io.zp[io.nzero] = a + o; io.zb[io.nzero++] = bytes; };
+    zero(ws[i].W, F);
+    zero(ws[i].V, F);
     if (s.flags & SEM_F_ADJOINT) {
-      CUDA_TRY(cudaMemsetAsync(a + ws[i].ckpt, 0, 2 * F, stream));
-      CUDA_TRY(cudaMemsetAsync(a + ws[i].ring, 0, F, stream));
-      CUDA_TRY(cudaMemsetAsync(a + ws[i].L, 0, 3 * F, stream));   // L[0], L[1], Mu
-      CUDA_TRY(cudaMemsetAsync(a + ws[i].grad, 0, 2 * F, stream));
+      zero(ws[i].ckpt, 2 * F);
+      zero(ws[i].ring, F);
+      zero(ws[i].L, 3 * F);      // L[0], L[1], Mu
+      zero(ws[i].grad, 2 * F);
     }
-    CUDA_TRY(cudaMemsetAsync(a + ws[i].misfit, 0, ws[i].status - ws[i].misfit + 256, stream));
-    set_c2_kernel<<<std::min(1024, (p->npoints + 255) / 256), 256, 0, stream>>>(
-        s.velocity, p->node_pos, (float*)(a + ws[i].c2), p->npoints);
+    zero(ws[i].misfit, ws[i].status - ws[i].misfit + 256);
+    io.grad_out = ((s.flags & SEM_F_ADJOINT) && s.grad_out) ? s.grad_out : nullptr;
+    io.gacc = (const double*)(a + ws[i].grad);
+    io.adj_scale = (const double*)(a + ws[i].misfit) + 2 * p->nrec;
+    io.inv_sigma2 = s.inv_sigma2;
+    io.misfit = (const double*)(a + ws[i].misfit);
+    io.nrec = p->nrec;
+    io.loglik_out = ((s.flags & SEM_F_MISFIT) && s.loglik_out) ? s.loglik_out : nullptr;
+    io.st = (const int*)(a + ws[i].status);
+    io.status_out = s.status_out;
+  }
+  if (n > b->io_cap) {
+    cudaFree(b->d_io);
+    b->d_io = nullptr;
+    CUDA_TRY(cudaMalloc((void**)&b->d_io, sizeof(SolveIo) * n));
+    b->io_cap = n;
+  }
+  CUDA_TRY(cudaMemcpyAsync(b->d_io, b->h_io.data(), sizeof(SolveIo) * n, cudaMemcpyHostToDevice, stream));
+  const unsigned io_bx = (unsigned)std::min<long long>(64, (max_pts + 2047) / 2048);
+  for (int s0 = 0; s0 < n; s0 += 65535) {
+    batch_setup_kernel<<<dim3(io_bx, (unsigned)std::min(65535, n - s0)), 256, 0, stream>>>(b->d_io, s0);
     b->last_launches++;
   }
   CUDA_TRY(cudaMemsetAsync(b->d_tick, 0, sizeof(int), stream));
@@ -1730,26 +1816,9 @@ static int run_group(sem_batch_t* b, const sem_solve_t* solves, int32_t n,
   b->last_ticks += max_prog;
 
   // ---- outputs
-  for (int oi = 0; oi < n; ++oi) {
-    const int i = order[oi];
-    const sem_solve_t& s = solves[i];
-    const sem_plan_s* p = s.plan;
-    char* a = b->arena + base[i];
-    if ((s.flags & SEM_F_ADJOINT) && s.grad_out) {
-      grad_out_kernel<<<std::min(1024, (p->npoints + 255) / 256), 256, 0, stream>>>(
-          s.velocity, p->node_pos, (const double*)(a + ws[i].grad), s.inv_sigma2,
-          (const double*)(a + ws[i].misfit) + 2 * p->nrec, s.grad_out, p->npoints);
-      b->last_launches++;
-    }
-    if ((s.flags & SEM_F_MISFIT) && s.loglik_out) {
-      loglik_kernel<<<1, 32, 0, stream>>>((const double*)(a + ws[i].misfit), p->nrec, s.inv_sigma2,
-                                          s.loglik_out);
-      b->last_launches++;
-    }
-    if (s.status_out) {
-      copy_status_kernel<<<1, 32, 0, stream>>>((const int*)(a + ws[i].status), s.status_out);
-      b->last_launches++;
-    }
+  for (int s0 = 0; s0 < n; s0 += 65535) {
+    batch_output_kernel<<<dim3(io_bx, (unsigned)std::min(65535, n - s0)), 256, 0, stream>>>(b->d_io, s0);
+    b->last_launches++;
   }
   CUDA_TRY(cudaGetLastError());
   return SEM_OK;
