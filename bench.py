@@ -115,33 +115,107 @@ def peaks():
 
 
 def cpu_baseline(W, nt_sample, threads):
-    """Oracle restatement of the reference's CPU path on one model.  Runs nt_sample and
+    """Oracle restatement of the reference's CPU path on one model.  nt_sample <= 0 (or
+    >= nt): one full-length solve, timed as is.  Otherwise runs nt_sample and
     2*nt_sample steps and fits set-up + per-step cost, so the full-length solve time is
     set-up + nt * per-step (the reference's loops are linear in nt)."""
+    if nt_sample <= 0 or nt_sample >= W["nt"]:
+        t = oracle_solve_s(W, W["nt"], threads)
+        return t, t
+    t1 = oracle_solve_s(W, nt_sample, threads)
+    t2 = oracle_solve_s(W, 2 * nt_sample, threads)
+    per_step = max((t2 - t1) / nt_sample, 1e-9)
+    setup = max(t1 - per_step * nt_sample, 0.0)
+    return setup + per_step * W["nt"], t1 + t2
+
+
+def oracle_solve_s(W, nts, threads):
+    """Wall time of one oracle fwd+adj solve of nts steps (set-up included)."""
     import torch
     from oracle import sem_oracle as so
     torch.set_num_threads(threads)
     kw = W["plan_kw"]
+    cfg = {"domain": {"xmin": kw["xmin"], "xmax": kw["xmax"], "zmin": kw["zmin"],
+                      "zmax": kw["zmax"], "nelem_x": kw["nelx"], "nelem_z": kw["nelz"]},
+           "time": {"total_time": (nts - 0.5) * W["dt"], "dt": W["dt"]},
+           "source": {"position": kw["src_xz"], "frequency": kw["f0"], "amplitude": kw["amp"]},
+           "receivers": {"positions": kw["receivers"]},
+           "method": {"polynomial_order": kw["npol"], "pml_thickness": kw["pml_thickness"]},
+           "velocity": {"outside_velocity": kw["sponge_cmax"]}}
+    t0 = time.perf_counter()
+    sim = so.build_sim(cfg, W["vels"][0], dt=W["dt"])
+    y = np.zeros((sim.nt, len(kw["receivers"])))
+    so.forward_adjoint(sim, y, W["sigma"])
+    return time.perf_counter() - t0
 
-    def one(nts):
-        cfg = {"domain": {"xmin": kw["xmin"], "xmax": kw["xmax"], "zmin": kw["zmin"],
-                          "zmax": kw["zmax"], "nelem_x": kw["nelx"], "nelem_z": kw["nelz"]},
-               "time": {"total_time": (nts - 0.5) * W["dt"], "dt": W["dt"]},
-               "source": {"position": kw["src_xz"], "frequency": kw["f0"], "amplitude": kw["amp"]},
-               "receivers": {"positions": kw["receivers"]},
-               "method": {"polynomial_order": kw["npol"], "pml_thickness": kw["pml_thickness"]},
-               "velocity": {"outside_velocity": kw["sponge_cmax"]}}
+
+def cpu_estimate(plan_kw, dt, nt, velocity, nt_sample, threads, sigma=1e-3):
+    """Oracle CPU time of one full fwd+adj solve, fitted from nt_sample and 2*nt_sample
+    step runs (set-up + per-step cost); exact when nt_sample >= nt."""
+    W = {"plan_kw": plan_kw, "dt": dt, "nt": nt, "vels": [velocity], "sigma": sigma}
+    if nt_sample >= nt:
+        el = oracle_solve_s(W, nt, threads)
+        return el, el
+    return cpu_baseline(W, nt_sample, threads)
+
+
+def run_plain(args):
+    """Plain method (CPU-runnable case): 2000x1000 m, 40x20 elements, order 4 (161x81
+    nodes), three-layer 1500/2200/3000 m/s (interfaces 300/650 m), Ricker 10 Hz at
+    (1000, 20), 50 receivers at 10 m depth, dt from CFL 0.4, 2000 steps, forward +
+    adjoint; observations from the model with +100 m/s on the central B-spline nodes.
+    One GPU solve at a time (events) and the oracle's full CPU run on the host cores."""
+    import torch
+    from mun_b200 import Batch, SEMPlan, SolveSpec
+    from mun_b200.bspline import grid_basis, layered_velocity
+    from mun_b200.mesh import create_global_mesh
+    xmin, xmax, zmin, zmax, nelx, nelz, N = 0.0, 2000.0, 0.0, 1000.0, 40, 20, 4
+    coords, _, ng = create_global_mesh(xmin, xmax, zmin, zmax, nelx, nelz, N)
+    v = layered_velocity(coords[:, 1], [300.0, 650.0], [1500.0, 2200.0, 3000.0])
+    B = grid_basis(coords, (xmin, xmax), (zmin, zmax), 8, 4)
+    th = np.zeros(32)
+    th[[10, 11, 13, 14, 18, 19, 21, 22]] = 100.0
+    v_obs = v + B @ th
+    h = min((xmax - xmin) / nelx, (zmax - zmin) / nelz)
+    dt = 0.4 * (h / (N + 1)) / (3100.0 * (N + 1) * np.sqrt(2.0))
+    nt = 2000
+    rec = np.stack([np.linspace(xmin, xmax, 50), np.full(50, 10.0)], 1)
+    kw = dict(xmin=xmin, xmax=xmax, zmin=zmin, zmax=zmax, nelx=nelx, nelz=nelz, npol=N, dt=dt, nt=nt,
+              src_xz=(1000.0, 20.0), f0=10.0, amp=1.0, receivers=rec, pml_thickness=200.0,
+              sponge_cmax=3000.0, coords=coords, node_grid=ng)
+    plan = SEMPlan(**kw)
+    dev = torch.device("cuda")
+    obs = SolveSpec(plan, torch.as_tensor(v_obs, device=dev), shift=True)
+    Batch().run([obs])
+    y = obs.rec.double()
+    b = Batch()
+    stream = torch.cuda.Stream()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ms = []
+    for it in range(args.warmup + max(args.steps, 5)):
+        s = SolveSpec(plan, torch.as_tensor(v, device=dev), adjoint=True, y_obs=y, inv_sigma2=1e6)
+        with torch.cuda.stream(stream):
+            ev0.record(stream)
+            b.run([s])
+            ev1.record(stream)
+        ev1.synchronize()
+        if it >= args.warmup:
+            ms.append(ev0.elapsed_time(ev1))
+    ms = np.array(ms)
+    out = {"workload": "plain: 40x20 el, N=4, 13041 nodes, 2000 steps, 50 receivers, fwd+adj",
+           "gpu_ms_per_solve": float(ms.mean()), "gpu_solves_per_s": 1e3 / float(ms.mean()),
+           "p50_ms": float(np.percentile(ms, 50)), "p99_ms": float(np.percentile(ms, 99)),
+           "kernel": b.last_kernel, "groups": b.last_groups, "status": int(s.status.item())}
+    if not args.no_cpu:
+        threads = os.cpu_count() or 1
+        kw_o = {k: kw[k] for k in kw if k not in ("coords", "node_grid")}
         t0 = time.perf_counter()
-        sim = so.build_sim(cfg, W["vels"][0], dt=W["dt"])
-        y = np.zeros((sim.nt, len(kw["receivers"])))
-        so.forward_adjoint(sim, y, W["sigma"])
-        return time.perf_counter() - t0
-
-    t1 = one(nt_sample)
-    t2 = one(2 * nt_sample)
-    per_step = max((t2 - t1) / nt_sample, 1e-9)
-    setup = max(t1 - per_step * nt_sample, 0.0)
-    return setup + per_step * W["nt"], t1 + t2
+        per, _ = cpu_estimate(kw_o, dt, nt, v, nt, threads)
+        out["cpu"] = {"s_per_solve": per, "solves_per_s": 1.0 / per, "cores": threads, "kind": "port",
+                      "sample": "one full 2000-step run, set-up included",
+                      "wall_s": time.perf_counter() - t0}
+        out["gpu_over_cpu"] = per / (ms.mean() / 1e3)
+    print(json.dumps(out), flush=True)
 
 
 def run_reference(args):
@@ -159,15 +233,18 @@ def run_reference(args):
         times.append(per)
     per = float(np.mean(times))
     val = 1.0 / per
+    sample_txt = ("1 model, one full 3000-step fwd+adj solve per step (set-up included)"
+                  if nt_sample <= 0 or nt_sample >= W["nt"] else
+                  f"1 model, {nt_sample}- and {2 * nt_sample}-step runs (of 3000) fitted to set-up + "
+                  "per-step cost")
     out = {"metric": "SEM fwd+adjoint solves/s", "value": val, "unit": "solves/s",
            "impl": "reference", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
            "ms_per_step": per * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
            "dtype": "f64", "data": "synthetic",
            "config": {"workload": "batched ELBO sampling: 100x50 el, N=4, 80601 nodes, 3000 steps",
-                      "sample": f"1 model, {nt_sample}/{2 * nt_sample} of 3000 steps, linear fit"},
+                      "sample": sample_txt},
            "cpu_baseline": {"value": val, "unit": "solves/s", "cores": threads, "kind": "port",
-                            "sample": f"1 model, {nt_sample}- and {2 * nt_sample}-step runs (of 3000) "
-                                      "fitted to set-up + per-step cost"},
+                            "sample": sample_txt},
            "e2e": {"value": val, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(out), flush=True)
 
@@ -246,7 +323,21 @@ def run_uneven(args):
     # plain time of the whole set, scaled by node-steps of the timed subset
     sub = plans[: len(plain_ms)]
     plain_total = sum(plain_ms) * node_steps / sum(p.npoints * p.nt for p in sub)
+    cpu = None
+    if args.cpu_sample > 0:
+        threads = os.cpu_count() or 1
+        per_ns, el = [], 0.0
+        for p, a in list(zip(plans, specs_args))[:2]:
+            kw_o = {k: a["plan"][k] for k in a["plan"] if k not in ("coords", "node_grid", "dt", "nt")}
+            per, e = cpu_estimate(kw_o, a["plan"]["dt"], p.nt, a["v"], args.cpu_sample, threads)
+            per_ns.append(per / (p.npoints * p.nt))
+            el += e
+        total = float(np.mean(per_ns)) * node_steps
+        cpu = {"solves_per_s": len(plans) / total, "s_all": total, "cores": threads, "kind": "port",
+               "sample": f"first 2 solves, {args.cpu_sample}/{2 * args.cpu_sample}-step runs, per node-step "
+                         f"cost scaled to all 64 ({el:.0f} s)"}
     print(json.dumps({"workload": "uneven batch: 64 solves, 40x20..200x100 el, N in {3,4,5}, nt 1500-6000",
+                      "cpu": cpu,
                       "metric": "SEM fwd+adjoint solves/s", "batched": batched, "unit": "solves/s",
                       "batched_ms": float(np.mean(ms)), "kernel": b.last_kernel,
                       "plain_estimated": len(plans) / (plain_total / 1e3), "plain_solves_timed": len(plain_ms),
@@ -378,7 +469,18 @@ def run_single(args):
         if it >= args.warmup:
             ms.append(ev0.elapsed_time(ev1))
     m = float(np.mean(ms))
+    cpu = None
+    if args.cpu_sample > 0:
+        kw_o = dict(xmin=0.0, xmax=8000.0, zmin=0.0, zmax=4000.0, nelx=nelx, nelz=nelz, npol=N,
+                    src_xz=(4000.0, 1e-3), f0=15.0, amp=1.0, receivers=rec, pml_thickness=400.0,
+                    sponge_cmax=4000.0)
+        threads = os.cpu_count() or 1
+        per, el = cpu_estimate(kw_o, dt, nt, v, args.cpu_sample, threads)
+        cpu = {"s_per_solve": per, "solves_per_s": 1.0 / per, "cores": threads, "kind": "port",
+               "sample": f"{args.cpu_sample}- and {2 * args.cpu_sample}-step runs of {nt}, linear fit "
+                         f"(float64 state, no checkpointing: {el:.0f} s)"}
     print(json.dumps({"workload": "single large solve: 400x200 el, N=4, 1,282,401 nodes, 5000 steps, k=250",
+                      "cpu": cpu,
                       "nt": nt, "ms_per_solve": m, "solves_per_s": 1e3 / m, "kernel": b.last_kernel,
                       "mnode_steps_per_s": plan.npoints * nt / (m / 1e3) / 1e6,
                       "achieved_gbs_56B": 56 * plan.npoints * nt / (m / 1e3) / 1e9,
@@ -398,10 +500,12 @@ def main():
     ap.add_argument("--graph-chunk", type=int, default=0)
     ap.add_argument("--kernel", type=int, default=0, help="0 auto, 1 tile, 2 strip")
     ap.add_argument("--ckpt-k", type=int, default=0)
-    ap.add_argument("--ref-nt", type=int, default=200)
-    ap.add_argument("--cpu-nt", type=int, default=200)
+    ap.add_argument("--ref-nt", type=int, default=0, help="reference arm sample steps (0 = full solve)")
+    ap.add_argument("--cpu-nt", type=int, default=0, help="cpu_baseline sample steps (0 = full solve)")
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--workload", default="elbo", choices=["elbo", "uneven", "serving", "single"])
+    ap.add_argument("--cpu-sample", type=int, default=0,
+                    help="single/uneven workloads: oracle CPU estimate from this many steps (0 = none)")
+    ap.add_argument("--workload", default="elbo", choices=["elbo", "plain", "uneven", "serving", "single"])
     ap.add_argument("--serve-rate", type=float, default=200.0)
     ap.add_argument("--serve-requests", type=int, default=400)
     ap.add_argument("--serve-T", type=float, default=0.25)
@@ -411,6 +515,8 @@ def main():
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
+    if args.workload == "plain":
+        return run_plain(args)
     if args.workload == "uneven":
         return run_uneven(args)
     if args.workload == "serving":
@@ -556,9 +662,11 @@ def main():
     if rank == 0 and not args.no_cpu:
         threads = os.cpu_count() or 1
         per, el = cpu_baseline(W, args.cpu_nt, threads)
+        full = args.cpu_nt <= 0 or args.cpu_nt >= W["nt"]
         cpu = {"value": 1.0 / per, "unit": "solves/s", "cores": threads, "kind": "port",
-               "sample": f"1 model, {args.cpu_nt}- and {2 * args.cpu_nt}-step runs of {W['nt']} "
-                         f"({el:.1f} s), fitted set-up + per-step cost"}
+               "sample": (f"1 model, one full {W['nt']}-step fwd+adj solve ({el:.1f} s)" if full else
+                          f"1 model, {args.cpu_nt}- and {2 * args.cpu_nt}-step runs of {W['nt']} "
+                          f"({el:.1f} s), fitted set-up + per-step cost")}
     if rank == 0:
         out = {
             "metric": "SEM fwd+adjoint solves/s (batched vs plain, same GPU, <=1e-4 rel); p50/p99 ms",
