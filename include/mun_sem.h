@@ -99,7 +99,11 @@ typedef struct {
                                  2 strip kernel (one CTA per full-height strip, TMA-
                                  staged element-row bands); auto picks strips when the
                                  batch has at least one strip per SM                   */
-  int32_t reserved;           /* must be 0                                             */
+  int32_t strip_bands;        /* strip kernel: element rows per CTA; 0 = automatic
+                                 (full-height strips when the batch's strips give 2
+                                 CTAs per SM, else chunks of >= 4 rows so that strips
+                                 x chunks comes near 4 per SM; a chunk recomputes the
+                                 z-line segments of the element row above it)        */
   int64_t memory_budget;      /* device bytes the workspaces of solves with ckpt_k = 0
                                  may use; 0 = 85% of (free + this batch's arena) less
                                  512 MiB.  Such batches run as consecutive groups, each

@@ -35,7 +35,7 @@ class Solve(C.Structure):
 
 class LaunchCfg(C.Structure):
     _fields_ = [("tile_ex", C.c_int32), ("tile_ez", C.c_int32), ("threads", C.c_int32),
-                ("graph_chunk", C.c_int32), ("kernel", C.c_int32), ("reserved", C.c_int32),
+                ("graph_chunk", C.c_int32), ("kernel", C.c_int32), ("strip_bands", C.c_int32),
                 ("memory_budget", C.c_int64)]
 
 

@@ -88,6 +88,7 @@ struct SolveDev {
   // geometry
   int nelx, nelz, nxg, nzg, pitch;
   int tiles_x, tiles_z, tile_base;
+  int zchunk;         // strip kernel: element rows per CTA (nelz: full-height strips)
   // program
   int nt, k, nseg, flags, start_tick;
   int it0, it1, decim;
@@ -564,6 +565,12 @@ constexpr int kStripInj = 256;               // receivers per band of one strip 
 constexpr long long kWaitNs = 2000000000LL;  // bounded mbarrier waits: 2 s
 // floats ahead of the ring: mbarriers (64), D (64), beta (16), the band's z-table rows (48)
 constexpr int kStripHdr = 192;
+// The strip kernel's operator constants: the GLL derivative matrix D and the factors beta
+// depend only on the order, so each device keeps one copy per order in constant memory
+// (filled at plan creation); FMAs take them as uniform constant operands, which keeps 30
+// registers free for the band's work.
+__constant__ float c_D[kMaxN + 1][64];
+__constant__ float c_B[kMaxN + 1][8];
 
 __host__ __device__ inline int strip_ew_max(int N) { return (kStripCols - N - 1) / N; }
 __host__ __device__ inline int strip_bw(int N) { return (kStripCols + 3 + 3) & ~3; }  // smem row
@@ -622,30 +629,6 @@ __device__ __forceinline__ void bulk_load(void* dst, const void* src, unsigned b
       : "memory");
 }
 
-#ifndef SEM_TMA_STORE
-#define SEM_TMA_STORE 0
-#endif
-#ifndef SEM_ISSUE_LAST
-#define SEM_ISSUE_LAST 0
-#endif
-// shared -> global bulk copy (16-byte aligned addresses, size a multiple of 16)
-__device__ __forceinline__ void bulk_store(void* dst, const void* src, unsigned bytes) {
-  asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;" ::"l"(dst),
-               "r"(smem_addr(src)), "r"(bytes)
-               : "memory");
-}
-__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
-// this thread's bulk stores have finished reading shared memory
-__device__ __forceinline__ void bulk_wait_read() {
-  asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
-}
-// this thread's bulk stores are complete
-__device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
-// generic-proxy shared-memory writes become visible to the async (bulk copy) proxy
-__device__ __forceinline__ void fence_proxy_async_smem() {
-  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-}
-
 __host__ __device__ inline long long strip_stage_floats(int N, bool adj) {
   const int nfloat = adj ? 4 : 3;  // cur, c2, v (+ forward field)
   const int ndouble = adj ? 1 : 0;  // gradient accumulator
@@ -684,8 +667,11 @@ __device__ __forceinline__ void load_seg(const float* p, float (&u)[N + 1], unsi
   }
 }
 
-// One tick of one strip, instantiated for forward-like ticks (FWD, FINAL, REPLAY) and for
-// adjoint ticks so that neither carries the other's branches.
+// One tick of one strip chunk (element rows [zb0, zb1) of one strip), instantiated for
+// forward-like ticks (FWD, FINAL, REPLAY) and for adjoint ticks so that neither carries
+// the other's branches.  A chunk below the first starts with a halo band (element row
+// zb0 - 1): only its z-line segments (the carry into row zb0 * N) and its adjoint
+// injection carry are computed there; the chunk above owns that band.
 template <int N, bool ADJ>
 __device__ __forceinline__ void strip_tick(const SolveDev& S, const int act, const int t,
                                            const int seg, float* smem, int* s_abort) {
@@ -701,7 +687,14 @@ __device__ __forceinline__ void strip_tick(const SolveDev& S, const int act, con
 
   // ---------------- strip geometry (tiles_z = elements per strip)
   const int nelx = S.nelx, nelz = S.nelz, nxg = S.nxg, nzg = S.nzg, pitch = S.pitch;
-  const int strip = blockIdx.x - S.tile_base;
+  const int zch = S.zchunk > 0 ? S.zchunk : nelz;          // element rows per chunk
+  const int nzc = (nelz + zch - 1) / zch;                   // chunks per strip
+  const int local = blockIdx.x - S.tile_base;
+  const int strip = local / nzc, chunk = local - strip * nzc;
+  const int zb0 = chunk * zch, zb1 = min(nelz, zb0 + zch);  // owned element rows
+  const bool has_halo = zb0 > 0 && !final_only;
+  const int ezs = zb0 - (has_halo ? 1 : 0);                 // first band processed
+  const int nbands = zb1 - ezs;
   const int EW = S.tiles_z;
   const int e0 = strip * EW, e1 = min(e0 + EW, nelx);
   const int sx0 = e0 * N;                                   // first owned column
@@ -715,17 +708,10 @@ __device__ __forceinline__ void strip_tick(const SolveDev& S, const int act, con
   const int gx = sx0 + tid;                                 // this thread's owned column
   const bool owned = gx < so1;
   const int sc = tid + N + off;                             // its smem column
-  // owned columns [h0, h1) leave by bulk stores of whole rows from the ring slot (16-byte
-  // aligned on both sides); the rest by plain stores from the owner thread
-  const int h0 = SEM_TMA_STORE ? ((sx0 + 3) & ~3) : so1, h1 = SEM_TMA_STORE ? (so1 & ~3) : so1;
-  const bool by_bulk = SEM_TMA_STORE && h1 > h0 && gx >= h0 && gx < h1;
 
   // ---------------- shared memory
   unsigned long long* bars = reinterpret_cast<unsigned long long*>(smem);
-  int* const done = reinterpret_cast<int*>(smem + 32);      // per slot: warps past phase B
-  float* const sD = smem + 64;
-  float* const sB = sD + 64;
-  float* const sTz = sB + 16;                     // [2][3][8] band rows of 1/mz, Rz, dz
+  float* const sTz = smem + 64 + 64 + 16;         // [2][3][8] band rows of 1/mz, Rz, dz
   const long long stage_f = strip_stage_floats(N, ADJ);
   float* const stages = smem + kStripHdr;
   float* const xs0 = stages + NST * stage_f;      // 2 exchange buffers: Xs [NP][SEGS][NP] (+ SXs)
@@ -759,17 +745,15 @@ __device__ __forceinline__ void strip_tick(const SolveDev& S, const int act, con
   const int nload = final_only ? 1 : NF;
 
   if (tid == 0) {
-    for (int s2 = 0; s2 < NST; ++s2) { mbar_init(bars + s2, 1); done[s2] = 0; }
+    for (int s2 = 0; s2 < NST; ++s2) mbar_init(bars + s2, 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
-  for (int i = tid; i < NP * NP; i += NT) sD[i] = S.D[i];
-  if (tid < NP) sB[tid] = S.beta[tid];
   __syncthreads();
 
-  // TMA: element row `ez` of every field into ring slot ez % NST (one warp: lane 0 posts
-  // the expected bytes, then each lane issues row copies)
+  // TMA: element row `ez` of every field into ring slot (ez - ezs) % NST (one warp: lane 0
+  // posts the expected bytes, then each lane issues row copies)
   auto issue = [&](int ez) {
-    const int slot = ez % NST;
+    const int slot = (ez - ezs) % NST;
     float* st = stages + slot * stage_f;
     const unsigned rowb = (unsigned)(ce - cs) * 4u;
     const int nd = ADJ ? NP : 0;
@@ -791,16 +775,11 @@ __device__ __forceinline__ void strip_tick(const SolveDev& S, const int act, con
     }
   };
   if (warp == 0)
-    for (int ez = 0; ez < min(NST, nelz); ++ez) issue(ez);
+    for (int r = 0; r < min(NST, nbands); ++r) issue(ezs + r);
 
-  // D and beta in registers (uniform across threads)
-  float Dr[NP][NP], Bt[NP];
-#pragma unroll
-  for (int a = 0; a < NP; ++a) {
-    Bt[a] = sB[a];
-#pragma unroll
-    for (int b = 0; b < NP; ++b) Dr[a][b] = sD[a * NP + b];
-  }
+  // D and beta: per-order constants (c_D[N], c_B[N])
+#define Dr(a, b) c_D[N][(a) * NP + (b)]
+#define Bt(a) c_B[N][(a)]
   float ixv = 0.f, Rxv = 0.f, dxv = 0.f;
   if (owned) { ixv = __ldg(S.tx + gx); Rxv = __ldg(S.tx + nxg + gx); dxv = __ldg(S.tx + 2 * nxg + gx); }
   // this column's x-segment results: its element's segment at local index ia, or on an
@@ -836,20 +815,22 @@ __device__ __forceinline__ void strip_tick(const SolveDev& S, const int act, con
   // receiver / injection list bounds of the current band, fetched one band ahead
   const int li0 = strip * nelz;
   int rec_lo = 0, rec_hi = 0, inj_lo = 0, inj_hi = 0;
-  if (rec_on) { rec_lo = S.rec_tile_off[li0]; rec_hi = S.rec_tile_off[li0 + 1]; }
-  if (ADJ && in_win) { inj_lo = S.inj_tile_off[li0]; inj_hi = S.inj_tile_off[li0 + 1]; }
+  if (rec_on) { rec_lo = S.rec_tile_off[li0 + ezs]; rec_hi = S.rec_tile_off[li0 + ezs + 1]; }
+  if (ADJ && in_win) { inj_lo = S.inj_tile_off[li0 + ezs]; inj_hi = S.inj_tile_off[li0 + ezs + 1]; }
   // z-table rows: threads tid < 3 NP stage entry (tk, ta) of each band, fetched a band ahead
   const bool tz_thr = !final_only && tid < 3 * NP;
   const int tk = tid / NP, ta = tid - tk * NP;
-  float tz_next = tz_thr ? __ldg(tzp + tk * nzg + ta) : 0.f;
+  float tz_next = tz_thr ? __ldg(tzp + tk * nzg + ezs * N + ta) : 0.f;
 
   float zc = 0.f, szc = 0.f;  // z-line carries into the next band's first row
   bool bad = false;
   int abort_ez = -1;
-  int gb = gx;                // offset of (row ez * N, column gx) in a field
+  int gb = gx + ezs * N * pitch;  // offset of (row ez * N, column gx) in a field
 
-  for (int ez = 0; ez < nelz; ++ez, gb += N * pitch) {
-    const int slot = ez % NST;
+  for (int rel = 0; rel < nbands; ++rel, gb += N * pitch) {
+    const int ez = ezs + rel;      // rel: band index within this chunk's ring sequence
+    const int slot = rel % NST;
+    const bool halo = has_halo && rel == 0;
     const float* st = stages + slot * stage_f;
     const float* Bs = st;
     const float* Cs = st + NP * BW;
@@ -860,20 +841,20 @@ __device__ __forceinline__ void strip_tick(const SolveDev& S, const int act, con
     float* const SXs = Xs + NP * SEGS * NP;
     float* const tzb = sTz + (ez & 1) * 24;
     const int r0 = rec_lo, r1 = rec_hi, j0 = inj_lo, j1 = inj_hi;
-    if (ez + 1 < nelz) {
+    if (rel + 1 < nbands) {
       if (rec_on) { rec_lo = rec_hi; rec_hi = S.rec_tile_off[li0 + ez + 2]; }
       if (ADJ && in_win) { inj_lo = inj_hi; inj_hi = S.inj_tile_off[li0 + ez + 2]; }
     }
     if (tz_thr) {
       tzb[tk * 8 + ta] = tz_next;
-      if (ez + 1 < nelz) tz_next = __ldg(tzp + tk * nzg + (ez + 1) * N + ta);
+      if (rel + 1 < nbands) tz_next = __ldg(tzp + tk * nzg + (ez + 1) * N + ta);
     }
     // a failed wait records the first band that failed; every thread tests "failed at or
     // before this band" after the band's barrier, so all threads leave at the same band
-    if (!mbar_wait(bars + slot, (unsigned)((ez / NST) & 1))) atomicMin(s_abort, ez);
+    if (!mbar_wait(bars + slot, (unsigned)((rel / NST) & 1))) atomicMin(s_abort, ez);
     const bool last = (ez == nelz - 1);
 
-    if (rec_on) {  // receivers read out of this band, one warp each
+    if (rec_on && !halo) {  // receivers read out of this band, one warp each
       const int cnt = r1 - r0;
       for (int q = warp; q < cnt; q += NW) {
         const int r = S.rec_tile_ids[r0 + q];
@@ -899,7 +880,7 @@ __device__ __forceinline__ void strip_tick(const SolveDev& S, const int act, con
     if (final_only) {
       __syncthreads();  // done with this slot
       if (*s_abort <= ez) { abort_ez = ez; break; }
-      if (warp == 0 && ez + NST < nelz) issue(ez + NST);
+      if (warp == 0 && rel + NST < nbands) issue(ez + NST);
       continue;
     }
     if (ADJ && in_win && j1 > j0) {  // adjoint source of receivers in this element row
@@ -937,16 +918,16 @@ __device__ __forceinline__ void strip_tick(const SolveDev& S, const int act, con
       for (int a2 = 0; a2 < NP; ++a2) {
         float v = 0.f;
 #pragma unroll
-        for (int b = 0; b < NP; ++b) v = fmaf(Dr[a2][b], u[b], v);
+        for (int b = 0; b < NP; ++b) v = fmaf(Dr(a2, b), u[b], v);
         du[a2] = v;
-        q[a2] = Bt[a2] * c[a2] * v;
+        q[a2] = Bt(a2) * c[a2] * v;
       }
       float* xo = Xs + (a * SEGS + sgi) * NP;
 #pragma unroll
       for (int i = 0; i < NP; ++i) {
         float v = 0.f;
 #pragma unroll
-        for (int a2 = 0; a2 < NP; ++a2) v = fmaf(Dr[a2][i], q[a2], v);
+        for (int a2 = 0; a2 < NP; ++a2) v = fmaf(Dr(a2, i), q[a2], v);
         xo[i] = v;
       }
       if (ADJ) {
@@ -956,13 +937,15 @@ __device__ __forceinline__ void strip_tick(const SolveDev& S, const int act, con
         for (int a2 = 0; a2 < NP; ++a2) {
           float v = 0.f;
 #pragma unroll
-          for (int b = 0; b < NP; ++b) v = fmaf(Dr[a2][b], u[b], v);
-          so[a2] = Bt[a2] * v * du[a2];
+          for (int b = 0; b < NP; ++b) v = fmaf(Dr(a2, b), u[b], v);
+          so[a2] = Bt(a2) * v * du[a2];
         }
       }
     };
-    if (xitem) xline(xa, xsg, mA, nextA);
-    if (last && xitem_last) xline(N, tid, mL, nextL);
+    if (!halo) {
+      if (xitem) xline(xa, xsg, mA, nextA);
+      if (last && xitem_last) xline(N, tid, mL, nextL);
+    }
     // ---- phase A, z-lines: one thread per owned column (the band is the segment)
     float rz[NP], sz[NP];
     if (owned) {
@@ -973,15 +956,15 @@ __device__ __forceinline__ void strip_tick(const SolveDev& S, const int act, con
       for (int a2 = 0; a2 < NP; ++a2) {
         float v = 0.f;
 #pragma unroll
-        for (int b = 0; b < NP; ++b) v = fmaf(Dr[a2][b], u[b], v);
+        for (int b = 0; b < NP; ++b) v = fmaf(Dr(a2, b), u[b], v);
         du[a2] = v;
-        q[a2] = Bt[a2] * Cs[a2 * BW + sc] * v;
+        q[a2] = Bt(a2) * Cs[a2 * BW + sc] * v;
       }
 #pragma unroll
       for (int j = 0; j < NP; ++j) {
         float v = 0.f;
 #pragma unroll
-        for (int a2 = 0; a2 < NP; ++a2) v = fmaf(Dr[a2][j], q[a2], v);
+        for (int a2 = 0; a2 < NP; ++a2) v = fmaf(Dr(a2, j), q[a2], v);
         rz[j] = v;
       }
       if (ADJ) {
@@ -991,17 +974,28 @@ __device__ __forceinline__ void strip_tick(const SolveDev& S, const int act, con
         for (int a2 = 0; a2 < NP; ++a2) {
           float v = 0.f;
 #pragma unroll
-          for (int b = 0; b < NP; ++b) v = fmaf(Dr[a2][b], u[b], v);
-          sz[a2] = Bt[a2] * v * du[a2];
+          for (int b = 0; b < NP; ++b) v = fmaf(Dr(a2, b), u[b], v);
+          sz[a2] = Bt(a2) * v * du[a2];
         }
       }
     }
     __syncthreads();
     if (*s_abort <= ez) { abort_ez = ez; break; }
-#if !SEM_ISSUE_LAST && !SEM_TMA_STORE
-    // every thread is past phase B of band ez - 1: warp 0 refills its slot
-    if (warp == 0 && ez >= 1 && ez - 1 + NST < nelz) issue(ez - 1 + NST);
-#endif
+    // every thread is past phase B of the previous band: warp 0 refills its slot
+    if (warp == 0 && rel >= 1 && rel - 1 + NST < nbands) issue(ez - 1 + NST);
+    if (halo) {  // carries into the first owned row only
+      if (owned) {
+        zc = rz[N];
+        if (ADJ) szc = sz[N];
+        if (ADJ && in_win) {
+          const float carry = sacc[N * NT + tid];
+#pragma unroll
+          for (int a = 1; a < NP; ++a) sacc[a * NT + tid] = 0.f;
+          sacc[tid] = carry;
+        }
+      }
+      continue;
+    }
     // ---- phase B: combine and advance the owned nodes of the band, row by row
     if (owned) {
 #pragma unroll
@@ -1040,15 +1034,9 @@ __device__ __forceinline__ void strip_tick(const SolveDev& S, const int act, con
         float res, vres;
         advance_node(ADJ, damp, Bs[a * BW + sc], Vs[a * BW + sc], X, Z, ixv, Rxv, dxv, izv, Rzv,
                      dzv, extra, res, vres);
-        if (by_bulk) {  // in place: only this thread reads its column of the slot in phase B
-          const_cast<float*>(Bs)[a * BW + sc] = res;
-          const_cast<float*>(Vs)[a * BW + sc] = vres;
-          if (ADJ && grad_on) const_cast<double*>(Gs)[a * BW + sc] = gnew;
-        } else {
-          out[g] = res;
-          vout[g] = vres;
-          if (ADJ && grad_on) gradp[g] = gnew;
-        }
+        out[g] = res;
+        vout[g] = vres;
+        if (ADJ && grad_on) gradp[g] = gnew;
         bad |= !isfinite(res);
       }
       zc = rz[N];
@@ -1060,50 +1048,21 @@ __device__ __forceinline__ void strip_tick(const SolveDev& S, const int act, con
         sacc[tid] = carry;
       }
     }
-    // the last warp past phase B of band ez writes the band's rows out of the slot (bulk
-    // stores) and refills the slot with band ez + NST
-    if (SEM_TMA_STORE || (SEM_ISSUE_LAST && ez + NST < nelz)) {
-      if (SEM_TMA_STORE) fence_proxy_async_smem();
-      __syncwarp();
-      int mine = 0;
-      if (lane == 0) mine = (atomicAdd(done + slot, 1) == NW - 1);
-      if (__shfl_sync(0xffffffffu, mine, 0)) {
-        if (SEM_TMA_STORE && h1 > h0) {
-          const int rows = last ? NP : N;
-          const int nf = (ADJ && grad_on) ? 3 : 2;
-          const unsigned nb = (unsigned)(h1 - h0) * 4u;
-          for (int q = lane; q < rows * nf; q += 32) {
-            const int f = q / rows, a = q - f * rows;
-            const long long grow = (long long)(ez * N + a) * pitch + h0;
-            const int srow = a * BW + (h0 - X0);
-            if (f == 0) bulk_store(out + grow, Bs + srow, nb);
-            else if (f == 1) bulk_store(vout + grow, Vs + srow, nb);
-            else bulk_store(gradp + grow, Gs + srow, 2u * nb);
-          }
-          bulk_commit();
-          bulk_wait_read();
-          __syncwarp();
-        }
-        if (lane == 0) done[slot] = 0;
-        if (ez + NST < nelz) issue(ez + NST);
-      }
-    }
   }
-  if (SEM_TMA_STORE) bulk_wait_all();
   if (abort_ez >= 0) {
-    // drain the copies still in flight (bands abort_ez .. abort_ez + NST - 1) before leaving
+    // drain the copies still in flight (issued bands from abort_ez on) before leaving
     if (tid == 0) atomicOr(S.status, SEM_ERR_TIMEOUT);
-    // refills issued so far: bands < NST, and band ez' - 1 + NST at each mid barrier ez' <
-    // abort_ez (or band ez' + NST after phase B of each band ez' < abort_ez)
-    const int issued = (SEM_ISSUE_LAST || SEM_TMA_STORE) ? abort_ez + NST
-                                                         : max(NST, abort_ez + NST - 1);
-    for (int b = abort_ez; b < min(issued, nelz); ++b)
-      mbar_wait(bars + b % NST, (unsigned)((b / NST) & 1));
-    if (SEM_TMA_STORE) bulk_wait_all();  // bulk stores of earlier bands still read the ring
+    // issued so far: bands rel < NST, then rel' - 1 + NST at the barrier of each band rel' <
+    // the aborting one (final read-out ticks: rel' + NST after each band rel' before it)
+    const int ra = abort_ez - ezs;
+    const int issued = min(nbands, final_only ? ra + NST : max(NST, ra + NST - 1));
+    for (int r = ra; r < issued; ++r) mbar_wait(bars + r % NST, (unsigned)((r / NST) & 1));
     return;
   }
   if (__any_sync(0xffffffffu, bad) && lane == 0) atomicOr(S.status, SEM_ERR_NONFINITE);
 }
+#undef Dr
+#undef Bt
 
 template <int N>
 __global__ void __launch_bounds__(kStripCols, (N <= 4) ? SEM_STRIP_MIN_BLOCKS : 3)
@@ -1289,6 +1248,28 @@ int upload(T** dst, const T* src, size_t n) {
   return SEM_OK;
 }
 
+// fills c_D[N] / c_B[N] on the current device once; later plans of the same order must
+// bring the same operators
+int set_order_constants(int dev, int N, const double* D, const double* beta) {
+  static std::mutex mu;
+  static std::map<std::pair<int, int>, std::vector<float>> have;
+  const int NP = N + 1;
+  std::vector<float> v((size_t)NP * NP + NP);
+  for (int i = 0; i < NP * NP; ++i) v[i] = (float)D[i];
+  for (int i = 0; i < NP; ++i) v[NP * NP + i] = (float)beta[i];
+  std::lock_guard<std::mutex> lk(mu);
+  auto it = have.find(std::make_pair(dev, N));
+  if (it != have.end()) {
+    if (it->second != v)
+      return fail(SEM_ERR_ARG, "GLL operators differ from an earlier plan of the same order");
+    return SEM_OK;
+  }
+  CUDA_TRY(cudaMemcpyToSymbol(c_D, v.data(), sizeof(float) * NP * NP, sizeof(float) * 64 * N));
+  CUDA_TRY(cudaMemcpyToSymbol(c_B, v.data() + NP * NP, sizeof(float) * NP, sizeof(float) * 8 * N));
+  have[std::make_pair(dev, N)] = v;
+  return SEM_OK;
+}
+
 int upload_f32(float** dst, const double* src, size_t n) {
   std::vector<float> tmp(n);
   for (size_t i = 0; i < n; ++i) tmp[i] = (float)src[i];
@@ -1302,6 +1283,27 @@ int tiles_of(const sem_plan_s* p, int tex, int tez, int* tx, int* tz) {
   *tz = (p->nelz + tez - 1) / tez;
   return (*tx) * (*tz);
 }
+
+// strip kernel: strips of a plan and elements per strip (balanced)
+int strips_of(const sem_plan_s* p, int* ew_out) {
+  const int ewm = strip_ew_max(p->npol);
+  int ns = (p->nelx + ewm - 1) / ewm;
+  const int ew = (p->nelx + ns - 1) / ns;
+  ns = (p->nelx + ew - 1) / ew;
+  if (ew_out) *ew_out = ew;
+  return ns;
+}
+constexpr int kMinChunk = 4;  // element rows per strip CTA at least: halo band <= 1/4 extra
+// element rows per strip CTA: full height when the strips alone give every SM two CTAs,
+// else chunks of at least kMinChunk rows so that strips x chunks comes near four per SM
+int strip_zchunk(long long total_strips, int nelz_max, int sms, int forced) {
+  if (forced > 0) return forced;
+  if (total_strips >= 2LL * sms) return nelz_max;
+  const long long want = (4LL * sms + total_strips - 1) / total_strips;  // chunks per strip
+  return std::max(kMinChunk, (int)((nelz_max + want - 1) / want));
+}
+// automatic variant choice: strips when the chunked strip grid gives every SM two CTAs
+bool strip_fills(long long min_chunk_ctas, int sms) { return min_chunk_ctas >= 2LL * sms; }
 
 int upload_lists(const sem_plan_s* p, std::pair<int, int> key, std::vector<std::vector<int>>& rec,
                  std::vector<std::vector<int>>& inj, sem_plan_s::Lists* out) {
@@ -1445,6 +1447,7 @@ struct sem_batch_s {
   long long cta_cap = 0;
   long long last_launches = 0;
   int last_kernel = 0;
+  int last_zchunk = 0;
   int last_groups = 0;
   long long last_ticks = 0;             // tick rounds of the last sem_run (all groups)
   std::vector<cudaEvent_t> tick_ev;     // per group: before / after its tick loop
@@ -1496,7 +1499,8 @@ int sem_plan_create(const sem_plan_desc_t* d, sem_plan_t** out) {
       return fail(SEM_ERR_ARG, "receiver element base outside the mesh");
     }
   }
-  if ((rc = upload_f32(&p->D, d->gll_D, NP * NP)) || (rc = upload_f32(&p->beta, d->gll_beta, NP)) ||
+  if ((rc = set_order_constants(p->device, d->npol, d->gll_D, d->gll_beta)) ||
+      (rc = upload_f32(&p->D, d->gll_D, NP * NP)) || (rc = upload_f32(&p->beta, d->gll_beta, NP)) ||
       (rc = upload_f32(&p->tx, d->tab_x, 3 * nxg)) || (rc = upload_f32(&p->tz, d->tab_z, 3 * nzg)) ||
       (rc = upload_f32(&p->src_term, d->src_term, d->nt)) ||
       (rc = upload(&p->rec_base, d->rec_base, 2 * (size_t)d->nrec)) ||
@@ -1584,20 +1588,25 @@ static int run_group(sem_batch_t* b, const sem_solve_t* solves, int32_t n,
     const int nt = s.plan->nt;
     prog[i] = nt + ((s.flags & SEM_F_SHIFT) ? 1 : 0) + (adj ? 1 + nt + kk[i] * (nseg[i] - 1) : 0);
   }
-  // kernel variant: strips when the batch alone fills the GPU, tiles otherwise
-  bool use_strip = (cfg.kernel == 2);
-  if (cfg.kernel == 0) {
-    int dev = 0, sms = 148;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    long long strips = 0;
-    for (int i = 0; i < n; ++i) {
-      const sem_plan_s* p = solves[i].plan;
-      strips += (p->nelx + strip_ew_max(p->npol) - 1) / strip_ew_max(p->npol);
-    }
-    use_strip = strips >= sms;
+  // kernel variant: strips (chunked in z when the strips alone do not fill the GPU) when
+  // that grid gives every SM two CTAs, tiles otherwise
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  long long total_strips = 0, min_chunk_ctas = 0;
+  int nelz_max = 1;
+  for (int i = 0; i < n; ++i) {
+    const sem_plan_s* p = solves[i].plan;
+    const int ns = strips_of(p, nullptr);
+    total_strips += ns;
+    min_chunk_ctas += (long long)ns * ((p->nelz + kMinChunk - 1) / kMinChunk);
+    nelz_max = std::max(nelz_max, p->nelz);
   }
+  bool use_strip = (cfg.kernel == 2);
+  if (cfg.kernel == 0) use_strip = strip_fills(min_chunk_ctas, sms);
+  const int zchunk = use_strip ? strip_zchunk(total_strips, nelz_max, sms, cfg.strip_bands) : 0;
   b->last_kernel = use_strip ? 2 : 1;
+  b->last_zchunk = zchunk;
   if (total > b->arena_bytes) {
     cudaFree(b->arena);
     b->arena = nullptr;
@@ -1626,11 +1635,8 @@ static int run_group(sem_batch_t* b, const sem_solve_t* solves, int32_t n,
     sem_plan_s::Lists L;
     int ntx, ntz, ntiles, rc;
     if (use_strip) {
-      const int ewm = strip_ew_max(p->npol);
-      ntx = (p->nelx + ewm - 1) / ewm;             // strips
-      ntz = (p->nelx + ntx - 1) / ntx;             // elements per strip (balanced)
-      ntx = (p->nelx + ntz - 1) / ntz;
-      ntiles = ntx;
+      ntx = strips_of(p, &ntz);                    // strips, elements per strip
+      ntiles = ntx * ((p->nelz + zchunk - 1) / zchunk);
       rc = get_strip_lists(p, ntz, &L);
     } else {
       ntiles = tiles_of(p, cfg.tile_ex, cfg.tile_ez, &ntx, &ntz);
@@ -1646,6 +1652,7 @@ static int run_group(sem_batch_t* b, const sem_solve_t* solves, int32_t n,
     SolveDev& d = b->h_solves[oi];
     d.nelx = p->nelx; d.nelz = p->nelz; d.nxg = p->nxg; d.nzg = p->nzg; d.pitch = p->pitch;
     d.tiles_x = ntx; d.tiles_z = ntz;
+    d.zchunk = use_strip ? zchunk : p->nelz;
     d.tile_base = (int)(b->h_cta.size() - G.cta0);
     d.nt = p->nt; d.k = kk[i]; d.nseg = nseg[i]; d.flags = s.flags; d.start_tick = 0;
     d.it0 = s.it0; d.it1 = s.it1; d.decim = s.decim;
@@ -1851,8 +1858,7 @@ int auto_schedule(const sem_solve_t* sv, int n, const sem_launch_cfg_t& cfg, lon
   std::vector<long long> strips(n), tiles(n);
   for (int i = 0; i < n; ++i) {
     const sem_plan_s* p = sv[i].plan;
-    const int ewm = strip_ew_max(p->npol);
-    strips[i] = (p->nelx + ewm - 1) / ewm;
+    strips[i] = strips_of(p, nullptr);
     int tx, tz;
     tiles[i] = tiles_of(p, cfg.tile_ex, cfg.tile_ez, &tx, &tz);
   }
@@ -1911,7 +1917,8 @@ int auto_schedule(const sem_solve_t* sv, int n, const sem_launch_cfg_t& cfg, lon
       }
       const int k = lo;
       // modelled time: forward-like ticks (forward + replay) and adjoint ticks (x1.5)
-      long long fwd_ticks = 0, adj_ticks = 0, nstrip = 0, ntile = 0;
+      long long fwd_ticks = 0, adj_ticks = 0, nstrip = 0, ntile = 0, nchunk_min = 0;
+      int nelz_max = 1;
       for (int i = b0; i < b1; ++i) {
         const sem_solve_t& s = sv[i];
         const int nt = s.plan->nt;
@@ -1922,9 +1929,16 @@ int auto_schedule(const sem_solve_t* sv, int n, const sem_launch_cfg_t& cfg, lon
         if (adj) adj_ticks = std::max(adj_ticks, (long long)nt);
         nstrip += strips[i];
         ntile += tiles[i];
+        nchunk_min += strips[i] * ((s.plan->nelz + kMinChunk - 1) / kMinChunk);
+        nelz_max = std::max(nelz_max, s.plan->nelz);
       }
-      const bool strip = cfg.kernel == 2 || (cfg.kernel == 0 && nstrip >= sms);
-      const double per_tick = strip ? tick_rounds(nstrip, slots_strip, sms) : tick_rounds(ntile, slots_tile, sms);
+      const bool strip = cfg.kernel == 2 || (cfg.kernel == 0 && strip_fills(nchunk_min, sms));
+      long long nstrip_ctas = 0;
+      if (strip) {
+        const int zc = strip_zchunk(nstrip, nelz_max, sms, cfg.strip_bands);
+        for (int i = b0; i < b1; ++i) nstrip_ctas += strips[i] * ((sv[i].plan->nelz + zc - 1) / zc);
+      }
+      const double per_tick = strip ? tick_rounds(nstrip_ctas, slots_strip, sms) : tick_rounds(ntile, slots_tile, sms);
       cost += per_tick * ((double)fwd_ticks + 1.5 * (double)adj_ticks);
       plan.push_back(GroupPlan{b0, b1, k});
     }
@@ -1954,6 +1968,7 @@ int sem_run(sem_batch_t* b, const sem_solve_t* solves, int32_t n, const sem_laun
   if (cfg.kernel < 0 || cfg.kernel > 2) return fail(SEM_ERR_ARG, "kernel must be 0 (auto), 1 (tile), 2 (strip)");
   if (cfg.threads < 32 || cfg.threads > 256 || cfg.threads % 32) cfg.threads = 256;
   if (cfg.memory_budget < 0) return fail(SEM_ERR_ARG, "memory_budget must be >= 0");
+  if (cfg.strip_bands < 0) return fail(SEM_ERR_ARG, "strip_bands must be >= 0");
   b->last_launches = 0;
   b->last_groups = 0;
   b->last_ticks = 0;
@@ -2381,6 +2396,7 @@ int sem_engine_step(sem_engine_t* e, void* stream_v) {
     SolveDev& d = e->h_solves[oi];
     d.nelx = p->nelx; d.nelz = p->nelz; d.nxg = p->nxg; d.nzg = p->nzg; d.pitch = p->pitch;
     d.tiles_x = ntx; d.tiles_z = ntz;
+    d.zchunk = p->nelz;  // full-height strips
     d.tile_base = (int)(e->h_cta.size() - G.cta0);
     d.nt = p->nt; d.k = j->k; d.nseg = j->nseg; d.flags = j->s.flags;
     d.start_tick = (int)j->start;

@@ -70,13 +70,14 @@ def choose_ckpt_k(plan, n_solves, budget_bytes=None):
 class Batch:
     """Owns a ``sem_batch_t`` (workspace arena, descriptors, tick counter)."""
 
-    def __init__(self, tile=(8, 8), threads=256, graph_chunk=0, kernel=0):
+    def __init__(self, tile=(8, 8), threads=256, graph_chunk=0, kernel=0, strip_bands=0):
         lib = _lib.load()
         h = C.c_void_p()
         _lib.check(lib.sem_batch_create(C.byref(h)))
         self.handle, self._lib = h, lib
         self.tile, self.threads, self.graph_chunk = tuple(tile), int(threads), int(graph_chunk)
         self.kernel = int(kernel)  # 0 auto, 1 tile, 2 strip
+        self.strip_bands = int(strip_bands)  # strip kernel: element rows per CTA (0 auto)
         self._side = None
 
     def __del__(self):
@@ -170,7 +171,7 @@ class Batch:
         t = tile or self.tile
         cfg = _lib.LaunchCfg(int(t[0]), int(t[1]), self.threads,
                              int(self.graph_chunk if graph_chunk is None else graph_chunk),
-                             int(self.kernel if kernel is None else kernel), 0,
+                             int(self.kernel if kernel is None else kernel), self.strip_bands,
                              int(memory_budget or 0))
         cur = torch.cuda.current_stream()
         if cfg.graph_chunk > 0 and cur.cuda_stream == 0:

@@ -89,3 +89,31 @@ def test_strip_exact_mode_and_window():
         outs.append(sp)
     assert rel_l2(outs[0].grad.cpu().numpy(), outs[1].grad.cpu().numpy()) <= 1e-6
     assert abs(float(outs[0].loglik.item()) - float(outs[1].loglik.item())) <= 1e-6 * abs(float(outs[0].loglik.item()))
+
+
+@pytest.mark.parametrize("name", ["inject_n1", "inject_n3", "inject_n6", "circle_n5", "layered_cfg0"])
+def test_strip_z_chunks_bitwise(name):
+    # strips split into chunks of 1..3 element rows (each recomputing the z-line segments
+    # of the row above) give bitwise the results of full-height strips
+    g = load(name)
+    plan = plan_for(g["config"], g["dt"], g["nt"])
+    nelz = g["config"]["domain"]["nelem_z"]
+
+    def run(bands, **kw):
+        s = SolveSpec(plan, dev(g["velocity"]), **kw)
+        Batch(kernel=2, strip_bands=bands).run([s])
+        return s
+    y = dev(aligned_obs(g))
+    inv = 1.0 / (float(g["sigma"]) ** 2 + 1e-24)
+    it1 = max(2, plan.nt // 2)
+    for kw in (dict(), dict(shift=True), dict(adjoint=True, y_obs=y, inv_sigma2=inv),
+               dict(adjoint=True, exact=True, y_obs=y[: -(-(it1 - 1) // 3)], inv_sigma2=inv,
+                    window=(1, it1, 3))):
+        full = run(nelz, **kw)
+        for bands in (1, 2, 3):
+            part = run(bands, **kw)
+            assert int(part.status.item()) == 0
+            assert torch.equal(full.rec, part.rec), (name, bands, kw.keys())
+            if full.grad is not None:
+                assert torch.equal(full.grad, part.grad), (name, bands)
+                assert torch.equal(full.loglik, part.loglik)

@@ -161,3 +161,53 @@ def test_strip_receiver_lists_cover():
                     listed.append((s0, s1))
             for i in range(N + 1):
                 assert sum(s0 <= bx + i < s1 for s0, s1 in listed) == 1
+
+
+def zchunk_of(total_strips, nelz_max, sms=148, forced=0, min_chunk=4):
+    """strip_zchunk in sem_kernels.cu."""
+    if forced > 0:
+        return forced
+    if total_strips >= 2 * sms:
+        return nelz_max
+    want = -(-4 * sms // total_strips)
+    return max(min_chunk, -(-nelz_max // want))
+
+
+def test_strip_zchunk_rule():
+    assert zchunk_of(512, 50) == 50                  # 128 models of 100x50: full height
+    assert zchunk_of(14, 200) == 5                   # one 400x200 mesh: 14 strips x 40 chunks
+    assert zchunk_of(4, 50) == 4                     # small mesh: at least 4 rows per chunk
+    assert zchunk_of(200, 50, forced=3) == 3
+
+
+@pytest.mark.parametrize("nelz,zch", [(1, 1), (5, 1), (5, 2), (50, 4), (50, 50), (200, 5), (7, 3)])
+def test_strip_chunks_partition_and_ring(nelz, zch):
+    nzc = -(-nelz // zch)
+    owner = np.zeros(nelz, dtype=int)
+    for final_only in (False, True):
+        for NST in (2, 3):
+            owner[:] = 0
+            for chunk in range(nzc):
+                zb0, zb1 = chunk * zch, min(nelz, chunk * zch + zch)
+                assert zb1 > zb0
+                has_halo = zb0 > 0 and not final_only
+                ezs = zb0 - (1 if has_halo else 0)
+                nbands = zb1 - ezs
+                assert ezs >= 0
+                # ring: band rel uses slot rel % NST with parity (rel // NST) & 1; a slot is
+                # refilled (band rel - 1 + NST at the barrier of band rel) only after the
+                # band that used it (rel - 1) is done, and every band is issued once
+                issued = list(range(min(NST, nbands)))
+                for rel in range(nbands):
+                    assert rel in issued
+                    if final_only:
+                        if rel + NST < nbands:
+                            issued.append(rel + NST)
+                    elif rel >= 1 and rel - 1 + NST < nbands:
+                        issued.append(rel - 1 + NST)
+                assert sorted(issued) == list(range(nbands))
+                for rel in range(nbands):
+                    ez = ezs + rel
+                    if not (has_halo and rel == 0):
+                        owner[ez] += 1
+            assert (owner == 1).all()
