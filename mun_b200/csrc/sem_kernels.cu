@@ -549,8 +549,11 @@ __global__ void __launch_bounds__(256) sem_tick_kernel(const SolveDev* __restric
 // one thread per owned column combines the segment results and advances the band's
 // nodes.  Arithmetic order matches the tile kernel (bitwise-equal results).
 // ----------------------------------------------------------------------------
+#ifndef SEM_GRAD_STAGE
+#define SEM_GRAD_STAGE 0
+#endif
 #ifndef SEM_STAGES_ADJ
-#define SEM_STAGES_ADJ 2
+#define SEM_STAGES_ADJ 3
 #endif
 #ifndef SEM_STRIP_MIN_BLOCKS
 #define SEM_STRIP_MIN_BLOCKS 4
@@ -631,7 +634,7 @@ __device__ __forceinline__ void bulk_load(void* dst, const void* src, unsigned b
 
 __host__ __device__ inline long long strip_stage_floats(int N, bool adj) {
   const int nfloat = adj ? 4 : 3;  // cur, c2, v (+ forward field)
-  const int ndouble = adj ? 1 : 0;  // gradient accumulator
+  const int ndouble = (adj && SEM_GRAD_STAGE) ? 1 : 0;  // gradient accumulator
   return ((long long)(nfloat + 2 * ndouble) * (N + 1) * strip_bw(N) + 31) & ~31LL;
 }
 // exchange arrays: x-segment results Xs[rows][segments][N+1] (+ sensitivity), z-segment
@@ -756,7 +759,7 @@ __device__ __forceinline__ void strip_tick(const SolveDev& S, const int act, con
     const int slot = (ez - ezs) % NST;
     float* st = stages + slot * stage_f;
     const unsigned rowb = (unsigned)(ce - cs) * 4u;
-    const int nd = ADJ ? NP : 0;
+    const int nd = (ADJ && SEM_GRAD_STAGE) ? NP : 0;
     const int ncopy = nload * NP + nd;
     if (lane == 0) mbar_expect_tx(bars + slot, (unsigned)(nload * NP) * rowb + (unsigned)nd * rowb * 2u);
     __syncwarp();
@@ -851,6 +854,14 @@ __device__ __forceinline__ void strip_tick(const SolveDev& S, const int act, con
     }
     // a failed wait records the first band that failed; every thread tests "failed at or
     // before this band" after the band's barrier, so all threads leave at the same band
+#if !SEM_GRAD_STAGE
+    // the owner's gradient rows of this band, loaded now and used in phase B
+    double gpre[N];
+    if (ADJ && grad_on && owned && !halo) {
+#pragma unroll
+      for (int a = 0; a < N; ++a) gpre[a] = gradp[gb + a * pitch];
+    }
+#endif
     if (!mbar_wait(bars + slot, (unsigned)((rel / NST) & 1))) atomicMin(s_abort, ez);
     const bool last = (ez == nelz - 1);
 
@@ -1029,7 +1040,11 @@ __device__ __forceinline__ void strip_tick(const SolveDev& S, const int act, con
           extra = (ez * N + a == src_row) ? src_val : 0.f;
         } else {
           extra = in_win ? sacc[a * NT + tid] : 0.f;
+#if SEM_GRAD_STAGE
           if (grad_on) gnew = Gs[a * BW + sc] + (double)(Rzv * SX + Rxv * SZ);
+#else
+          if (grad_on) gnew = (a < N ? gpre[a < N ? a : 0] : gradp[g]) + (double)(Rzv * SX + Rxv * SZ);
+#endif
         }
         float res, vres;
         advance_node(ADJ, damp, Bs[a * BW + sc], Vs[a * BW + sc], X, Z, ixv, Rxv, dxv, izv, Rzv,

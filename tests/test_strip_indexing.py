@@ -90,15 +90,16 @@ def audit(N, nelx, nelz):
     assert (owner == 1).all()
 
 
-STAGES, STAGES_ADJ, INJ, HDR, NBUF = 3, 2, 256, 192, 2
+STAGES, STAGES_ADJ, INJ, HDR, NBUF = 3, 3, 256, 192, 2
 
 
 def smem_bytes(N, adj):
-    """strip_smem_floats(N, adj) * 4: header, ring slots, exchange buffers, injection."""
+    """strip_smem_floats(N, adj) * 4: header, ring slots, exchange buffers, injection.
+    The float64 gradient is not staged (owner threads load their rows)."""
     NP, segs = N + 1, ew_max(N) + 1
 
     def stage(a):
-        return (((4 if a else 3) + (2 if a else 0)) * NP * bw(N) + 31) & ~31
+        return ((4 if a else 3) * NP * bw(N) + 31) & ~31
 
     def xch(a):
         f = NBUF * (2 if a else 1) * NP * segs * NP + ((NP * THREADS + INJ) if a else 0)
