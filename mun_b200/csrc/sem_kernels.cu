@@ -151,6 +151,16 @@ __device__ __forceinline__ void decode(const SolveDev& s, int sig, int& act, int
   else { act = A_ADJ; t = (j + 1) * s.k - 1 - (w - s.k); }
 }
 
+// Programmatic dependent launch: a tick kernel lets the next tick's grid start launching
+// at once (its CTAs run their prologue in this grid's tail) and, before touching any
+// field, waits until the previous grid in the stream has completed.  Every CTA waits
+// before it may exit, so grid completion stays ordered along the stream.  Both are no-ops
+// for a plain launch.
+__device__ __forceinline__ void grid_dep_launch() {
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+__device__ __forceinline__ void grid_dep_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
 // where b_t / v_t live during the forward sweep (t in [0, nt])
 __device__ __forceinline__ const float* fwd_b(const SolveDev& s, int t) {
   if (!(s.flags & F_ADJ)) return s.W + (long long)(t & 1) * s.fstride;
@@ -224,11 +234,12 @@ template <int N>
 __global__ void __launch_bounds__(256) sem_tick_kernel(const SolveDev* __restrict__ solves,
                                                        const int* __restrict__ cta_solve,
                                                        const int* __restrict__ tick_ptr,
-                                                       int tex, int tez) {
+                                                       int tex, int tez, int tick_arg) {
   constexpr int NP = N + 1;
   extern __shared__ float smem[];
   __shared__ SolveDev S;
   __shared__ int s_act, s_t, s_seg;
+  grid_dep_launch();
 
   const int sid = cta_solve[blockIdx.x];
   {
@@ -240,10 +251,11 @@ __global__ void __launch_bounds__(256) sem_tick_kernel(const SolveDev* __restric
   __syncthreads();
   if (threadIdx.x == 0) {
     int act, t, seg;
-    decode(S, *tick_ptr - S.start_tick, act, t, seg);
+    decode(S, (tick_ptr ? *tick_ptr : tick_arg) - S.start_tick, act, t, seg);
     s_act = act; s_t = t; s_seg = seg;
   }
   __syncthreads();
+  grid_dep_wait();  // the previous tick's fields are complete from here on
   const int act = s_act;
   if (act == A_NONE) return;
   const int t = s_t, seg = s_seg;
@@ -549,6 +561,9 @@ __global__ void __launch_bounds__(256) sem_tick_kernel(const SolveDev* __restric
 // one thread per owned column combines the segment results and advances the band's
 // nodes.  Arithmetic order matches the tile kernel (bitwise-equal results).
 // ----------------------------------------------------------------------------
+#ifndef SEM_PDL
+#define SEM_PDL 1
+#endif
 #ifndef SEM_GRAD_STAGE
 #define SEM_GRAD_STAGE 0
 #endif
@@ -839,7 +854,9 @@ __device__ __forceinline__ void strip_tick(const SolveDev& S, const int act, con
     const float* Cs = st + NP * BW;
     const float* Vs = st + 2 * NP * BW;
     const float* Us = st + 3 * NP * BW;
+#if SEM_GRAD_STAGE
     const double* Gs = reinterpret_cast<const double*>(st + NF * NP * BW);
+#endif
     float* const Xs = xs0 + (ez & 1) * XSZ;
     float* const SXs = Xs + NP * SEGS * NP;
     float* const tzb = sTz + (ez & 1) * 24;
@@ -1082,10 +1099,11 @@ __device__ __forceinline__ void strip_tick(const SolveDev& S, const int act, con
 template <int N>
 __global__ void __launch_bounds__(kStripCols, (N <= 4) ? SEM_STRIP_MIN_BLOCKS : 3)
     sem_strip_kernel(const SolveDev* __restrict__ solves, const int* __restrict__ cta_solve,
-                     const int* __restrict__ tick_ptr, int unused0, int unused1) {
+                     const int* __restrict__ tick_ptr, int unused0, int unused1, int tick_arg) {
   extern __shared__ __align__(128) float smem[];
   __shared__ SolveDev S;
   __shared__ int s_act, s_t, s_seg, s_abort;
+  grid_dep_launch();
 
   const int sid = cta_solve[blockIdx.x];
   {
@@ -1096,10 +1114,11 @@ __global__ void __launch_bounds__(kStripCols, (N <= 4) ? SEM_STRIP_MIN_BLOCKS : 
   __syncthreads();
   if (threadIdx.x == 0) {
     int act, t, seg;
-    decode(S, *tick_ptr - S.start_tick, act, t, seg);
+    decode(S, (tick_ptr ? *tick_ptr : tick_arg) - S.start_tick, act, t, seg);
     s_act = act; s_t = t; s_seg = seg; s_abort = 0x7fffffff;
   }
   __syncthreads();
+  grid_dep_wait();  // the previous tick's fields are complete from here on
   const int act = s_act;
   if (act == A_NONE) return;
   const int t = s_t, seg = s_seg;
@@ -1394,7 +1413,7 @@ int get_strip_lists(const sem_plan_s* p, int ew, sem_plan_s::Lists* out) {
   return upload_lists(p, key, rec, inj, out);
 }
 
-typedef void (*KernelFn)(const SolveDev*, const int*, const int*, int, int);
+typedef void (*KernelFn)(const SolveDev*, const int*, const int*, int, int, int);
 KernelFn strip_kernel_for(int N) {
   switch (N) {
     case 1: return sem_strip_kernel<1>;
@@ -1789,14 +1808,36 @@ static int run_group(sem_batch_t* b, const sem_solve_t* solves, int32_t n,
       while (oi < n && solves[order[oi]].plan->npol == G.N) ++oi;
     }
   }
+  // captured chunks replay with a device tick counter; plain launches pass the tick and
+  // chain through programmatic dependent launch (no counter kernel between ticks)
   auto launch_tick = [&]() -> int {
     for (size_t gi = 0; gi < launches.size(); ++gi) {
       const Launch& Lc = launches[gi];
       Lc.fn<<<(unsigned)Lc.ncta, use_strip ? strip_threads(Lc.N) : cfg.threads, Lc.smem, stream>>>(
-          gdesc[gi], b->d_cta + Lc.cta0, b->d_tick, cfg.tile_ex, cfg.tile_ez);
+          gdesc[gi], b->d_cta + Lc.cta0, b->d_tick, cfg.tile_ex, cfg.tile_ez, 0);
     }
     tick_advance_kernel<<<1, 1, 0, stream>>>(b->d_tick);
     return SEM_OK;
+  };
+  auto launch_tick_pdl = [&](int tick) -> cudaError_t {
+    for (size_t gi = 0; gi < launches.size(); ++gi) {
+      const Launch& Lc = launches[gi];
+      cudaLaunchConfig_t lc = {};
+      lc.gridDim = dim3((unsigned)Lc.ncta);
+      lc.blockDim = dim3(use_strip ? strip_threads(Lc.N) : cfg.threads);
+      lc.dynamicSmemBytes = Lc.smem;
+      lc.stream = stream;
+      cudaLaunchAttribute at[1];
+      at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+      at[0].val.programmaticStreamSerializationAllowed = SEM_PDL ? 1 : 0;
+      lc.attrs = at;
+      lc.numAttrs = 1;
+      const int* no_counter = nullptr;
+      cudaError_t e = cudaLaunchKernelEx(&lc, Lc.fn, gdesc[gi], (const int*)(b->d_cta + Lc.cta0),
+                                         no_counter, cfg.tile_ex, cfg.tile_ez, tick);
+      if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
   };
 
   // ---- the tick loop: plain launches or captured chunks, bracketed by events
@@ -1807,7 +1848,7 @@ static int run_group(sem_batch_t* b, const sem_solve_t* solves, int32_t n,
   }
   cudaEvent_t ev_begin = b->tick_ev[b->tick_ev_used], ev_end = b->tick_ev[b->tick_ev_used + 1];
   CUDA_TRY(cudaEventRecord(ev_begin, stream));
-  const long long per_tick = (long long)launches.size() + 1;
+  const long long per_tick = (long long)launches.size() + 1;  // graphed: + counter kernel
   bool graphed = false;
   if (cfg.graph_chunk > 0 && stream != nullptr && stream != cudaStreamLegacy &&
       stream != cudaStreamPerThread) {
@@ -1829,8 +1870,8 @@ static int run_group(sem_batch_t* b, const sem_solve_t* solves, int32_t n,
     cudaGetLastError();  // clear a failed capture
   }
   if (!graphed) {
-    for (int tick = 0; tick < max_prog; ++tick) launch_tick();
-    b->last_launches += (long long)max_prog * per_tick;
+    for (int tick = 0; tick < max_prog; ++tick) CUDA_TRY(launch_tick_pdl(tick));
+    b->last_launches += (long long)max_prog * (long long)launches.size();
   }
   CUDA_TRY(cudaGetLastError());
   CUDA_TRY(cudaEventRecord(ev_end, stream));
@@ -2115,7 +2156,7 @@ int sem_forward_noalloc(const sem_plan_t* p, const double* velocity, float* rec_
   CUDA_TRY(cudaFuncSetAttribute((const void*)fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   for (int tick = 0; tick < p->nt; ++tick) {
     fn<<<ntiles, 256, smem, stream>>>((const SolveDev*)(base + o_desc), (const int*)(base + o_cta),
-                                      (const int*)(base + o_tick), kNoAllocTile, kNoAllocTile);
+                                      (const int*)(base + o_tick), kNoAllocTile, kNoAllocTile, 0);
     tick_advance_kernel<<<1, 1, 0, stream>>>((int*)(base + o_tick));
   }
   if (status_out) copy_status_kernel<<<1, 32, 0, stream>>>((const int*)(base + o_st), status_out);
@@ -2467,7 +2508,7 @@ int sem_engine_step(sem_engine_t* e, void* stream_v) {
       if (c == 0)
         CUDA_TRY(cudaFuncSetAttribute((const void*)fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
       fn<<<(unsigned)G.ncta, use_strip ? strip_threads(G.N) : 256, smem, stream>>>(
-          e->d_solves + G.first, e->d_cta + G.cta0, e->d_tick, e->cfg.tile_ex, e->cfg.tile_ez);
+          e->d_solves + G.first, e->d_cta + G.cta0, e->d_tick, e->cfg.tile_ex, e->cfg.tile_ez, 0);
       e->launches++;
     }
     tick_advance_kernel<<<1, 1, 0, stream>>>(e->d_tick);
