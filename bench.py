@@ -61,6 +61,11 @@ def workload(nmodels=256, nelx=100, nelz=50, nt=3000, nrec=100, seed0=0):
                 npoints=len(coords), dt=dt, nt=nt, sigma=1e-3)
 
 
+def parse_tile(t):
+    """'8x4' -> (8, 4); 'auto' -> (0, 0) (the library picks the shape)."""
+    return (0, 0) if t == "auto" else tuple(int(x) for x in t.split("x"))
+
+
 class Clocks:
     """nvidia-smi sampler running during the timed region."""
 
@@ -188,7 +193,8 @@ def run_plain(args):
     obs = SolveSpec(plan, torch.as_tensor(v_obs, device=dev), shift=True)
     Batch().run([obs])
     y = obs.rec.double()
-    b = Batch()
+    tex, tez = parse_tile(args.tile)
+    b = Batch(tile=(tex, tez), graph_chunk=args.graph_chunk, kernel=args.kernel)
     stream = torch.cuda.Stream()
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     ms = []
@@ -205,7 +211,8 @@ def run_plain(args):
     out = {"workload": "plain: 40x20 el, N=4, 13041 nodes, 2000 steps, 50 receivers, fwd+adj",
            "gpu_ms_per_solve": float(ms.mean()), "gpu_solves_per_s": 1e3 / float(ms.mean()),
            "p50_ms": float(np.percentile(ms, 50)), "p99_ms": float(np.percentile(ms, 99)),
-           "kernel": b.last_kernel, "groups": b.last_groups, "status": int(s.status.item())}
+           "kernel": b.last_kernel, "shape": b.last_shape, "graph_chunk": args.graph_chunk,
+           "groups": b.last_groups, "status": int(s.status.item())}
     if not args.no_cpu:
         threads = os.cpu_count() or 1
         kw_o = {k: kw[k] for k in kw if k not in ("coords", "node_grid")}
@@ -496,7 +503,7 @@ def main():
     ap.add_argument("--models", type=int, default=256)
     ap.add_argument("--nt", type=int, default=3000)
     ap.add_argument("--plain", type=int, default=6, help="one-at-a-time solves timed")
-    ap.add_argument("--tile", default="8x8")
+    ap.add_argument("--tile", default="auto", help="tile kernel shape EXxEZ, or auto")
     ap.add_argument("--graph-chunk", type=int, default=0)
     ap.add_argument("--kernel", type=int, default=0, help="0 auto, 1 tile, 2 strip")
     ap.add_argument("--ckpt-k", type=int, default=0)
@@ -539,7 +546,7 @@ def main():
     W = workload(nmodels=args.models, nt=args.nt, seed0=1000 * rank)
     plan = SEMPlan(**W["plan_kw"])
     dev = torch.device("cuda", local)
-    tex, tez = (int(x) for x in args.tile.split("x"))
+    tex, tez = parse_tile(args.tile)
     batch = Batch(tile=(tex, tez), graph_chunk=args.graph_chunk, kernel=args.kernel)
     stream = torch.cuda.Stream()
 
@@ -570,6 +577,7 @@ def main():
     launches_per_step = batch.last_launches
     kernel_used = batch.last_kernel
     groups_used = batch.last_groups
+    shape_used = batch.last_shape
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     step_ms, tick_ms = [], []
     clocks = Clocks(os.path.join(HERE, "gpurun_out", f"clocks_r{rank}.csv") if os.path.isdir(
@@ -641,6 +649,7 @@ def main():
             if i >= args.warmup:
                 plain_ms.append(ev0.elapsed_time(ev1))
     plain_kernel = pbatch.last_kernel
+    plain_shape = pbatch.last_shape
     plain_ms = np.array(plain_ms)
     plain_value = 1e3 / plain_ms.mean()
 
@@ -676,11 +685,12 @@ def main():
             "config": {"workload": "batched ELBO sampling (256 models, 100x50 el, N=4, 80601 nodes, "
                                    "3000 steps, 100 receivers)",
                        "models_per_gpu": n, "nodes": W["npoints"], "nt": W["nt"],
-                       "kernel": kernel_used, "tile": args.tile, "graph_chunk": args.graph_chunk,
+                       "kernel": kernel_used, "shape (tile_ex, tile_ez, strip_bands)": shape_used,
+                       "graph_chunk": args.graph_chunk,
                        "ckpt_k": args.ckpt_k or "auto", "groups": groups_used,
                        "l2": "inputs larger than L2 (state+c2 of 256 models ~250 MB per field set)",
                        "parallelism": f"replicas x{world}"},
-            "plain": {"value": plain_value, "unit": "solves/s", "kernel": plain_kernel,
+            "plain": {"value": plain_value, "unit": "solves/s", "kernel": plain_kernel, "shape": plain_shape,
                       "p50_ms": float(np.percentile(plain_ms, 50)),
                       "p99_ms": float(np.percentile(plain_ms, 99)), "solves": int(len(plain_ms))},
             "batched_over_plain": value / world / plain_value,

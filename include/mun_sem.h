@@ -92,7 +92,9 @@ typedef struct {
 
 /* Launch configuration (the autotuner's knobs). */
 typedef struct {
-  int32_t tile_ex, tile_ez;   /* tile kernel: elements per CTA tile in x and z        */
+  int32_t tile_ex, tile_ez;   /* tile kernel: elements per CTA tile in x and z; 0 x 0 =
+                                 automatic (largest of 8x8 .. 2x1 whose tiles over the
+                                 batch give every SM two CTAs, else 2x1)            */
   int32_t threads;            /* tile kernel: threads per CTA (multiple of 32, <= 256) */
   int32_t graph_chunk;        /* ticks per captured CUDA graph; 0 = plain launches    */
   int32_t kernel;             /* 0 auto, 1 tile kernel (one CTA per element tile),
@@ -128,6 +130,10 @@ int64_t sem_batch_last_launches(const sem_batch_t* batch);
 /* number of consecutive groups the last sem_run ran (1 unless ckpt_k = 0 solves were
  * split under the memory budget) */
 int32_t sem_batch_last_groups(const sem_batch_t* batch);
+/* launch shape the last sem_run used: tile kernel tile (elements) and strip kernel
+ * element rows per CTA (0 when the tile kernel ran); any pointer may be NULL */
+int sem_batch_last_shape(const sem_batch_t* batch, int32_t* tile_ex, int32_t* tile_ez,
+                         int32_t* strip_bands);
 /* tick rounds the last sem_run launched, summed over its groups (each round launches the
  * tick kernel once per polynomial order, then the tick counter kernel) */
 int64_t sem_batch_last_ticks(const sem_batch_t* batch);

@@ -53,7 +53,8 @@ class EngineCfg(C.Structure):
 
 EXPORTS = ["sem_plan_create", "sem_plan_destroy", "sem_plan_workspace_bytes", "sem_batch_create",
            "sem_batch_destroy", "sem_run", "sem_batch_last_launches", "sem_batch_last_kernel",
-           "sem_batch_last_groups", "sem_batch_last_ticks", "sem_batch_last_tick_ms", "sem_forward",
+           "sem_batch_last_groups", "sem_batch_last_shape", "sem_batch_last_ticks",
+           "sem_batch_last_tick_ms", "sem_forward",
            "sem_forward_adjoint", "sem_forward_noalloc", "sem_engine_create", "sem_engine_destroy",
            "sem_engine_submit", "sem_engine_step", "sem_engine_status", "sem_engine_release",
            "sem_engine_stats", "sem_velocity_from_curve", "sem_velocity_last_error", "sem_last_error"]
@@ -91,6 +92,7 @@ def load(path=None):
     lib.sem_batch_last_kernel.restype = i32
     lib.sem_batch_last_groups.argtypes = [vp]
     lib.sem_batch_last_groups.restype = i32
+    lib.sem_batch_last_shape.argtypes = [vp, vp, vp, vp]
     lib.sem_batch_last_ticks.argtypes = [vp]
     lib.sem_batch_last_ticks.restype = i64
     lib.sem_batch_last_tick_ms.argtypes = [vp, C.POINTER(C.c_double)]

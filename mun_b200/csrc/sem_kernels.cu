@@ -1338,6 +1338,25 @@ int strip_zchunk(long long total_strips, int nelz_max, int sms, int forced) {
 }
 // automatic variant choice: strips when the chunked strip grid gives every SM two CTAs
 bool strip_fills(long long min_chunk_ctas, int sms) { return min_chunk_ctas >= 2LL * sms; }
+// automatic tile shape of the tile kernel: the largest tile (in elements) whose tiles over
+// the batch give every SM two CTAs, else the smallest shape (small single solves are
+// latency-bound: more, smaller CTAs finish a tick sooner)
+void auto_tile(const sem_solve_t* sv, int n, int sms, int* tex, int* tez) {
+  static const int cand[][2] = {{8, 8}, {8, 4}, {4, 4}, {4, 2}, {2, 4}, {2, 2}, {2, 1}};
+  const int nc = (int)(sizeof(cand) / sizeof(cand[0]));
+  for (int c = 0; c < nc; ++c) {
+    long long tiles = 0;
+    for (int i = 0; i < n; ++i) {
+      int tx, tz;
+      tiles += tiles_of(sv[i].plan, cand[c][0], cand[c][1], &tx, &tz);
+    }
+    if (tiles >= 2LL * sms || c == nc - 1) {
+      *tex = cand[c][0];
+      *tez = cand[c][1];
+      return;
+    }
+  }
+}
 
 int upload_lists(const sem_plan_s* p, std::pair<int, int> key, std::vector<std::vector<int>>& rec,
                  std::vector<std::vector<int>>& inj, sem_plan_s::Lists* out) {
@@ -1482,6 +1501,7 @@ struct sem_batch_s {
   long long last_launches = 0;
   int last_kernel = 0;
   int last_zchunk = 0;
+  int last_tile_ex = 0, last_tile_ez = 0;
   int last_groups = 0;
   long long last_ticks = 0;             // tick rounds of the last sem_run (all groups)
   std::vector<cudaEvent_t> tick_ev;     // per group: before / after its tick loop
@@ -2020,7 +2040,8 @@ int sem_run(sem_batch_t* b, const sem_solve_t* solves, int32_t n, const sem_laun
   if (!b || (!solves && n) || n < 0) return fail(SEM_ERR_ARG, "null argument");
   cudaStream_t stream = (cudaStream_t)stream_v;
   sem_launch_cfg_t cfg = cfg_in ? *cfg_in : sem_launch_cfg_t{8, 8, 256, 0, 0, 0, 0};
-  if (cfg.tile_ex < 1 || cfg.tile_ez < 1) return fail(SEM_ERR_ARG, "tile size must be >= 1");
+  if (!(cfg.tile_ex == 0 && cfg.tile_ez == 0) && (cfg.tile_ex < 1 || cfg.tile_ez < 1))
+    return fail(SEM_ERR_ARG, "tile size must be >= 1 (or 0 x 0: automatic)");
   if (cfg.kernel < 0 || cfg.kernel > 2) return fail(SEM_ERR_ARG, "kernel must be 0 (auto), 1 (tile), 2 (strip)");
   if (cfg.threads < 32 || cfg.threads > 256 || cfg.threads % 32) cfg.threads = 256;
   if (cfg.memory_budget < 0) return fail(SEM_ERR_ARG, "memory_budget must be >= 0");
@@ -2035,6 +2056,14 @@ int sem_run(sem_batch_t* b, const sem_solve_t* solves, int32_t n, const sem_laun
     if (!solves[i].plan) return fail(SEM_ERR_ARG, "solve missing plan/velocity/rec_out");
     any_auto |= (solves[i].flags & SEM_F_ADJOINT) && solves[i].ckpt_k <= 0;
   }
+  if (cfg.tile_ex == 0) {
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    auto_tile(solves, n, sms, &cfg.tile_ex, &cfg.tile_ez);
+  }
+  b->last_tile_ex = cfg.tile_ex;
+  b->last_tile_ez = cfg.tile_ez;
   if (!any_auto) {
     b->last_groups = 1;
     return run_group(b, solves, n, cfg, stream);
@@ -2061,6 +2090,14 @@ int sem_run(sem_batch_t* b, const sem_solve_t* solves, int32_t n, const sem_laun
 }
 
 int32_t sem_batch_last_groups(const sem_batch_t* b) { return b ? b->last_groups : -1; }
+
+int sem_batch_last_shape(const sem_batch_t* b, int32_t* tile_ex, int32_t* tile_ez, int32_t* strip_bands) {
+  if (!b) return fail(SEM_ERR_ARG, "null argument");
+  if (tile_ex) *tile_ex = b->last_tile_ex;
+  if (tile_ez) *tile_ez = b->last_tile_ez;
+  if (strip_bands) *strip_bands = b->last_zchunk;
+  return SEM_OK;
+}
 
 int64_t sem_batch_last_ticks(const sem_batch_t* b) { return b ? b->last_ticks : -1; }
 

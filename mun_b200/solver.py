@@ -70,7 +70,7 @@ def choose_ckpt_k(plan, n_solves, budget_bytes=None):
 class Batch:
     """Owns a ``sem_batch_t`` (workspace arena, descriptors, tick counter)."""
 
-    def __init__(self, tile=(8, 8), threads=256, graph_chunk=0, kernel=0, strip_bands=0):
+    def __init__(self, tile=(0, 0), threads=256, graph_chunk=0, kernel=0, strip_bands=0):
         lib = _lib.load()
         h = C.c_void_p()
         _lib.check(lib.sem_batch_create(C.byref(h)))
@@ -99,6 +99,13 @@ class Batch:
         """Consecutive groups the last run used (automatic checkpointing may split a
         batch so that each group's forward history fits the memory budget)."""
         return int(self._lib.sem_batch_last_groups(self.handle))
+
+    @property
+    def last_shape(self):
+        """(tile_ex, tile_ez, strip_bands) of the last run (strip_bands 0: tile kernel)."""
+        v = [C.c_int32() for _ in range(3)]
+        _lib.check(self._lib.sem_batch_last_shape(self.handle, *[C.byref(x) for x in v]))
+        return tuple(int(x.value) for x in v)
 
     @property
     def last_ticks(self):
