@@ -408,7 +408,7 @@ def run_serving(args):
                                     "flow"))
             k_flow += 1
     eng = Engine(max_solves=args.serve_slots, memory_cap_bytes=int(args.serve_cap_gb * (1 << 30)),
-                 ticks_per_step=args.serve_ticks, kernel=1)
+                 ticks_per_step=args.serve_ticks, kernel=args.kernel)
     done, lat, wall = serve(eng, reqs)
     # serialized reference: the same requests one at a time, back to back
     b = Batch()

@@ -190,8 +190,9 @@ typedef struct {
   int32_t max_solves;      /* concurrent solves                                        */
   int64_t memory_cap;      /* device bytes for solve workspaces (allocated at creation) */
   int32_t ticks_per_step;  /* ticks launched by one sem_engine_step                    */
-  int32_t kernel;          /* 1 tile kernel, 2 strip kernel (fixed for the engine)     */
-  int32_t tile_ex, tile_ez;/* tile kernel tile size                                    */
+  int32_t kernel;          /* 0 automatic per step (as in sem_run), 1 tile kernel,
+                              2 strip kernel                                           */
+  int32_t tile_ex, tile_ez;/* tile kernel tile size; 0 x 0 = automatic per step        */
 } sem_engine_cfg_t;
 
 int sem_engine_create(const sem_engine_cfg_t* cfg, sem_engine_t** out);

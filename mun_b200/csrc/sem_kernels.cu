@@ -1147,26 +1147,6 @@ __global__ void set_c2_kernel(const double* __restrict__ c, const int* __restric
   }
 }
 
-// grad_out[i] = 2 c_i * acc[pos_i] * scale     (dJ/dc = 2c dJ/dc^2, core.py:84)
-__global__ void grad_out_kernel(const double* __restrict__ c, const int* __restrict__ pos,
-                                const double* __restrict__ acc, double inv_sigma2,
-                                const double* __restrict__ adj_scale, double* __restrict__ out,
-                                int n) {
-  const double scale = inv_sigma2 / *adj_scale;  // exact: adj_scale is a power of two
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
-    out[i] = 2.0 * c[i] * acc[pos[i]] * scale;
-}
-
-// loglik = -0.5 inv_sigma2 sum_r misfit_r   (fixed order: deterministic)
-__global__ void loglik_kernel(const double* __restrict__ misfit, int nrec, double inv_sigma2,
-                              double* __restrict__ out) {
-  if (threadIdx.x == 0 && blockIdx.x == 0) {
-    double s = 0.0;
-    for (int r = 0; r < nrec; ++r) s += misfit[r];
-    *out = -0.5 * s * inv_sigma2;
-  }
-}
-
 __global__ void copy_status_kernel(const int* __restrict__ st, int* __restrict__ out) {
   if (threadIdx.x == 0 && blockIdx.x == 0) *out = *st;
 }
@@ -1207,8 +1187,10 @@ __global__ void batch_setup_kernel(const SolveIo* __restrict__ io, int s0) {
   }
 }
 
-// gradient in reference node order, log-likelihood and status of every solve
-// (same arithmetic as grad_out_kernel / loglik_kernel / copy_status_kernel)
+// gradient in reference node order, log-likelihood and status of every solve:
+//   grad_out[i] = 2 c_i * acc[pos_i] * inv_sigma2 / adj_scale   (dJ/dc = 2c dJ/dc^2,
+//     core.py:84; adj_scale is a power of two, so the division is exact)
+//   loglik = -0.5 inv_sigma2 sum_r misfit_r   (fixed receiver order: deterministic)
 __global__ void batch_output_kernel(const SolveIo* __restrict__ io, int s0) {
   const SolveIo& s = io[s0 + blockIdx.y];
   if (s.grad_out) {
@@ -2256,9 +2238,40 @@ struct sem_engine_s {
   long long launches = 0;
   std::vector<SolveDev> h_solves;
   std::vector<int> h_cta;
+  SolveIo* d_io = nullptr;  // [2 * max_solves]: outputs of retiring solves | set-up of admitted
+  std::vector<SolveIo> h_io;
 };
 
 namespace {
+
+// set-up / output table entry of one solve whose workspace starts at `a`
+SolveIo solve_io(const sem_solve_t& s, const Workspace& ws, char* a) {
+  const sem_plan_s* p = s.plan;
+  const long long F = p->fstride * 4;
+  SolveIo io{};
+  io.vel = s.velocity; io.pos = p->node_pos; io.c2 = (float*)(a + ws.c2);
+  io.npoints = p->npoints;
+  auto zero = [&](long long o, long long bytes) { io.zp[io.nzero] = a + o; io.zb[io.nzero++] = bytes; };
+  zero(ws.W, F);
+  zero(ws.V, F);
+  if (s.flags & SEM_F_ADJOINT) {
+    zero(ws.ckpt, 2 * F);
+    zero(ws.ring, F);
+    zero(ws.L, 3 * F);  // L[0], L[1], Mu
+    zero(ws.grad, 2 * F);
+  }
+  zero(ws.misfit, ws.status - ws.misfit + 256);
+  io.grad_out = ((s.flags & SEM_F_ADJOINT) && s.grad_out) ? s.grad_out : nullptr;
+  io.gacc = (const double*)(a + ws.grad);
+  io.adj_scale = (const double*)(a + ws.misfit) + 2 * p->nrec;
+  io.inv_sigma2 = s.inv_sigma2;
+  io.misfit = (const double*)(a + ws.misfit);
+  io.nrec = p->nrec;
+  io.loglik_out = ((s.flags & SEM_F_MISFIT) && s.loglik_out) ? s.loglik_out : nullptr;
+  io.st = (const int*)(a + ws.status);
+  io.status_out = s.status_out;
+  return io;
+}
 
 long long arena_alloc(sem_engine_s* e, long long bytes) {
   bytes = round_up(bytes, 256);
@@ -2299,7 +2312,8 @@ extern "C" {
 int sem_engine_create(const sem_engine_cfg_t* cfg, sem_engine_t** out) {
   if (!cfg || !out) return fail(SEM_ERR_ARG, "null argument");
   if (cfg->max_solves < 1 || cfg->memory_cap < (1 << 20) || cfg->ticks_per_step < 1 ||
-      cfg->kernel < 1 || cfg->kernel > 2 || cfg->tile_ex < 1 || cfg->tile_ez < 1)
+      cfg->kernel < 0 || cfg->kernel > 2 ||
+      (!(cfg->tile_ex == 0 && cfg->tile_ez == 0) && (cfg->tile_ex < 1 || cfg->tile_ez < 1)))
     return fail(SEM_ERR_ARG, "bad engine configuration");
   auto* e = new sem_engine_s();
   e->cfg = *cfg;
@@ -2329,6 +2343,7 @@ int sem_engine_destroy(sem_engine_t* e) {
     delete kv.second;
   }
   cudaFree(e->arena); cudaFree(e->d_tick); cudaFree(e->d_solves); cudaFree(e->d_cta);
+  cudaFree(e->d_io);
   delete e;
   return SEM_OK;
 }
@@ -2400,35 +2415,25 @@ int sem_engine_stats(const sem_engine_t* e, int64_t* out) {
 int sem_engine_step(sem_engine_t* e, void* stream_v) {
   if (!e) return fail(SEM_ERR_ARG, "null argument");
   cudaStream_t stream = (cudaStream_t)stream_v;
-  const bool use_strip = (e->cfg.kernel == 2);
-  // ---- retire solves whose program has ended: outputs, then free the workspace
+  if (!e->d_io) {
+    CUDA_TRY(cudaMalloc((void**)&e->d_io, sizeof(SolveIo) * 2 * (size_t)e->cfg.max_solves));
+  }
+  e->h_io.clear();
+  // ---- retire solves whose program has ended: outputs (one launch), then free the workspace
+  std::vector<EngineJob*> retiring;
   for (size_t i = 0; i < e->running.size();) {
     EngineJob* j = e->running[i];
     if (e->tick < j->start + j->prog) { ++i; continue; }
-    const sem_plan_s* p = j->s.plan;
-    char* a = e->arena + j->off;
-    if ((j->s.flags & SEM_F_ADJOINT) && j->s.grad_out) {
-      grad_out_kernel<<<std::min(1024, (p->npoints + 255) / 256), 256, 0, stream>>>(
-          j->s.velocity, p->node_pos, (const double*)(a + j->ws.grad), j->s.inv_sigma2,
-          (const double*)(a + j->ws.misfit) + 2 * p->nrec, j->s.grad_out, p->npoints);
-      e->launches++;
-    }
-    if ((j->s.flags & SEM_F_MISFIT) && j->s.loglik_out) {
-      loglik_kernel<<<1, 32, 0, stream>>>((const double*)(a + j->ws.misfit), p->nrec, j->s.inv_sigma2,
-                                          j->s.loglik_out);
-      e->launches++;
-    }
-    if (j->s.status_out) {
-      copy_status_kernel<<<1, 32, 0, stream>>>((const int*)(a + j->ws.status), j->s.status_out);
-      e->launches++;
-    }
-    CUDA_TRY(cudaEventCreateWithFlags(&j->ev, cudaEventDisableTiming));
-    CUDA_TRY(cudaEventRecord(j->ev, stream));
-    arena_free(e, j->off, j->ws.bytes);
-    j->state = 2;
+    e->h_io.push_back(solve_io(j->s, j->ws, e->arena + j->off));
+    retiring.push_back(j);
     e->running.erase(e->running.begin() + i);
   }
-  // ---- admit queued solves in arrival order while a slot and memory are free
+  const int nret = (int)e->h_io.size();
+  // ---- admit queued solves in arrival order while a slot and memory are free (their
+  // workspaces may reuse the retiring solves' memory: the set-up launch follows the
+  // output launch on the stream)
+  for (EngineJob* j : retiring) arena_free(e, j->off, j->ws.bytes);
+  std::vector<EngineJob*> admitted;
   while (!e->queue.empty() && (int)e->running.size() < e->cfg.max_solves) {
     EngineJob* j = e->queue.front();
     const long long off = arena_alloc(e, j->ws.bytes);
@@ -2437,24 +2442,53 @@ int sem_engine_step(sem_engine_t* e, void* stream_v) {
     j->off = off;
     j->start = e->tick;
     j->state = 1;
-    const sem_plan_s* p = j->s.plan;
-    char* a = e->arena + off;
-    const long long F = p->fstride * 4;
-    CUDA_TRY(cudaMemsetAsync(a + j->ws.W, 0, F, stream));
-    CUDA_TRY(cudaMemsetAsync(a + j->ws.V, 0, F, stream));
-    if (j->s.flags & SEM_F_ADJOINT) {
-      CUDA_TRY(cudaMemsetAsync(a + j->ws.ckpt, 0, 2 * F, stream));
-      CUDA_TRY(cudaMemsetAsync(a + j->ws.ring, 0, F, stream));
-      CUDA_TRY(cudaMemsetAsync(a + j->ws.L, 0, 3 * F, stream));
-      CUDA_TRY(cudaMemsetAsync(a + j->ws.grad, 0, 2 * F, stream));
-    }
-    CUDA_TRY(cudaMemsetAsync(a + j->ws.misfit, 0, j->ws.status - j->ws.misfit + 256, stream));
-    set_c2_kernel<<<std::min(1024, (p->npoints + 255) / 256), 256, 0, stream>>>(
-        j->s.velocity, p->node_pos, (float*)(a + j->ws.c2), p->npoints);
-    e->launches++;
+    e->h_io.push_back(solve_io(j->s, j->ws, e->arena + off));
+    admitted.push_back(j);
     e->running.push_back(j);
   }
+  const int nadm = (int)e->h_io.size() - nret;
+  if (!e->h_io.empty())
+    CUDA_TRY(cudaMemcpyAsync(e->d_io, e->h_io.data(), sizeof(SolveIo) * e->h_io.size(),
+                             cudaMemcpyHostToDevice, stream));
+  auto io_blocks = [&](int s0, int cnt) {
+    long long mx = 1;
+    for (int i = s0; i < s0 + cnt; ++i) mx = std::max(mx, (long long)e->h_io[i].npoints);
+    return (unsigned)std::min<long long>(64, (mx + 2047) / 2048);
+  };
+  if (nret > 0) {
+    batch_output_kernel<<<dim3(io_blocks(0, nret), (unsigned)nret), 256, 0, stream>>>(e->d_io, 0);
+    e->launches++;
+    for (EngineJob* j : retiring) {
+      CUDA_TRY(cudaEventCreateWithFlags(&j->ev, cudaEventDisableTiming));
+      CUDA_TRY(cudaEventRecord(j->ev, stream));
+      j->state = 2;
+    }
+  }
+  if (nadm > 0) {
+    batch_setup_kernel<<<dim3(io_blocks(nret, nadm), (unsigned)nadm), 256, 0, stream>>>(e->d_io, nret);
+    e->launches++;
+  }
   if (e->running.empty()) return SEM_OK;
+  // ---- kernel and launch shape for the running set (as in sem_run: automatic variant,
+  // strip chunks and tile shape unless the configuration fixes them)
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  std::vector<sem_solve_t> run_sv;
+  long long total_strips = 0, min_chunk_ctas = 0;
+  int nelz_max = 1;
+  for (EngineJob* j : e->running) {
+    run_sv.push_back(j->s);
+    const sem_plan_s* p = j->s.plan;
+    const int ns = strips_of(p, nullptr);
+    total_strips += ns;
+    min_chunk_ctas += (long long)ns * ((p->nelz + kMinChunk - 1) / kMinChunk);
+    nelz_max = std::max(nelz_max, p->nelz);
+  }
+  const bool use_strip = e->cfg.kernel == 2 || (e->cfg.kernel == 0 && strip_fills(min_chunk_ctas, sms));
+  const int zchunk = use_strip ? strip_zchunk(total_strips, nelz_max, sms, 0) : 0;
+  int tex = e->cfg.tile_ex, tez = e->cfg.tile_ez;
+  if (!use_strip && tex == 0) auto_tile(run_sv.data(), (int)run_sv.size(), sms, &tex, &tez);
   // ---- descriptors and CTA maps of the running set, grouped by order
   std::vector<EngineJob*> order(e->running);
   std::stable_sort(order.begin(), order.end(),
@@ -2470,15 +2504,12 @@ int sem_engine_step(sem_engine_t* e, void* stream_v) {
     sem_plan_s::Lists L;
     int ntx, ntz, ntiles, rc;
     if (use_strip) {
-      const int ewm = strip_ew_max(p->npol);
-      ntx = (p->nelx + ewm - 1) / ewm;
-      ntz = (p->nelx + ntx - 1) / ntx;
-      ntx = (p->nelx + ntz - 1) / ntz;
-      ntiles = ntx;
+      ntx = strips_of(p, &ntz);
+      ntiles = ntx * ((p->nelz + zchunk - 1) / zchunk);
       rc = get_strip_lists(p, ntz, &L);
     } else {
-      ntiles = tiles_of(p, e->cfg.tile_ex, e->cfg.tile_ez, &ntx, &ntz);
-      rc = get_lists(p, e->cfg.tile_ex, e->cfg.tile_ez, &L);
+      ntiles = tiles_of(p, tex, tez, &ntx, &ntz);
+      rc = get_lists(p, tex, tez, &L);
     }
     if (rc) return rc;
     if (groups.empty() || groups.back().N != p->npol)
@@ -2489,7 +2520,7 @@ int sem_engine_step(sem_engine_t* e, void* stream_v) {
     SolveDev& d = e->h_solves[oi];
     d.nelx = p->nelx; d.nelz = p->nelz; d.nxg = p->nxg; d.nzg = p->nzg; d.pitch = p->pitch;
     d.tiles_x = ntx; d.tiles_z = ntz;
-    d.zchunk = p->nelz;  // full-height strips
+    d.zchunk = use_strip ? zchunk : p->nelz;
     d.tile_base = (int)(e->h_cta.size() - G.cta0);
     d.nt = p->nt; d.k = j->k; d.nseg = j->nseg; d.flags = j->s.flags;
     d.start_tick = (int)j->start;
@@ -2534,22 +2565,32 @@ int sem_engine_step(sem_engine_t* e, void* stream_v) {
                            cudaMemcpyHostToDevice, stream));
   CUDA_TRY(cudaMemcpyAsync(e->d_cta, e->h_cta.data(), sizeof(int) * e->h_cta.size(),
                            cudaMemcpyHostToDevice, stream));
-  // ---- ticks
+  // ---- ticks: the tick number is passed; launches chain by programmatic dependent launch
   for (int c = 0; c < e->cfg.ticks_per_step; ++c) {
     for (auto& G : groups) {
       KernelFn fn = use_strip ? strip_kernel_for(G.N) : kernel_for(G.N);
       if (!fn) return fail(SEM_ERR_UNSUPPORTED, "polynomial order");
       const size_t smem = (size_t)(use_strip ? strip_smem_floats(G.N, G.adj)
-                                             : smem_floats(G.N, e->cfg.tile_ex, e->cfg.tile_ez, G.adj)) *
-                          sizeof(float);
+                                             : smem_floats(G.N, tex, tez, G.adj)) * sizeof(float);
+      if (smem > 227 * 1024) return fail(SEM_ERR_ARG, "tile too large for shared memory");
       if (c == 0)
         CUDA_TRY(cudaFuncSetAttribute((const void*)fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-      fn<<<(unsigned)G.ncta, use_strip ? strip_threads(G.N) : 256, smem, stream>>>(
-          e->d_solves + G.first, e->d_cta + G.cta0, e->d_tick, e->cfg.tile_ex, e->cfg.tile_ez, 0);
+      cudaLaunchConfig_t lc = {};
+      lc.gridDim = dim3((unsigned)G.ncta);
+      lc.blockDim = dim3(use_strip ? strip_threads(G.N) : 256);
+      lc.dynamicSmemBytes = smem;
+      lc.stream = stream;
+      cudaLaunchAttribute at[1];
+      at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+      at[0].val.programmaticStreamSerializationAllowed = SEM_PDL ? 1 : 0;
+      lc.attrs = at;
+      lc.numAttrs = 1;
+      const int* no_counter = nullptr;
+      CUDA_TRY(cudaLaunchKernelEx(&lc, fn, (const SolveDev*)(e->d_solves + G.first),
+                                  (const int*)(e->d_cta + G.cta0), no_counter, tex, tez,
+                                  (int)(e->tick + c)));
       e->launches++;
     }
-    tick_advance_kernel<<<1, 1, 0, stream>>>(e->d_tick);
-    e->launches++;
   }
   e->tick += e->cfg.ticks_per_step;
   CUDA_TRY(cudaGetLastError());

@@ -25,8 +25,9 @@ from .solver import SolveSpec
 class Engine:
     """Owns a ``sem_engine_t``."""
 
-    def __init__(self, max_solves=512, memory_cap_bytes=8 << 30, ticks_per_step=16, kernel=1,
-                 tile=(8, 8), stream=None):
+    def __init__(self, max_solves=512, memory_cap_bytes=8 << 30, ticks_per_step=16, kernel=0,
+                 tile=(0, 0), stream=None):
+        """kernel 0 / tile (0, 0): chosen per step for the running set (as in sem_run)."""
         lib = _lib.load()
         cfg = _lib.EngineCfg(int(max_solves), int(memory_cap_bytes), int(ticks_per_step), int(kernel),
                              int(tile[0]), int(tile[1]))

@@ -28,7 +28,7 @@ def _specs():
     return out
 
 
-@pytest.mark.parametrize("kernel", [1, 2])
+@pytest.mark.parametrize("kernel", [0, 1, 2])
 def test_engine_mix_is_bitwise_equal_to_alone(kernel):
     makers = _specs()
     alone = []
