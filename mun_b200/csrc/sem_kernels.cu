@@ -564,6 +564,9 @@ __global__ void __launch_bounds__(256) sem_tick_kernel(const SolveDev* __restric
 #ifndef SEM_PDL
 #define SEM_PDL 1
 #endif
+#ifndef SEM_PAIRED
+#define SEM_PAIRED 1
+#endif
 #ifndef SEM_GRAD_STAGE
 #define SEM_GRAD_STAGE 0
 #endif
@@ -589,6 +592,9 @@ constexpr int kStripHdr = 192;
 // registers free for the band's work.
 __constant__ float c_D[kMaxN + 1][64];
 __constant__ float c_B[kMaxN + 1][8];
+// the same values duplicated into both halves of a float2, for packed FFMA2 / FMUL2
+__constant__ float2 c_D2[kMaxN + 1][64];
+__constant__ float2 c_B2[kMaxN + 1][8];
 
 __host__ __device__ inline int strip_ew_max(int N) { return (kStripCols - N - 1) / N; }
 __host__ __device__ inline int strip_bw(int N) { return (kStripCols + 3 + 3) & ~3; }  // smem row
@@ -682,6 +688,22 @@ __device__ __forceinline__ void load_seg(const float* p, float (&u)[N + 1], unsi
   } else {
 #pragma unroll
     for (int b = 0; b <= N; ++b) u[b] = p[b];
+  }
+}
+
+// Paired phase A: every lane loads its x-line segment (zeros when it has no item) so
+// that the whole warp takes part in the edge-node shuffle.
+template <int N>
+__device__ __forceinline__ void load_seg_all(const float* p, bool valid, bool from_next,
+                                             float (&u)[N + 1]) {
+  if constexpr (N == 4) {
+    const float4 q = valid ? *reinterpret_cast<const float4*>(p) : make_float4(0.f, 0.f, 0.f, 0.f);
+    u[0] = q.x; u[1] = q.y; u[2] = q.z; u[3] = q.w;
+    const float nx = __shfl_down_sync(0xffffffffu, q.x, 1);
+    u[4] = from_next ? nx : (valid ? p[4] : 0.f);
+  } else {
+#pragma unroll
+    for (int b = 0; b <= N; ++b) u[b] = valid ? p[b] : 0.f;
   }
 }
 
@@ -970,40 +992,78 @@ __device__ __forceinline__ void strip_tick(const SolveDev& S, const int act, con
         }
       }
     };
-    if (!halo) {
-      if (xitem) xline(xa, xsg, mA, nextA);
-      if (last && xitem_last) xline(N, tid, mL, nextL);
-    }
-    // ---- phase A, z-lines: one thread per owned column (the band is the segment)
     float rz[NP], sz[NP];
-    if (owned) {
-      float u[NP], du[NP], q[NP];
+    // ---- phase A of forward-like ticks, paired: this thread's x-line segment (lane .x of
+    // every float2) and its column's z-line segment (lane .y) share D and beta, so each
+    // packed FFMA2 / FMUL2 does one step of both; per half it is the scalar fmaf / multiply
+    // sequence.  Adjoint ticks (two more contractions, more live values) stay scalar.
+    if (SEM_PAIRED && !ADJ) {
+      const bool xi = !halo && xitem;
+      const int o = xi ? xa * BW + off + xsg * N : 0;
+      float2 u2[NP], c2v[NP], du2[NP], q2[NP];
+      {
+        float ux[NP], cx[NP];
+        load_seg_all<N>(Bs + o, xi, nextA, ux);
+        load_seg_all<N>(Cs + o, xi, nextA, cx);
 #pragma unroll
-      for (int b = 0; b < NP; ++b) u[b] = Bs[b * BW + sc];
+        for (int b = 0; b < NP; ++b) {
+          u2[b] = make_float2(ux[b], Bs[b * BW + sc]);
+          c2v[b] = make_float2(cx[b], Cs[b * BW + sc]);
+        }
+      }
 #pragma unroll
       for (int a2 = 0; a2 < NP; ++a2) {
-        float v = 0.f;
+        float2 v = make_float2(0.f, 0.f);
 #pragma unroll
-        for (int b = 0; b < NP; ++b) v = fmaf(Dr(a2, b), u[b], v);
-        du[a2] = v;
-        q[a2] = Bt(a2) * Cs[a2 * BW + sc] * v;
+        for (int b = 0; b < NP; ++b) v = __ffma2_rn(c_D2[N][a2 * NP + b], u2[b], v);
+        du2[a2] = v;
+        q2[a2] = __fmul2_rn(__fmul2_rn(c_B2[N][a2], c2v[a2]), v);
       }
+      float* xo = Xs + (xa * SEGS + xsg) * NP;
 #pragma unroll
-      for (int j = 0; j < NP; ++j) {
-        float v = 0.f;
+      for (int i = 0; i < NP; ++i) {
+        float2 v = make_float2(0.f, 0.f);
 #pragma unroll
-        for (int a2 = 0; a2 < NP; ++a2) v = fmaf(Dr(a2, j), q[a2], v);
-        rz[j] = v;
+        for (int a2 = 0; a2 < NP; ++a2) v = __ffma2_rn(c_D2[N][a2 * NP + i], q2[a2], v);
+        if (xi) xo[i] = v.x;
+        rz[i] = v.y;
       }
-      if (ADJ) {
+      if (!halo && last && xitem_last) xline(N, tid, mL, nextL);
+    } else {
+      if (!halo) {
+        if (xitem) xline(xa, xsg, mA, nextA);
+        if (last && xitem_last) xline(N, tid, mL, nextL);
+      }
+      // ---- phase A, z-lines: one thread per owned column (the band is the segment)
+      if (owned) {
+        float u[NP], du[NP], q[NP];
 #pragma unroll
-        for (int b = 0; b < NP; ++b) u[b] = Us[b * BW + sc];
+        for (int b = 0; b < NP; ++b) u[b] = Bs[b * BW + sc];
 #pragma unroll
         for (int a2 = 0; a2 < NP; ++a2) {
           float v = 0.f;
 #pragma unroll
           for (int b = 0; b < NP; ++b) v = fmaf(Dr(a2, b), u[b], v);
-          sz[a2] = Bt(a2) * v * du[a2];
+          du[a2] = v;
+          q[a2] = Bt(a2) * Cs[a2 * BW + sc] * v;
+        }
+#pragma unroll
+        for (int j = 0; j < NP; ++j) {
+          float v = 0.f;
+#pragma unroll
+          for (int a2 = 0; a2 < NP; ++a2) v = fmaf(Dr(a2, j), q[a2], v);
+          rz[j] = v;
+        }
+        if (ADJ) {
+#pragma unroll
+          for (int b = 0; b < NP; ++b) u[b] = Us[b * BW + sc];
+#pragma unroll
+          for (int a2 = 0; a2 < NP; ++a2) {
+            float v = 0.f;
+#pragma unroll
+            for (int b = 0; b < NP; ++b) v = fmaf(Dr(a2, b), u[b], v);
+            sz[a2] = Bt(a2) * v * du[a2];
+          }
         }
       }
     }
@@ -1282,6 +1342,10 @@ int set_order_constants(int dev, int N, const double* D, const double* beta) {
   }
   CUDA_TRY(cudaMemcpyToSymbol(c_D, v.data(), sizeof(float) * NP * NP, sizeof(float) * 64 * N));
   CUDA_TRY(cudaMemcpyToSymbol(c_B, v.data() + NP * NP, sizeof(float) * NP, sizeof(float) * 8 * N));
+  std::vector<float2> v2(v.size());
+  for (size_t i = 0; i < v.size(); ++i) v2[i] = make_float2(v[i], v[i]);
+  CUDA_TRY(cudaMemcpyToSymbol(c_D2, v2.data(), sizeof(float2) * NP * NP, sizeof(float2) * 64 * N));
+  CUDA_TRY(cudaMemcpyToSymbol(c_B2, v2.data() + NP * NP, sizeof(float2) * NP, sizeof(float2) * 8 * N));
   have[std::make_pair(dev, N)] = v;
   return SEM_OK;
 }
