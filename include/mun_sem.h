@@ -122,7 +122,8 @@ int64_t sem_plan_workspace_bytes(const sem_plan_t* plan, int32_t flags, int32_t 
 int sem_batch_create(sem_batch_t** out);
 int sem_batch_destroy(sem_batch_t* batch);
 /* Run n solves (any mix of plans/orders/nt) to completion on ``stream``.  Solves of
- * the same polynomial order share one kernel launch per time tick. */
+ * the same polynomial order share one kernel launch per time tick.  cfg may be NULL:
+ * every launch choice automatic (kernel, tile shape, strip chunks, memory budget). */
 int sem_run(sem_batch_t* batch, const sem_solve_t* solves, int32_t n,
             const sem_launch_cfg_t* cfg, void* stream);
 /* number of kernel launches issued by the last sem_run (for accounting) */

@@ -2085,7 +2085,8 @@ int sem_run(sem_batch_t* b, const sem_solve_t* solves, int32_t n, const sem_laun
             void* stream_v) {
   if (!b || (!solves && n) || n < 0) return fail(SEM_ERR_ARG, "null argument");
   cudaStream_t stream = (cudaStream_t)stream_v;
-  sem_launch_cfg_t cfg = cfg_in ? *cfg_in : sem_launch_cfg_t{8, 8, 256, 0, 0, 0, 0};
+  // no configuration: automatic kernel, tile shape, strip chunks and memory budget
+  sem_launch_cfg_t cfg = cfg_in ? *cfg_in : sem_launch_cfg_t{0, 0, 256, 0, 0, 0, 0};
   if (!(cfg.tile_ex == 0 && cfg.tile_ez == 0) && (cfg.tile_ex < 1 || cfg.tile_ez < 1))
     return fail(SEM_ERR_ARG, "tile size must be >= 1 (or 0 x 0: automatic)");
   if (cfg.kernel < 0 || cfg.kernel > 2) return fail(SEM_ERR_ARG, "kernel must be 0 (auto), 1 (tile), 2 (strip)");
