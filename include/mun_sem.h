@@ -240,6 +240,26 @@ int sem_velocity_from_curve(const sem_curve_t* curve, int32_t npoints, const dou
                             double* sd_out, double* ustar_out, double* normal_out, void* stream);
 const char* sem_velocity_last_error(void);
 
+/* Gradient of the log-likelihood w.r.t. the curve's K free control points for a batch
+ * of S samples on one mesh, from dL/dv at the nodes (MUN's
+ * _analytical_gradient_projection_improved, Bspline_Coupling/SEM/sem_waveform/core.py:902-970,
+ * CO2_plume/layered_model/inversion/sem_waveform/core.py:1047-1117,
+ * CO2_plume/one_stage/single_cubic/sem_waveform/core.py:1128-1202):
+ *   sum over nodes with |dv| above the reference's threshold of
+ *   dL/dv * (v_in - v_bg) sig (1 - sig) (-1/tau) * basis_j(u*) * outward normal.
+ * knots: HOST [ncoef + 4] of the closed cubic spline (ncoef = K + 3: the clamped closure
+ * repeats the first point 3 times, the periodic one the first 3 points; both fold back).
+ * periodic != 0 applies the gridded package's parameter mapping lo + mod(u, 1) (hi - lo).
+ * DEVICE inputs, row s = sample s: dL_dv, sd, ustar [S * npoints], normal [S * npoints * 2];
+ * v_background DEVICE [npoints] or NULL (then v_background_const).  floor_one: threshold
+ * 1e-8 * max(1, |v_in - v_bg|) (layered, gridded) instead of 1e-8 * |v_in - v_bg| (canonical).
+ * grad_out DEVICE [S * 2K]: per sample K x-components, then K z-components.  Deterministic. */
+int sem_project_from_curve(const double* knots, int32_t ncoef, int32_t K, int32_t periodic,
+                           int32_t nsamples, int32_t npoints, const double* dL_dv, const double* sd,
+                           const double* ustar, const double* normal, const double* v_background,
+                           double v_background_const, double v_inside, double tau, int32_t floor_one,
+                           double* grad_out, void* stream);
+
 /* last error message of the calling thread (static storage) */
 const char* sem_last_error(void);
 

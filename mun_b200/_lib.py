@@ -57,7 +57,8 @@ EXPORTS = ["sem_plan_create", "sem_plan_destroy", "sem_plan_workspace_bytes", "s
            "sem_batch_last_tick_ms", "sem_forward",
            "sem_forward_adjoint", "sem_forward_noalloc", "sem_engine_create", "sem_engine_destroy",
            "sem_engine_submit", "sem_engine_step", "sem_engine_status", "sem_engine_release",
-           "sem_engine_stats", "sem_velocity_from_curve", "sem_velocity_last_error", "sem_last_error"]
+           "sem_engine_stats", "sem_velocity_from_curve", "sem_project_from_curve",
+           "sem_velocity_last_error", "sem_last_error"]
 
 _lib = None
 
@@ -107,6 +108,8 @@ def load(path=None):
     lib.sem_engine_release.argtypes = [vp, i64]
     lib.sem_engine_stats.argtypes = [vp, C.POINTER(i64)]
     lib.sem_velocity_from_curve.argtypes = [C.POINTER(CurveDesc), i32, vp, vp, dbl, vp, vp, vp, vp, vp]
+    lib.sem_project_from_curve.argtypes = [vp, i32, i32, i32, i32, i32, vp, vp, vp, vp, vp, dbl, dbl,
+                                           dbl, i32, vp, vp]
     lib.sem_velocity_last_error.restype = C.c_char_p
     lib.sem_last_error.restype = C.c_char_p
     for name in EXPORTS:

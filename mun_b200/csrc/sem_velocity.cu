@@ -151,9 +151,114 @@ __global__ void velocity_kernel(CurveDev curve, const double* __restrict__ u0,
   }
 }
 
+// Control-point projection of dL/dv for a batch of samples (row s of every (S, P) input):
+//   dv_p = (v_in - bg_p) sig_p (1 - sig_p) (-1/tau),  sig_p = 1 / (1 + exp(clip(sd_p/tau, +-50)))
+//   mask: |dv_p| > 1e-8 * (floor_one ? max(1, |v_in - bg_p|) : |v_in - bg_p|)
+//   out[s][j]     = sum_p mask w_p B_j(u_p) n_p,x,   out[s][K + j] = ... n_p,z,  w_p = dL_p dv_p
+// B_j is the cubic basis at the closest-point parameter (periodic curves: the gridded
+// package's mapping t = lo + mod(u, 1) (hi - lo)), with the duplicated closing controls
+// folded back onto the points they copy.  One block per (sample, control point); each
+// thread sums a fixed node subset, then a fixed-order tree: deterministic.
+__global__ void project_kernel(CurveDev curve, int K, int periodic, int P, const double* __restrict__ dL,
+                               const double* __restrict__ sd, const double* __restrict__ us,
+                               const double* __restrict__ nrm, const double* __restrict__ bg,
+                               double bg_const, double v_in, double tau, int floor_one,
+                               double* __restrict__ out) {
+  const int j = blockIdx.x, smp = blockIdx.y;
+  const long long row = (long long)smp * P;
+  const double ts = fmax(tau, 1e-12);
+  double ax = 0.0, az = 0.0;
+  for (int p = threadIdx.x; p < P; p += blockDim.x) {
+    const double b = bg ? bg[p] : bg_const;
+    const double delta = v_in - b;
+    const double x = fmin(fmax(sd[row + p] / ts, -50.0), 50.0);
+    const double sig = 1.0 / (1.0 + exp(x));
+    const double dv = delta * sig * (1.0 - sig) * (-1.0 / ts);
+    const double lim = 1e-8 * (floor_one ? fmax(1.0, fabs(delta)) : fabs(delta));
+    if (!(fabs(dv) > lim)) continue;
+    double u = us[row + p];
+    if (periodic) {
+      const double fr = u - floor(u);  // mod(u, 1)
+      u = fmin(fmax(curve.lo + fr * (curve.hi - curve.lo), curve.lo), nextafter(curve.hi, curve.lo));
+    }
+    // span i: t[i] <= u < t[i+1], clamped to the last valid span
+    int i = 3;
+    for (int q = 3; q < curve.ncoef; ++q)
+      if (curve.knots[q] <= u) i = q;
+    double Nb[4][4];
+    Nb[0][0] = 1.0;
+    double left[4], right[4];
+    for (int d = 1; d <= 3; ++d) {
+      left[d] = u - curve.knots[i + 1 - d];
+      right[d] = curve.knots[i + d] - u;
+      double saved = 0.0;
+      for (int r = 0; r < d; ++r) {
+        const double den = right[r + 1] + left[d - r];
+        const double tmp = (den != 0.0) ? Nb[d - 1][r] / den : 0.0;
+        Nb[d][r] = saved + right[r + 1] * tmp;
+        saved = left[d - r] * tmp;
+      }
+      Nb[d][d] = saved;
+    }
+    double bj = 0.0;
+    for (int r = 0; r < 4; ++r) {
+      const int c = i - 3 + r;
+      const int f = (c < K) ? c : (periodic ? c - K : 0);
+      if (f == j) bj += Nb[3][r];
+    }
+    if (bj == 0.0) continue;
+    const double w = dL[row + p] * dv;
+    ax += w * bj * nrm[2 * (row + p)];
+    az += w * bj * nrm[2 * (row + p) + 1];
+  }
+  __shared__ double sx[256], sz[256];
+  sx[threadIdx.x] = ax;
+  sz[threadIdx.x] = az;
+  __syncthreads();
+  for (int h = blockDim.x / 2; h > 0; h >>= 1) {
+    if (threadIdx.x < h) {
+      sx[threadIdx.x] += sx[threadIdx.x + h];
+      sz[threadIdx.x] += sz[threadIdx.x + h];
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    out[(long long)smp * 2 * K + j] = sx[0];
+    out[(long long)smp * 2 * K + K + j] = sz[0];
+  }
+}
+
 }  // namespace
 
 extern "C" {
+
+int sem_project_from_curve(const double* knots, int32_t ncoef, int32_t K, int32_t periodic,
+                           int32_t nsamples, int32_t npoints, const double* dL_dv, const double* sd,
+                           const double* ustar, const double* normal, const double* v_background,
+                           double v_background_const, double v_inside, double tau, int32_t floor_one,
+                           double* grad_out, void* stream) {
+  if (!knots || !dL_dv || !sd || !ustar || !normal || !grad_out) {
+    g_verr = "null argument";
+    return SEM_ERR_ARG;
+  }
+  if (ncoef < 4 || ncoef > kMaxCoef || K < 1 || K > ncoef || nsamples < 0 || npoints < 0 ||
+      nsamples > 65535) {
+    g_verr = "bad curve size, control-point count or batch size";
+    return SEM_ERR_ARG;
+  }
+  if (nsamples == 0) return SEM_OK;
+  CurveDev cd{};
+  cd.ncoef = ncoef;
+  for (int i = 0; i < ncoef + 4; ++i) cd.knots[i] = knots[i];
+  cd.lo = knots[3];
+  cd.hi = knots[ncoef];
+  project_kernel<<<dim3((unsigned)K, (unsigned)nsamples), 256, 0, (cudaStream_t)stream>>>(
+      cd, K, periodic, npoints, dL_dv, sd, ustar, normal, v_background, v_background_const, v_inside,
+      tau, floor_one, grad_out);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) { g_verr = cudaGetErrorString(e); return SEM_ERR_CUDA; }
+  return SEM_OK;
+}
 
 const char* sem_velocity_last_error(void) { return g_verr.c_str(); }
 

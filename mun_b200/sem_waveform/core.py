@@ -249,6 +249,45 @@ class SEMSimulation:
         return vel.build_velocity_2d_background_with_anomaly(
             self.global_coords, self.v_background, ctrl, v_in, tau, samples, 7, blend)
 
+    def _velocity_on_device(self):
+        return self.device.type == "cuda" and self.config["method"].get("velocity_on_device", True)
+
+    def _build_velocity_dev(self, ctrl_abs, sync=False):
+        """Device tensors (velocity, sd, u_star, normal) of ``_build_velocity``'s on-device
+        branch, left on the GPU."""
+        vp = self.config["velocity"]
+        tau, samples = float(vp["tau"]), int(vp["spline_samples"])
+        anom = vp.get("anomaly", {}) if isinstance(vp.get("anomaly", {}), dict) else {}
+        ctrl = np.reshape(ctrl_abs, (6, 2) if self.variant == "canonical" else (-1, 2))
+        v_in = self.vmin if self.variant == "canonical" else float(anom.get("v_inside", self.vmin))
+        blend = "smooth" if self.variant == "canonical" else str(anom.get("blend", "smooth"))
+        if not hasattr(self, "_coords_dev"):
+            self._coords_dev = torch.as_tensor(self.global_coords, device=self.device)
+            bg = self._background()
+            self._bg_dev = None if bg is None else torch.as_tensor(bg, device=self.device)
+        return vel.build_velocity_device(
+            self._coords_dev, ctrl, tau, samples, v_in, v_outside=self.vmax, v_background_dev=self._bg_dev,
+            periodic=(self.variant == "grid2d"), blend=blend, sync=sync)
+
+    def _project_dev(self, ctrl_abs, dL, sd, us, nrm):
+        """(S, 2K) interleaved [x0, z0, x1, z1, ...] control-point gradients on the device
+        (the same projection as ``_analytical_gradient_projection_improved``)."""
+        vp = self.config["velocity"]
+        anom = vp.get("anomaly", {}) if isinstance(vp.get("anomaly", {}), dict) else {}
+        ctrl = np.reshape(ctrl_abs, (-1, 2))
+        K = ctrl.shape[0]
+        if self.variant == "canonical":
+            g = vel.project_ctrl_device(ctrl, False, dL, sd, us, nrm, self.vmin, float(vp["tau"]),
+                                        v_background_const=self.vmax, floor_one=False)
+        else:
+            g = vel.project_ctrl_device(ctrl, self.variant == "grid2d", dL, sd, us, nrm,
+                                        float(anom.get("v_inside", self.vmin)), float(vp["tau"]),
+                                        v_background_dev=self._bg_dev, floor_one=True)
+        out = torch.empty_like(g)
+        out[:, 0::2] = g[:, :K]
+        out[:, 1::2] = g[:, K:]
+        return out
+
     def _background(self):
         if self.variant == "layered":
             return self.v_layer_background
@@ -342,21 +381,29 @@ class SEMSimulation:
     def _align_observation_data(self, y_obs, obs_dt, obs_nt):
         return align_observation(y_obs, obs_dt, obs_nt, self.dt, self.nt)
 
-    def _solve_spec(self, velocity, y_obs, obs_dt, obs_nt, sigma2, exact=False, ckpt_k=0):
+    def _solve_spec(self, velocity, y_obs, obs_dt, obs_nt, sigma2, exact=False, ckpt_k=0, y_cache=None,
+                    y_key=None):
         it0, it1, decim = misfit_window(self.config.get("method", {}).get("misfit_window", None),
                                         self.dt, self.nt)
         nt_eff = it1 - it0
         nt_dec = -(-nt_eff // decim)
         dt_eff = self.dt * decim
-        y = np.asarray(y_obs, dtype=np.float64)
-        if abs(dt_eff - obs_dt) < 1e-12 and nt_dec == obs_nt and y.shape[0] == nt_dec:
-            ya = y
+        if y_cache is not None and y_key in y_cache:
+            y_dev = y_cache[y_key]
         else:
-            ya = align_observation(y, obs_dt, obs_nt, dt_eff, nt_dec)
-        if ya.shape[1] != self.num_receivers:
-            raise ValueError(f"y_obs has {ya.shape[1]} receivers, expected {self.num_receivers}")
-        return SolveSpec(self._plan(), self._dev(velocity), adjoint=True, exact=exact,
-                         y_obs=self._dev(ya), window=(it0, it1, decim), inv_sigma2=1.0 / sigma2,
+            y = np.asarray(y_obs, dtype=np.float64)
+            if abs(dt_eff - obs_dt) < 1e-12 and nt_dec == obs_nt and y.shape[0] == nt_dec:
+                ya = y
+            else:
+                ya = align_observation(y, obs_dt, obs_nt, dt_eff, nt_dec)
+            if ya.shape[1] != self.num_receivers:
+                raise ValueError(f"y_obs has {ya.shape[1]} receivers, expected {self.num_receivers}")
+            y_dev = self._dev(ya)
+            if y_cache is not None:
+                y_cache[y_key] = y_dev
+        v_dev = velocity if isinstance(velocity, torch.Tensor) else self._dev(velocity)
+        return SolveSpec(self._plan(), v_dev, adjoint=True, exact=exact,
+                         y_obs=y_dev, window=(it0, it1, decim), inv_sigma2=1.0 / sigma2,
                          ckpt_k=ckpt_k), (it0, it1)
 
     def run_forward_and_adjoint(self, params_dict):
@@ -378,13 +425,20 @@ class SEMSimulation:
         obs_nt = int(params_dict["obs_nt"])
         sigma = float(params_dict.get("noise_std", 0.0))
         sigma2 = sigma * sigma + 1e-24
-        velocity_model, signed_dist, extras = self._build_velocity(perts)
+        dev_build = None
+        if self._velocity_on_device():
+            dev_build = self._build_velocity_dev(perts)
+            velocity_model = dev_build[0].cpu().numpy()
+            signed_dist = dev_build[1].cpu().numpy()
+            extras = {"u_star": dev_build[2].cpu().numpy(), "normal_out": dev_build[3].cpu().numpy()}
+        else:
+            velocity_model, signed_dist, extras = self._build_velocity(perts)
         self.velocity_model, self.signed_dist, self.spline_extras = velocity_model, signed_dist, extras
         self.velocity_model_torch = torch.from_numpy(velocity_model)
         self._cfl_update()
         mode = self.config.get("method", {}).get("adjoint_mode", "reference")
-        spec, (it0, it1) = self._solve_spec(velocity_model, y_obs, obs_dt, obs_nt, sigma2,
-                                            exact=(mode == "exact"))
+        spec, (it0, it1) = self._solve_spec(dev_build[0] if dev_build is not None else velocity_model,
+                                            y_obs, obs_dt, obs_nt, sigma2, exact=(mode == "exact"))
         self._get_batch().run([spec])
         self._check_status([spec])
         loglik = float(spec.loglik.item())
@@ -392,10 +446,15 @@ class SEMSimulation:
         clean = spec.rec.double().cpu().numpy()[it0:it1]
         self.dJ_dv = dJ_dv
         dL_dv = -dJ_dv
-        proj = self._analytical_gradient_projection_improved(
-            dL_dv_np=dL_dv, bspline_ctrl=perts, tau=float(self.config["velocity"]["tau"]),
-            signed_dist=signed_dist, extras=extras,
-            spline_samples=int(self.config["velocity"]["spline_samples"]))
+        if dev_build is not None:  # projection on the device, as in the batch path
+            G = self._project_dev(perts, -spec.grad[None], dev_build[1][None], dev_build[2][None],
+                                  dev_build[3][None]).cpu().numpy()[0]
+            proj = {"grad_ctrl_x": G[0::2], "grad_ctrl_z": G[1::2]}
+        else:
+            proj = self._analytical_gradient_projection_improved(
+                dL_dv_np=dL_dv, bspline_ctrl=perts, tau=float(self.config["velocity"]["tau"]),
+                signed_dist=signed_dist, extras=extras,
+                spline_samples=int(self.config["velocity"]["spline_samples"]))
         if self.config["method"].get("VERIFY_PROJECTION", False):
             self._verify_projection(perts, dL_dv, proj, sigma2, obs_dt, obs_nt, y_obs)
         gx = np.asarray(proj["grad_ctrl_x"], dtype=np.float64).reshape(-1)
@@ -409,12 +468,42 @@ class SEMSimulation:
         """Many ``run_forward_and_adjoint`` requests in one batched launch sequence.
         All requests share this simulation's mesh; dt follows the CFL rule applied to
         the fastest model of the batch (the reference would lower ``self.dt`` the same
-        way when the calls run one after another)."""
+        way when the calls run one after another).  With the on-device velocity builder
+        the models, solves and control-point projection stay on the GPU; only the
+        per-sample outputs come back (one copy each for all samples)."""
+        if not self._velocity_on_device():
+            return self._run_forward_and_adjoint_batch_host(params_list, ckpt_k)
+        ctrls = [np.asarray(prm["bspline_ctrl"], dtype=np.float64).reshape(-1, 2) for prm in params_list]
+        builds = [self._build_velocity_dev(c) for c in ctrls]
+        V = torch.stack([b[0] for b in builds])
+        imax = int(torch.argmax(V.max(dim=1).values).item())
+        self.velocity_model = V[imax].cpu().numpy()
+        self._cfl_update()
+        specs, wins, ycache = [], [], {}
+        for i, prm in enumerate(params_list):
+            sigma = float(prm.get("noise_std", 0.0))
+            key = (id(prm["y_obs"]), float(prm["obs_dt"]), int(prm["obs_nt"]))
+            sp, win = self._solve_spec(V[i], prm["y_obs"], float(prm["obs_dt"]), int(prm["obs_nt"]),
+                                       sigma * sigma + 1e-24, ckpt_k=ckpt_k, y_cache=ycache, y_key=key)
+            specs.append(sp)
+            wins.append(win)
+        self._get_batch().run(specs)
+        self._check_status(specs)
+        dL = -torch.stack([sp.grad for sp in specs])
+        G = self._project_dev(ctrls[0], dL, torch.stack([b[1] for b in builds]),
+                              torch.stack([b[2] for b in builds]), torch.stack([b[3] for b in builds])).cpu().numpy()
+        ll = torch.cat([sp.loglik for sp in specs]).cpu().numpy()
+        it0, it1 = wins[0]
+        rec = torch.stack([sp.rec for sp in specs]).double().cpu().numpy()
+        return [{"loglik": float(ll[i]), "grad_wrt_ctrl": G[i], "clean_data": rec[i, it0:it1],
+                 "dt": float(self.dt), "nt": int(self.nt)} for i in range(len(specs))]
+
+    def _run_forward_and_adjoint_batch_host(self, params_list, ckpt_k=0):
+        """Batch path with the host velocity builders and host projection."""
         builds = []
         for prm in params_list:
             perts = np.asarray(prm["bspline_ctrl"], dtype=np.float64).reshape(-1, 2)
             builds.append((perts,) + tuple(self._build_velocity(perts)))
-        vmax_model = max(float(np.max(b[1])) for b in builds)
         self.velocity_model = builds[int(np.argmax([np.max(b[1]) for b in builds]))][1]
         self._cfl_update()
         specs, wins = [], []
@@ -437,7 +526,6 @@ class SEMSimulation:
             outs.append({"loglik": float(sp.loglik.item()), "grad_wrt_ctrl": g,
                          "clean_data": sp.rec.double().cpu().numpy()[it0:it1],
                          "dt": float(self.dt), "nt": int(self.nt)})
-        del vmax_model
         return outs
 
     def run_forward_only_for_loglik(self, ctrl12, sigma2, obs_dt, obs_nt, y_obs):

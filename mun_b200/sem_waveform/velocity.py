@@ -280,11 +280,12 @@ def build_velocity_2d_background_with_anomaly(nodes_xy, v_background, ctrl6_xy=N
 
 
 def build_velocity_device(coords_dev, ctrl, tau, samples, v_inside, v_outside=None, v_background_dev=None,
-                          newton_steps=7, periodic=False, blend="smooth", stream=None):
+                          newton_steps=7, periodic=False, blend="smooth", stream=None, sync=True):
     """Same result as the host builders above, computed on the GPU
     (``sem_velocity_from_curve``).  ``coords_dev``: (P,2) float64 CUDA tensor; the
     background is either ``v_outside`` (constant) or ``v_background_dev`` (P,).
-    Returns CUDA tensors (velocity, sd, u_star, normal_out)."""
+    Returns CUDA tensors (velocity, sd, u_star, normal_out).  ``sync=False`` leaves the
+    build queued on the current stream (the outputs are stream-ordered tensors)."""
     import ctypes as C
 
     import torch
@@ -320,6 +321,37 @@ def build_velocity_device(coords_dev, ctrl, tau, samples, v_inside, v_outside=No
         C.c_void_p(sd.data_ptr()), C.c_void_p(us.data_ptr()), C.c_void_p(nr.data_ptr()), C.c_void_p(strm))
     if rc != 0:
         raise ValueError("sem_velocity_from_curve: " + lib.sem_velocity_last_error().decode())
-    torch.cuda.current_stream().synchronize() if stream is None else None
+    if sync and stream is None:
+        torch.cuda.current_stream().synchronize()
     del u0_d, s_d, cs
     return vel, sd, us, nr
+
+
+def project_ctrl_device(ctrl, periodic, dL, sd, us, nrm, v_inside, tau, v_background_dev=None,
+                        v_background_const=0.0, floor_one=True):
+    """Control-point gradients for a batch on the GPU (``sem_project_from_curve``).
+    dL, sd, us: (S, P) float64 CUDA tensors, nrm (S, P, 2); returns (S, 2K) with the K
+    x-components first, then the K z-components."""
+    import ctypes as C
+
+    import torch
+
+    from .. import _lib
+    P = np.asarray(ctrl, dtype=np.float64).reshape(-1, 2)
+    K = P.shape[0]
+    sp = closed_spline_periodic(P) if periodic else closed_spline_clamped(P)
+    knots = np.ascontiguousarray(sp.t, dtype=np.float64)
+    S, npts = dL.shape
+    out = torch.empty((S, 2 * K), dtype=torch.float64, device=dL.device)
+    tens = [t.contiguous() for t in (dL, sd, us, nrm)]
+    lib = _lib.load()
+    rc = lib.sem_project_from_curve(
+        knots.ctypes.data_as(C.c_void_p), int(len(sp.c)), int(K), 1 if periodic else 0, int(S), int(npts),
+        C.c_void_p(tens[0].data_ptr()), C.c_void_p(tens[1].data_ptr()), C.c_void_p(tens[2].data_ptr()),
+        C.c_void_p(tens[3].data_ptr()),
+        C.c_void_p(v_background_dev.data_ptr()) if v_background_dev is not None else None,
+        float(v_background_const), float(v_inside), float(tau), 1 if floor_one else 0,
+        C.c_void_p(out.data_ptr()), C.c_void_p(torch.cuda.current_stream().cuda_stream))
+    if rc != 0:
+        raise ValueError("sem_project_from_curve: " + lib.sem_velocity_last_error().decode())
+    return out
