@@ -16,6 +16,7 @@ O((nt/k + k) npoints) and results do not depend on k (bitwise).
 """
 from __future__ import annotations
 
+import collections
 import os
 import time
 import warnings
@@ -34,6 +35,13 @@ from .receivers import receiver_matrix, circle_positions
 from .boundary import setup_pml
 from .sources import create_source_wavelet
 from .utils import adjust_time_step_for_stability, check_cfl_condition
+
+
+# Plans (device tables of one mesh / dt / nt / source / receiver set) shared by every
+# simulation in the process: MUN's MCMC constructs a new simulation for each proposal
+# (Bspline_Coupling/MCMC/MCMC.py:193-208), which then finds its plan here.  LRU-bounded.
+_PLAN_CACHE = collections.OrderedDict()
+_PLAN_CACHE_MAX = 64
 
 
 class SEMSimulation:
@@ -300,12 +308,24 @@ class SEMSimulation:
         key = (float(self.dt), int(self.nt))
         p = self._plans.get(key)
         if p is None:
-            p = SEMPlan(xmin=self.xmin, xmax=self.xmax, zmin=self.zmin, zmax=self.zmax,
-                        nelx=self.nelem_x, nelz=self.nelem_z, npol=self.npol, dt=self.dt, nt=self.nt,
-                        src_xz=(self.src_x, self.src_z), f0=self.src_f0, amp=self.src_amp,
-                        receivers=np.asarray(self.receiver_coords_sem), pml_thickness=float(
-                            self.config["method"]["pml_thickness"]), sponge_cmax=self.vmax,
-                        coords=self.global_coords, node_grid=self.node_grid)
+            rec = np.ascontiguousarray(self.receiver_coords_sem, dtype=np.float64)
+            gkey = (torch.cuda.current_device(), float(self.xmin), float(self.xmax), float(self.zmin),
+                    float(self.zmax), int(self.nelem_x), int(self.nelem_z), int(self.npol), float(self.dt),
+                    int(self.nt), float(self.src_x), float(self.src_z), float(self.src_f0),
+                    float(self.src_amp), rec.tobytes(), float(self.config["method"]["pml_thickness"]),
+                    float(self.vmax))
+            p = _PLAN_CACHE.get(gkey)
+            if p is None:
+                p = SEMPlan(xmin=self.xmin, xmax=self.xmax, zmin=self.zmin, zmax=self.zmax,
+                            nelx=self.nelem_x, nelz=self.nelem_z, npol=self.npol, dt=self.dt, nt=self.nt,
+                            src_xz=(self.src_x, self.src_z), f0=self.src_f0, amp=self.src_amp,
+                            receivers=rec, pml_thickness=float(self.config["method"]["pml_thickness"]),
+                            sponge_cmax=self.vmax, coords=self.global_coords, node_grid=self.node_grid)
+                _PLAN_CACHE[gkey] = p
+                while len(_PLAN_CACHE) > _PLAN_CACHE_MAX:
+                    _PLAN_CACHE.popitem(last=False)
+            else:
+                _PLAN_CACHE.move_to_end(gkey)
             self._plans[key] = p
         return p
 
@@ -642,3 +662,45 @@ class SEMSimulation:
         for i in range(len(pa)):
             ratio = pa[i] / pf[i] if pf[i] != 0 else float("inf")
             print(f"{i:2d}   | {pa[i]:14.6e} | {pf[i]:14.6e} | {ratio:11.3f}")
+
+
+def run_forward_and_adjoint_sources(sims, params_list):
+    """Several ``run_forward_and_adjoint`` requests on different simulations (e.g. one
+    per source position, as MUN's multi-source likelihood builds them:
+    ``CO2_plume/one_stage/single_cubic/RQS_NF.py:1028-1091``) in one batched launch
+    sequence instead of one solve per thread.  Each simulation keeps its own plan, CFL
+    update and side effects; the returned dicts are those of the separate calls, bitwise.
+    The simulations must live on one CUDA device and build their velocity on it."""
+    if len(sims) != len(params_list):
+        raise ValueError("one parameter dict per simulation")
+    if not sims:
+        return []
+    for s in sims:
+        if not s._velocity_on_device():
+            raise ValueError("run_forward_and_adjoint_sources needs the on-device velocity builder")
+    reqs = []
+    for sim, prm in zip(sims, params_list):
+        perts = np.asarray(prm["bspline_ctrl"], dtype=np.float64).reshape(-1, 2)
+        build = sim._build_velocity_dev(perts)
+        sim.velocity_model = build[0].cpu().numpy()
+        sim.signed_dist = build[1].cpu().numpy()
+        sim.spline_extras = {"u_star": build[2].cpu().numpy(), "normal_out": build[3].cpu().numpy()}
+        sim.velocity_model_torch = torch.from_numpy(sim.velocity_model)
+        sim._cfl_update()
+        sigma = float(prm.get("noise_std", 0.0))
+        mode = sim.config.get("method", {}).get("adjoint_mode", "reference")
+        spec, win = sim._solve_spec(build[0], prm["y_obs"], float(prm["obs_dt"]), int(prm["obs_nt"]),
+                                    sigma * sigma + 1e-24, exact=(mode == "exact"))
+        reqs.append((sim, perts, build, spec, win))
+    specs = [r[3] for r in reqs]
+    sims[0]._get_batch().run(specs)
+    for sim, _, _, spec, _ in reqs:
+        sim._check_status([spec])
+    outs = []
+    for sim, perts, build, spec, (it0, it1) in reqs:
+        sim.dJ_dv = spec.grad.cpu().numpy()
+        G = sim._project_dev(perts, -spec.grad[None], build[1][None], build[2][None], build[3][None])
+        outs.append({"loglik": float(spec.loglik.item()), "grad_wrt_ctrl": G.cpu().numpy()[0],
+                     "clean_data": spec.rec.double().cpu().numpy()[it0:it1], "dt": float(sim.dt),
+                     "nt": int(sim.nt)})
+    return outs
