@@ -61,6 +61,18 @@ def workload(nmodels=256, nelx=100, nelz=50, nt=3000, nrec=100, seed0=0):
                 npoints=len(coords), dt=dt, nt=nt, sigma=1e-3)
 
 
+def max_over_ranks(x, world, device=None):
+    """Largest value of x over the ranks of the job (the job's time is its slowest rank's);
+    every rank must call it at the same point."""
+    if world <= 1:
+        return float(x)
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def parse_tile(t):
     """'8x4' -> (8, 4); 'auto' -> (0, 0) (the library picks the shape)."""
     return (0, 0) if t == "auto" else tuple(int(x) for x in t.split("x"))
@@ -605,10 +617,7 @@ def main():
     kern_bytes = W["npoints"] * (n // groups_used) * (
         BYTES_PER_NODE_FWD_TICK * fwd_like + BYTES_PER_NODE_ADJ_TICK * groups_used * W["nt"])
     tick_loop_ms = float(np.mean(tick_ms))
-    if world > 1:
-        t = torch.tensor([ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = max_over_ranks(ms, world, dev)
     status = torch.cat([s.status for s in specs]).max().item()
     value = n * world / (ms / 1e3)
 
@@ -633,7 +642,7 @@ def main():
         ev1.synchronize()
         if it >= args.warmup:
             e2e_ms.append(ev0.elapsed_time(ev1))
-    e2e = float(np.mean(e2e_ms))
+    e2e = max_over_ranks(float(np.mean(e2e_ms)), world, dev)
     h2d = pin_v.numel() * 8 + pin_y.numel() * 8
     d2h = out_g.numel() * 8 + out_l.numel() * 8
 
