@@ -567,6 +567,9 @@ __global__ void __launch_bounds__(256) sem_tick_kernel(const SolveDev* __restric
 #ifndef SEM_PAIRED
 #define SEM_PAIRED 1
 #endif
+#ifndef SEM_SPREAD_ISSUE
+#define SEM_SPREAD_ISSUE 1
+#endif
 #ifndef SEM_GRAD_STAGE
 #define SEM_GRAD_STAGE 0
 #endif
@@ -798,9 +801,12 @@ __device__ __forceinline__ void strip_tick(const SolveDev& S, const int act, con
     const unsigned rowb = (unsigned)(ce - cs) * 4u;
     const int nd = (ADJ && SEM_GRAD_STAGE) ? NP : 0;
     const int ncopy = nload * NP + nd;
-    if (lane == 0) mbar_expect_tx(bars + slot, (unsigned)(nload * NP) * rowb + (unsigned)nd * rowb * 2u);
+    // copies spread over the warps (or warp 0 alone); a copy may complete before the
+    // expected bytes are posted: the barrier's pending arrival keeps the phase open
+    if (warp == 0 && lane == 0)
+      mbar_expect_tx(bars + slot, (unsigned)(nload * NP) * rowb + (unsigned)nd * rowb * 2u);
     __syncwarp();
-    for (int q = lane; q < ncopy; q += 32) {
+    for (int q = SEM_SPREAD_ISSUE ? lane * NW + warp : lane; q < ncopy; q += SEM_SPREAD_ISSUE ? 32 * NW : 32) {
       if (q < nload * NP) {
         const int f = q / NP, a = q - f * NP;
         const float* base = (f == 0) ? cur : (f == 1) ? c2p : (f == 2) ? vin : fwdu;
@@ -814,7 +820,7 @@ __device__ __forceinline__ void strip_tick(const SolveDev& S, const int act, con
       }
     }
   };
-  if (warp == 0)
+  if (SEM_SPREAD_ISSUE || warp == 0)
     for (int r = 0; r < min(NST, nbands); ++r) issue(ezs + r);
 
   // D and beta: per-order constants (c_D[N], c_B[N])
@@ -930,7 +936,7 @@ __device__ __forceinline__ void strip_tick(const SolveDev& S, const int act, con
     if (final_only) {
       __syncthreads();  // done with this slot
       if (*s_abort <= ez) { abort_ez = ez; break; }
-      if (warp == 0 && rel + NST < nbands) issue(ez + NST);
+      if ((SEM_SPREAD_ISSUE || warp == 0) && rel + NST < nbands) issue(ez + NST);
       continue;
     }
     if (ADJ && in_win && j1 > j0) {  // adjoint source of receivers in this element row
@@ -1070,7 +1076,7 @@ __device__ __forceinline__ void strip_tick(const SolveDev& S, const int act, con
     __syncthreads();
     if (*s_abort <= ez) { abort_ez = ez; break; }
     // every thread is past phase B of the previous band: warp 0 refills its slot
-    if (warp == 0 && rel >= 1 && rel - 1 + NST < nbands) issue(ez - 1 + NST);
+    if ((SEM_SPREAD_ISSUE || warp == 0) && rel >= 1 && rel - 1 + NST < nbands) issue(ez - 1 + NST);
     if (halo) {  // carries into the first owned row only
       if (owned) {
         zc = rz[N];
