@@ -567,12 +567,6 @@ __global__ void __launch_bounds__(256) sem_tick_kernel(const SolveDev* __restric
 #ifndef SEM_PAIRED
 #define SEM_PAIRED 1
 #endif
-#ifndef SEM_SPREAD_ISSUE
-#define SEM_SPREAD_ISSUE 1
-#endif
-#ifndef SEM_GRAD_STAGE
-#define SEM_GRAD_STAGE 0
-#endif
 #ifndef SEM_STAGES_ADJ
 #define SEM_STAGES_ADJ 3
 #endif
@@ -658,7 +652,7 @@ __device__ __forceinline__ void bulk_load(void* dst, const void* src, unsigned b
 
 __host__ __device__ inline long long strip_stage_floats(int N, bool adj) {
   const int nfloat = adj ? 4 : 3;  // cur, c2, v (+ forward field)
-  const int ndouble = (adj && SEM_GRAD_STAGE) ? 1 : 0;  // gradient accumulator
+  const int ndouble = 0;  // the float64 gradient is loaded by its owner threads, not staged
   return ((long long)(nfloat + 2 * ndouble) * (N + 1) * strip_bw(N) + 31) & ~31LL;
 }
 // exchange arrays: x-segment results Xs[rows][segments][N+1] (+ sensitivity), z-segment
@@ -795,33 +789,28 @@ __device__ __forceinline__ void strip_tick(const SolveDev& S, const int act, con
 
   // TMA: element row `ez` of every field into ring slot (ez - ezs) % NST (one warp: lane 0
   // posts the expected bytes, then each lane issues row copies)
+  // The row copies of a band (field f, row a: nload * NP <= 4 * 8 < NT of them) are spread
+  // over all warps, one per thread at most (copy q = lane * NW + warp, so every warp
+  // issues a few): each thread fixes its copy's slot offset and source once per tick and
+  // adds the band's offset.  A copy may complete before lane 0 of warp 0 posts the
+  // expected bytes: the barrier's pending arrival keeps the phase open until then.
+  const unsigned rowb = (unsigned)(ce - cs) * 4u;
+  const int myq = lane * NW + warp;
+  const bool has_copy = myq < nload * NP;
+  int cp_dst = 0;
+  const float* cp_src = cur;
+  if (has_copy) {
+    const int f = myq / NP, a = myq - f * NP;
+    cp_src = ((f == 0) ? cur : (f == 1) ? c2p : (f == 2) ? vin : fwdu) + (long long)a * pitch + cs;
+    cp_dst = (f * NP + a) * BW + (cs - X0);
+  }
+  const long long band_floats = (long long)N * pitch;
   auto issue = [&](int ez) {
     const int slot = (ez - ezs) % NST;
-    float* st = stages + slot * stage_f;
-    const unsigned rowb = (unsigned)(ce - cs) * 4u;
-    const int nd = (ADJ && SEM_GRAD_STAGE) ? NP : 0;
-    const int ncopy = nload * NP + nd;
-    // copies spread over the warps (or warp 0 alone); a copy may complete before the
-    // expected bytes are posted: the barrier's pending arrival keeps the phase open
-    if (warp == 0 && lane == 0)
-      mbar_expect_tx(bars + slot, (unsigned)(nload * NP) * rowb + (unsigned)nd * rowb * 2u);
-    __syncwarp();
-    for (int q = SEM_SPREAD_ISSUE ? lane * NW + warp : lane; q < ncopy; q += SEM_SPREAD_ISSUE ? 32 * NW : 32) {
-      if (q < nload * NP) {
-        const int f = q / NP, a = q - f * NP;
-        const float* base = (f == 0) ? cur : (f == 1) ? c2p : (f == 2) ? vin : fwdu;
-        bulk_load(st + (f * NP + a) * BW + (cs - X0), base + (long long)(ez * N + a) * pitch + cs,
-                  rowb, bars + slot);
-      } else {
-        const int a = q - nload * NP;
-        double* gs = reinterpret_cast<double*>(st + NF * NP * BW);
-        bulk_load(gs + a * BW + (cs - X0), gradp + (long long)(ez * N + a) * pitch + cs,
-                  rowb * 2u, bars + slot);
-      }
-    }
+    if (warp == 0 && lane == 0) mbar_expect_tx(bars + slot, (unsigned)(nload * NP) * rowb);
+    if (has_copy) bulk_load(stages + slot * stage_f + cp_dst, cp_src + ez * band_floats, rowb, bars + slot);
   };
-  if (SEM_SPREAD_ISSUE || warp == 0)
-    for (int r = 0; r < min(NST, nbands); ++r) issue(ezs + r);
+  for (int r = 0; r < min(NST, nbands); ++r) issue(ezs + r);
 
   // D and beta: per-order constants (c_D[N], c_B[N])
 #define Dr(a, b) c_D[N][(a) * NP + (b)]
@@ -882,9 +871,6 @@ __device__ __forceinline__ void strip_tick(const SolveDev& S, const int act, con
     const float* Cs = st + NP * BW;
     const float* Vs = st + 2 * NP * BW;
     const float* Us = st + 3 * NP * BW;
-#if SEM_GRAD_STAGE
-    const double* Gs = reinterpret_cast<const double*>(st + NF * NP * BW);
-#endif
     float* const Xs = xs0 + (ez & 1) * XSZ;
     float* const SXs = Xs + NP * SEGS * NP;
     float* const tzb = sTz + (ez & 1) * 24;
@@ -899,14 +885,12 @@ __device__ __forceinline__ void strip_tick(const SolveDev& S, const int act, con
     }
     // a failed wait records the first band that failed; every thread tests "failed at or
     // before this band" after the band's barrier, so all threads leave at the same band
-#if !SEM_GRAD_STAGE
     // the owner's gradient rows of this band, loaded now and used in phase B
     double gpre[N];
     if (ADJ && grad_on && owned && !halo) {
 #pragma unroll
       for (int a = 0; a < N; ++a) gpre[a] = gradp[gb + a * pitch];
     }
-#endif
     if (!mbar_wait(bars + slot, (unsigned)((rel / NST) & 1))) atomicMin(s_abort, ez);
     const bool last = (ez == nelz - 1);
 
@@ -936,7 +920,7 @@ __device__ __forceinline__ void strip_tick(const SolveDev& S, const int act, con
     if (final_only) {
       __syncthreads();  // done with this slot
       if (*s_abort <= ez) { abort_ez = ez; break; }
-      if ((SEM_SPREAD_ISSUE || warp == 0) && rel + NST < nbands) issue(ez + NST);
+      if (rel + NST < nbands) issue(ez + NST);
       continue;
     }
     if (ADJ && in_win && j1 > j0) {  // adjoint source of receivers in this element row
@@ -1076,7 +1060,7 @@ __device__ __forceinline__ void strip_tick(const SolveDev& S, const int act, con
     __syncthreads();
     if (*s_abort <= ez) { abort_ez = ez; break; }
     // every thread is past phase B of the previous band: warp 0 refills its slot
-    if ((SEM_SPREAD_ISSUE || warp == 0) && rel >= 1 && rel - 1 + NST < nbands) issue(ez - 1 + NST);
+    if (rel >= 1 && rel - 1 + NST < nbands) issue(ez - 1 + NST);
     if (halo) {  // carries into the first owned row only
       if (owned) {
         zc = rz[N];
@@ -1123,11 +1107,7 @@ __device__ __forceinline__ void strip_tick(const SolveDev& S, const int act, con
           extra = (ez * N + a == src_row) ? src_val : 0.f;
         } else {
           extra = in_win ? sacc[a * NT + tid] : 0.f;
-#if SEM_GRAD_STAGE
-          if (grad_on) gnew = Gs[a * BW + sc] + (double)(Rzv * SX + Rxv * SZ);
-#else
           if (grad_on) gnew = (a < N ? gpre[a < N ? a : 0] : gradp[g]) + (double)(Rzv * SX + Rxv * SZ);
-#endif
         }
         float res, vres;
         advance_node(ADJ, damp, Bs[a * BW + sc], Vs[a * BW + sc], X, Z, ixv, Rxv, dxv, izv, Rzv,

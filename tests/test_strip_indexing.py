@@ -212,3 +212,13 @@ def test_strip_chunks_partition_and_ring(nelz, zch):
                     if not (has_halo and rel == 0):
                         owner[ez] += 1
             assert (owner == 1).all()
+
+
+@pytest.mark.parametrize("N", [1, 2, 3, 4, 5, 6, 7])
+def test_ring_copies_one_per_thread(N):
+    # copy q = lane * NW + warp of each band: every (field, row) copy exactly once
+    NP, NW = N + 1, THREADS // 32
+    for nload in (1, 3, 4):
+        qs = [lane * NW + warp for tid in range(THREADS) for warp, lane in [divmod(tid, 32)]]
+        mine = [q for q in qs if q < nload * NP]
+        assert sorted(mine) == list(range(nload * NP))
