@@ -200,6 +200,18 @@ __host__ __device__ inline long long smem_floats(int N, int tex, int tez, bool a
 }
 
 
+// The zero-lag sensitivity increment of one node, R_z S_x + R_x S_z, rounded the same way
+// in every kernel.
+__device__ __forceinline__ double sens_increment(float Rzv, float SX, float Rxv, float SZ) {
+  return (double)__fmaf_rn(Rzv, SX, __fmul_rn(Rxv, SZ));
+}
+// Sensitivity of one segment node, beta_a (D w)_a (D lambda)_a, multiplied left to right.
+__device__ __forceinline__ float sens_product(float beta, float dw, float du) {
+  return __fmul_rn(__fmul_rn(beta, dw), du);
+}
+// Squared residual accumulated into a receiver's misfit (multiply, then add).
+__device__ __forceinline__ void misfit_add(double* m, double res) { *m = __dadd_rn(*m, __dmul_rn(res, res)); }
+
 // One owned node: combine the line operators, advance (b, v) or (lambda, mu), apply
 // the sponge.  Shared by both kernel variants so their arithmetic is identical.
 //   forward:  w = v - P K + src          adjoint: w = mu + P (inj - K)
@@ -208,22 +220,23 @@ __device__ __forceinline__ void advance_node(bool adj, bool damp, float b, float
                                              float Z, float ixv, float Rxv, float dxv, float izv,
                                              float Rzv, float dzv, float extra, float& bout,
                                              float& vout) {
-  const float P = ixv * izv;
-  const float Kv = Rzv * X + Rxv * Z;
+  // explicit rounding: the same operations in every kernel that inlines this, whatever
+  // the compiler would contract
+  const float P = __fmul_rn(ixv, izv);
+  const float Kv = __fmaf_rn(Rzv, X, __fmul_rn(Rxv, Z));
   float wv;
   if (!adj) {
-    wv = v - P * Kv;
-    wv += extra;
+    wv = __fadd_rn(__fmaf_rn(-P, Kv, v), extra);
   } else {
-    wv = v + P * (extra - Kv);
+    wv = __fmaf_rn(P, __fsub_rn(extra, Kv), v);
   }
   if (damp) {
-    const float d = dxv * dzv;
-    vout = d * wv;
-    bout = d * (b + wv);
+    const float d = __fmul_rn(dxv, dzv);
+    vout = __fmul_rn(d, wv);
+    bout = __fmul_rn(d, __fadd_rn(b, wv));
   } else {
     vout = wv;
-    bout = b + wv;
+    bout = __fadd_rn(b, wv);
   }
 }
 
@@ -364,7 +377,7 @@ __global__ void __launch_bounds__(256) sem_tick_kernel(const SolveDev* __restric
           S.rec_out[(long long)m * S.nrec + r] = acc;
           if ((S.flags & F_MISFIT) && m >= S.it0 && m < S.it1 && ((m - S.it0) % S.decim) == 0) {
             const double res = (double)acc - S.yobs[(long long)((m - S.it0) / S.decim) * S.nrec + r];
-            S.misfit[r] += res * res;
+            misfit_add(S.misfit + r, res);
             S.rmax[r] = fmax(S.rmax[r], fabs(res));
           }
         }
@@ -402,7 +415,8 @@ __global__ void __launch_bounds__(256) sem_tick_kernel(const SolveDev* __restric
             const int j = e / NP, i = e - j * NP;
             const int gx = bx + i, gz = bz + j;
             if (gx >= gxo0 && gx < gxo1 && gz >= gzo0 && gz < gzo1)
-              sacc[(gz - gzo0) * nco + (gx - gxo0)] += wr[e] * rs;
+              sacc[(gz - gzo0) * nco + (gx - gxo0)] =
+                  __fmaf_rn(wr[e], rs, sacc[(gz - gzo0) * nco + (gx - gxo0)]);
           }
           __syncwarp();
         }
@@ -441,7 +455,7 @@ __global__ void __launch_bounds__(256) sem_tick_kernel(const SolveDev* __restric
         float v = 0.f;
 #pragma unroll
         for (int b = 0; b < NP; ++b) v = fmaf(sD[a * NP + b], u[b], v);
-        xs[(sg * NP + a) * nrop + r] = sB[a] * v * du[a];
+        xs[(sg * NP + a) * nrop + r] = sens_product(sB[a], v, du[a]);
       }
     }
   }
@@ -476,7 +490,7 @@ __global__ void __launch_bounds__(256) sem_tick_kernel(const SolveDev* __restric
         float v = 0.f;
 #pragma unroll
         for (int b = 0; b < NP; ++b) v = fmaf(sD[a * NP + b], u[b], v);
-        zs[(sg * NP + a) * ncop + cc] = sB[a] * v * du[a];
+        zs[(sg * NP + a) * ncop + cc] = sens_product(sB[a], v, du[a]);
       }
     }
   }
@@ -505,8 +519,8 @@ __global__ void __launch_bounds__(256) sem_tick_kernel(const SolveDev* __restric
       }
       if (exr < S.nelx) {
         const int o = ((exr - segx0) * NP) * nrop + r;
-        X += xr[o];
-        if (adj) SX += xs[o];
+        X = __fadd_rn(X, xr[o]);
+        if (adj) SX = __fadd_rn(SX, xs[o]);
       }
     }
     if (ja) {
@@ -522,8 +536,8 @@ __global__ void __launch_bounds__(256) sem_tick_kernel(const SolveDev* __restric
       }
       if (ezr < S.nelz) {
         const int o = ((ezr - segz0) * NP) * ncop + cc;
-        Z += zr[o];
-        if (adj) SZ += zs[o];
+        Z = __fadd_rn(Z, zr[o]);
+        if (adj) SZ = __fadd_rn(SZ, zs[o]);
       }
     }
     const float ixv = __ldg(S.tx + gx), Rxv = __ldg(S.tx + S.nxg + gx);
@@ -537,7 +551,7 @@ __global__ void __launch_bounds__(256) sem_tick_kernel(const SolveDev* __restric
       if (gx == S.src_gx && gz == S.src_gz) extra = S.src_term[t];
     } else {
       extra = have_inj ? sacc[r * nco + cc] : 0.f;
-      if (grad_on) S.grad[g] += (double)(Rzv * SX + Rxv * SZ);
+      if (grad_on) S.grad[g] += sens_increment(Rzv, SX, Rxv, SZ);
     }
     float res, vres;
     advance_node(adj, damp, b, v, X, Z, ixv, Rxv, dxv, izv, Rzv, dzv, extra, res, vres);
@@ -911,7 +925,7 @@ __device__ __forceinline__ void strip_tick(const SolveDev& S, const int act, con
           S.rec_out[(long long)ms * S.nrec + r] = acc;
           if ((S.flags & F_MISFIT) && ms >= S.it0 && ms < S.it1 && ((ms - S.it0) % S.decim) == 0) {
             const double res = (double)acc - S.yobs[(long long)((ms - S.it0) / S.decim) * S.nrec + r];
-            S.misfit[r] += res * res;
+            misfit_add(S.misfit + r, res);
             S.rmax[r] = fmax(S.rmax[r], fabs(res));
           }
         }
@@ -942,7 +956,8 @@ __device__ __forceinline__ void strip_tick(const SolveDev& S, const int act, con
           for (int e = lane; e < NP * NP; e += 32) {
             const int j = e / NP, i = e - j * NP;
             const int gxx = bx + i;
-            if (gxx >= sx0 && gxx < so1) sacc[j * NT + (gxx - sx0)] += wr[e] * rs;
+            if (gxx >= sx0 && gxx < so1)
+              sacc[j * NT + (gxx - sx0)] = __fmaf_rn(wr[e], rs, sacc[j * NT + (gxx - sx0)]);
           }
           __syncwarp();
         }
@@ -978,7 +993,7 @@ __device__ __forceinline__ void strip_tick(const SolveDev& S, const int act, con
           float v = 0.f;
 #pragma unroll
           for (int b = 0; b < NP; ++b) v = fmaf(Dr(a2, b), u[b], v);
-          so[a2] = Bt(a2) * v * du[a2];
+          so[a2] = sens_product(Bt(a2), v, du[a2]);
         }
       }
     };
@@ -1052,7 +1067,7 @@ __device__ __forceinline__ void strip_tick(const SolveDev& S, const int act, con
             float v = 0.f;
 #pragma unroll
             for (int b = 0; b < NP; ++b) v = fmaf(Dr(a2, b), u[b], v);
-            sz[a2] = Bt(a2) * v * du[a2];
+            sz[a2] = sens_product(Bt(a2), v, du[a2]);
           }
         }
       }
@@ -1084,17 +1099,19 @@ __device__ __forceinline__ void strip_tick(const SolveDev& S, const int act, con
         // interior column: its segment's entry; edge column: left + right (or one of them)
         const float xL = hasL ? xr[xoL] : 0.f;
         const float xR = hasR ? xr[xoR] : 0.f;
-        const float X = !edge ? xR : (hasR ? xL + xR : xL);
+        const float X = !edge ? xR : (hasR ? __fadd_rn(xL, xR) : xL);
         float SX = 0.f;
         if (ADJ) {
           const float sL = hasL ? sxr[xoL] : 0.f;
           const float sR = hasR ? sxr[xoR] : 0.f;
-          SX = !edge ? sR : (hasR ? sL + sR : sL);
+          SX = !edge ? sR : (hasR ? __fadd_rn(sL, sR) : sL);
         }
         float Z, SZ = 0.f;
         if (a == 0) {
-          Z = (ez >= 1 ? zc : 0.f) + rz[0];
-          if (ADJ) SZ = (ez >= 1 ? szc : 0.f) + sz[0];
+          // explicit adds: the lower segment's value is computed in this thread and must
+          // not be fused with its product into an FMA (the tile kernel adds stored values)
+          Z = __fadd_rn(ez >= 1 ? zc : 0.f, rz[0]);
+          if (ADJ) SZ = __fadd_rn(ez >= 1 ? szc : 0.f, sz[0]);
         } else {
           Z = rz[a];
           if (ADJ) SZ = sz[a];
@@ -1107,7 +1124,7 @@ __device__ __forceinline__ void strip_tick(const SolveDev& S, const int act, con
           extra = (ez * N + a == src_row) ? src_val : 0.f;
         } else {
           extra = in_win ? sacc[a * NT + tid] : 0.f;
-          if (grad_on) gnew = (a < N ? gpre[a < N ? a : 0] : gradp[g]) + (double)(Rzv * SX + Rxv * SZ);
+          if (grad_on) gnew = (a < N ? gpre[a < N ? a : 0] : gradp[g]) + sens_increment(Rzv, SX, Rxv, SZ);
         }
         float res, vres;
         advance_node(ADJ, damp, Bs[a * BW + sc], Vs[a * BW + sc], X, Z, ixv, Rxv, dxv, izv, Rzv,

@@ -36,7 +36,9 @@ def test_strip_forward_adjoint_matches_reference(name):
     print(f"{name} strip: clean {e_clean:.2e} loglik {e_ll:.2e} dL/dv {e_grad:.2e} "
           f"(vs tile kernel {d_tile:.1e}, bitwise={torch.equal(s.grad, t.grad)})")
     assert max(e_clean, e_grad, e_ll) <= TOL
-    assert d_tile <= 1e-6
+    # same arithmetic in both kernels (explicit rounding where a compiler could fuse)
+    assert torch.equal(s.grad, t.grad) and torch.equal(s.rec, t.rec), d_tile
+    assert torch.equal(s.loglik, t.loglik)
 
 
 @pytest.mark.parametrize("name", ["inject_n3", "layered_cfg0"])
