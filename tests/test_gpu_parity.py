@@ -96,13 +96,16 @@ def test_batch_invariance_and_graphs():
             assert torch.equal(a.loglik, b.loglik)
 
 
-def test_nonfinite_velocity_sets_status():
+@pytest.mark.parametrize("kernel", [1, 2])
+@pytest.mark.parametrize("adjoint", [False, True])
+def test_nonfinite_velocity_sets_status(kernel, adjoint):
     g = load("inject_n2")
     plan = plan_for(g["config"], g["dt"], g["nt"])
     v = np.array(g["velocity"])
     v[len(v) // 2] = np.inf
-    s = SolveSpec(plan, dev(v))
-    Batch().run([s])
+    kw = dict(adjoint=True, y_obs=dev(aligned_obs(g)), inv_sigma2=1.0) if adjoint else {}
+    s = SolveSpec(plan, dev(v), **kw)
+    Batch(kernel=kernel).run([s])
     assert int(s.status.item()) != 0
 
 
