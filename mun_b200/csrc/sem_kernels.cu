@@ -1353,6 +1353,25 @@ int set_order_constants(int dev, int N, const double* D, const double* beta) {
   return SEM_OK;
 }
 
+// The dynamic shared-memory limit is an attribute of the kernel function, shared by every
+// host thread that launches it.  It is only ever raised here, so a launch on one thread
+// never finds the limit lowered below its own size by a launch of another thread (the
+// strip and tile kernels of one order run with different sizes for forward-only and
+// adjoint groups).
+cudaError_t raise_smem_limit(const void* fn, size_t smem) {
+  static std::mutex mu;
+  static std::map<std::pair<int, const void*>, size_t> cur;
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  std::lock_guard<std::mutex> lk(mu);
+  size_t& c = cur[std::make_pair(dev, fn)];
+  if (smem <= c) return cudaSuccess;
+  e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e == cudaSuccess) c = smem;
+  return e;
+}
+
 int upload_f32(float** dst, const double* src, size_t n) {
   std::vector<float> tmp(n);
   for (size_t i = 0; i < n; ++i) tmp[i] = (float)src[i];
@@ -1865,7 +1884,7 @@ static int run_group(sem_batch_t* b, const sem_solve_t* solves, int32_t n,
                                            : smem_floats(G.N, cfg.tile_ex, cfg.tile_ez, G.adj)) *
                         sizeof(float);
     if (smem > 227 * 1024) return fail(SEM_ERR_ARG, "tile too large for shared memory");
-    CUDA_TRY(cudaFuncSetAttribute((const void*)fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    CUDA_TRY(raise_smem_limit((const void*)fn, smem));
     launches.push_back(Launch{fn, G.cta0, G.ncta, smem, G.N});
   }
   // solve descriptor sub-array of each group starts at the first solve of that group
@@ -1996,7 +2015,7 @@ int auto_schedule(const sem_solve_t* sv, int n, const sem_launch_cfg_t& cfg, lon
                                        : smem_floats(N0, cfg.tile_ex, cfg.tile_ez, any_adj)) * 4;
     int nb = 1;
     if (smem <= 227 * 1024 &&
-        cudaFuncSetAttribute((const void*)fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) == cudaSuccess &&
+        raise_smem_limit((const void*)fn, smem) == cudaSuccess &&
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, fn, strip ? strip_threads(N0) : cfg.threads, smem) ==
             cudaSuccess)
       nb = std::max(nb, 1);
@@ -2240,7 +2259,7 @@ int sem_forward_noalloc(const sem_plan_t* p, const double* velocity, float* rec_
       velocity, p->node_pos, (float*)(base + o_c2), p->npoints);
   KernelFn fn = kernel_for(p->npol);
   const size_t smem = (size_t)smem_floats(p->npol, kNoAllocTile, kNoAllocTile, false) * sizeof(float);
-  CUDA_TRY(cudaFuncSetAttribute((const void*)fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  CUDA_TRY(raise_smem_limit((const void*)fn, smem));
   for (int tick = 0; tick < p->nt; ++tick) {
     fn<<<ntiles, 256, smem, stream>>>((const SolveDev*)(base + o_desc), (const int*)(base + o_cta),
                                       (const int*)(base + o_tick), kNoAllocTile, kNoAllocTile, 0);
@@ -2642,7 +2661,7 @@ int sem_engine_step(sem_engine_t* e, void* stream_v) {
                                              : smem_floats(G.N, tex, tez, G.adj)) * sizeof(float);
       if (smem > 227 * 1024) return fail(SEM_ERR_ARG, "tile too large for shared memory");
       if (c == 0)
-        CUDA_TRY(cudaFuncSetAttribute((const void*)fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        CUDA_TRY(raise_smem_limit((const void*)fn, smem));
       cudaLaunchConfig_t lc = {};
       lc.gridDim = dim3((unsigned)G.ncta);
       lc.blockDim = dim3(use_strip ? strip_threads(G.N) : 256);

@@ -17,6 +17,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <map>
+#include <mutex>
 #include <string>
 
 #include "../../include/mun_sem.h"
@@ -24,6 +26,22 @@
 namespace {
 
 thread_local std::string g_verr;
+
+// the kernel's dynamic shared-memory limit is shared by all host threads; only raise it,
+// so that a concurrent call with fewer curve samples cannot lower it under a larger launch
+cudaError_t raise_smem_limit(const void* fn, size_t smem) {
+  static std::mutex mu;
+  static std::map<int, size_t> cur;
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  std::lock_guard<std::mutex> lk(mu);
+  size_t& c = cur[dev];
+  if (smem <= c) return cudaSuccess;
+  e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e == cudaSuccess) c = smem;
+  return e;
+}
 
 constexpr int kMaxCoef = 64;
 constexpr int kMaxSamples = 4096;
@@ -294,8 +312,7 @@ int sem_velocity_from_curve(const sem_curve_t* c, int32_t npoints, const double*
   if (npoints == 0) return SEM_OK;
   const int threads = 128;
   const size_t smem = (size_t)2 * c->nsamples * sizeof(double);
-  cudaError_t e = cudaFuncSetAttribute((const void*)velocity_kernel,
-                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  cudaError_t e = raise_smem_limit((const void*)velocity_kernel, smem);
   if (e != cudaSuccess) { g_verr = cudaGetErrorString(e); return SEM_ERR_CUDA; }
   velocity_kernel<<<(npoints + threads - 1) / threads, threads, smem, (cudaStream_t)stream>>>(
       cd, c->u0, c->samples, c->nsamples, c->newton_steps, coords, npoints, v_background,

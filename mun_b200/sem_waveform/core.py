@@ -18,6 +18,7 @@ from __future__ import annotations
 
 import collections
 import os
+import threading
 import time
 import warnings
 
@@ -40,8 +41,12 @@ from .utils import adjust_time_step_for_stability, check_cfl_condition
 # Plans (device tables of one mesh / dt / nt / source / receiver set) shared by every
 # simulation in the process: MUN's MCMC constructs a new simulation for each proposal
 # (Bspline_Coupling/MCMC/MCMC.py:193-208), which then finds its plan here.  LRU-bounded.
+# MUN's CO2 drivers call run_forward_and_adjoint from several threads at once, each on its
+# own cached simulation (CO2_plume/one_stage/single_cubic/RQS_NF.py:1064-1072): the lookup, insertion and
+# eviction happen under one lock.
 _PLAN_CACHE = collections.OrderedDict()
 _PLAN_CACHE_MAX = 64
+_PLAN_LOCK = threading.Lock()
 
 
 class SEMSimulation:
@@ -314,18 +319,22 @@ class SEMSimulation:
                     int(self.nt), float(self.src_x), float(self.src_z), float(self.src_f0),
                     float(self.src_amp), rec.tobytes(), float(self.config["method"]["pml_thickness"]),
                     float(self.vmax))
-            p = _PLAN_CACHE.get(gkey)
+            with _PLAN_LOCK:
+                p = _PLAN_CACHE.get(gkey)
+                if p is not None:
+                    _PLAN_CACHE.move_to_end(gkey)
             if p is None:
                 p = SEMPlan(xmin=self.xmin, xmax=self.xmax, zmin=self.zmin, zmax=self.zmax,
                             nelx=self.nelem_x, nelz=self.nelem_z, npol=self.npol, dt=self.dt, nt=self.nt,
                             src_xz=(self.src_x, self.src_z), f0=self.src_f0, amp=self.src_amp,
                             receivers=rec, pml_thickness=float(self.config["method"]["pml_thickness"]),
                             sponge_cmax=self.vmax, coords=self.global_coords, node_grid=self.node_grid)
-                _PLAN_CACHE[gkey] = p
-                while len(_PLAN_CACHE) > _PLAN_CACHE_MAX:
-                    _PLAN_CACHE.popitem(last=False)
-            else:
-                _PLAN_CACHE.move_to_end(gkey)
+                with _PLAN_LOCK:
+                    # another thread may have built the same plan meanwhile: keep the first
+                    p = _PLAN_CACHE.setdefault(gkey, p)
+                    _PLAN_CACHE.move_to_end(gkey)
+                    while len(_PLAN_CACHE) > _PLAN_CACHE_MAX:
+                        _PLAN_CACHE.popitem(last=False)
             self._plans[key] = p
         return p
 

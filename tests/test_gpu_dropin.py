@@ -86,3 +86,41 @@ def test_multi_source_batch_equals_separate_calls():
         np.testing.assert_array_equal(s["grad_wrt_ctrl"], b["grad_wrt_ctrl"])
         np.testing.assert_array_equal(s["clean_data"], b["clean_data"])
         assert s["dt"] == b["dt"] and s["nt"] == b["nt"]
+
+
+def test_concurrent_threads_on_separate_simulations():
+    """MUN's multi-source likelihood runs one simulation per source on up to three Python
+    threads (CO2_plume/one_stage/single_cubic/RQS_NF.py:1064-1072).  The same pattern here,
+    with fresh simulations so the threads also race on the shared plan cache, gives bitwise
+    the serial results."""
+    import copy
+    from concurrent.futures import ThreadPoolExecutor
+    from mun_b200.sem_waveform import core
+    g = load("layered_cfg0")
+    nt = int(g["nt"])
+    xs = (500.0, 800.0, 1000.0, 1200.0, 1500.0)
+
+    def cfg_for(x):
+        cfg = copy.deepcopy(g["config"])
+        cfg["source"]["position"] = [x, float(cfg["source"]["position"][1])]
+        return cfg
+
+    def params(k):
+        return {"bspline_ctrl": (np.asarray(g["ctrl"]) + 5.0 * k).reshape(-1), "y_obs": g["y_obs"],
+                "obs_dt": float(g["dt"]), "obs_nt": nt, "noise_std": 1e-9}
+
+    serial = [SEMSimulation(cfg_for(x)).run_forward_and_adjoint(params(k)) for k, x in enumerate(xs)]
+    with core._PLAN_LOCK:
+        core._PLAN_CACHE.clear()
+
+    def one(task):
+        k, x = task
+        return SEMSimulation(cfg_for(x)).run_forward_and_adjoint(params(k))
+
+    for _ in range(2):
+        with ThreadPoolExecutor(max_workers=3) as ex:
+            threaded = list(ex.map(one, enumerate(xs)))
+        for s, t in zip(serial, threaded):
+            assert s["loglik"] == t["loglik"]
+            np.testing.assert_array_equal(s["grad_wrt_ctrl"], t["grad_wrt_ctrl"])
+            np.testing.assert_array_equal(s["clean_data"], t["clean_data"])
