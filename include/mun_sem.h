@@ -99,7 +99,11 @@ typedef struct {
   int32_t graph_chunk;        /* ticks per captured CUDA graph; 0 = plain launches    */
   int32_t kernel;             /* 0 auto, 1 tile kernel (one CTA per element tile),
                                  2 strip kernel (one CTA per full-height strip, TMA-
-                                 staged element-row bands); auto picks strips when the
+                                 staged element-row bands), 3 persistent tile kernel
+                                 (the tile kernel's ticks in one cooperative launch with
+                                 a grid barrier between ticks, for one-order groups
+                                 whose tiles are all resident at once; otherwise the
+                                 tile kernel per tick); auto picks strips when the
                                  batch has at least one strip per SM                   */
   int32_t strip_bands;        /* strip kernel: element rows per CTA; 0 = automatic
                                  (full-height strips when the batch's strips give 2
@@ -142,7 +146,7 @@ int64_t sem_batch_last_ticks(const sem_batch_t* batch);
  * around each group's tick launches; set-up and output kernels excluded), in ms.
  * Waits for those events. */
 int sem_batch_last_tick_ms(const sem_batch_t* batch, double* ms_out);
-/* kernel variant used by the last sem_run: 1 tile, 2 strip */
+/* kernel variant used by the last sem_run: 1 tile, 2 strip, 3 persistent tile */
 int32_t sem_batch_last_kernel(const sem_batch_t* batch);
 
 /* Single-solve conveniences (plain path): forward with receivers in the run()

@@ -243,42 +243,32 @@ __device__ __forceinline__ void advance_node(bool adj, bool damp, float b, float
 // ----------------------------------------------------------------------------
 // tile kernel: one CTA per tile of elements (used for small batches)
 // ----------------------------------------------------------------------------
-template <int N>
-__global__ void __launch_bounds__(256) sem_tick_kernel(const SolveDev* __restrict__ solves,
-                                                       const int* __restrict__ cta_solve,
-                                                       const int* __restrict__ tick_ptr,
-                                                       int tex, int tez, int tick_arg) {
-  constexpr int NP = N + 1;
-  extern __shared__ float smem[];
-  __shared__ SolveDev S;
-  __shared__ int s_act, s_t, s_seg;
-  grid_dep_launch();
+// Loads of data that other CTAs of the same launch may have written: in the persistent
+// kernel (one launch for every tick, grid barrier between ticks) they bypass L1, which
+// is not coherent across SMs; the per-tick kernels read through the read-only path.
+template <bool COH>
+__device__ __forceinline__ float ld_xf(const float* p) {
+  if constexpr (COH) return __ldcg(p); else return __ldg(p);
+}
+template <bool COH>
+__device__ __forceinline__ double ld_xd(const double* p) {
+  if constexpr (COH) return __ldcg(p); else return *p;
+}
 
-  const int sid = cta_solve[blockIdx.x];
-  {
-    static_assert(sizeof(SolveDev) % 8 == 0, "descriptor is copied as 8-byte words");
-    const unsigned long long* src = reinterpret_cast<const unsigned long long*>(solves + sid);
-    unsigned long long* dst = reinterpret_cast<unsigned long long*>(&S);
-    for (int i = threadIdx.x; i < (int)(sizeof(SolveDev) / 8); i += blockDim.x) dst[i] = src[i];
-  }
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    int act, t, seg;
-    decode(S, (tick_ptr ? *tick_ptr : tick_arg) - S.start_tick, act, t, seg);
-    s_act = act; s_t = t; s_seg = seg;
-  }
-  __syncthreads();
-  grid_dep_wait();  // the previous tick's fields are complete from here on
-  const int act = s_act;
-  if (act == A_NONE) return;
-  const int t = s_t, seg = s_seg;
+// One tick of one element tile (act != A_NONE), shared by the per-tick tile kernel and
+// the persistent kernel (COH: cross-CTA data read coherently).
+template <int N, bool COH>
+__device__ __forceinline__ void tile_tick(const SolveDev& S, const int act, const int t,
+                                          const int seg, const int tex, const int tez,
+                                          float* smem) {
+  constexpr int NP = N + 1;
   const bool adj = (act == A_ADJ);
   if (act == A_SCALE) {
     // one CTA per solve picks the power of two that brings max|r| to ~1, so the
     // float32 adjoint field and the sensitivity products stay far from underflow
     if (blockIdx.x == S.tile_base && threadIdx.x == 0) {
       double m = 0.0;
-      for (int r = 0; r < S.nrec; ++r) m = fmax(m, S.rmax[r]);
+      for (int r = 0; r < S.nrec; ++r) m = fmax(m, ld_xd<COH>(S.rmax + r));
       *S.adj_scale = (m > 0.0 && isfinite(m)) ? ldexp(1.0, -ilogb(m)) : 1.0;
     }
     return;
@@ -336,31 +326,58 @@ __global__ void __launch_bounds__(256) sem_tick_kernel(const SolveDev* __restric
     fwdu = S.ring + (long long)(t + 1 - seg * S.k) * S.fstride;
   }
 
-  // ---------------- stage operators and the haloed tile
+  // ---------------- this thread's first owned node: its own inputs are loaded before the
+  // tile is staged, so their latency overlaps the staging (small tiles are latency-bound)
+  const int w0 = threadIdx.x;
+  const bool pre = (act != A_FINAL) && w0 < nro * nco;
+  float p_v = 0.f, p_ix = 0.f, p_Rx = 0.f, p_dx = 0.f, p_iz = 0.f, p_Rz = 0.f, p_dz = 0.f;
+  double p_g = 0.0;
+  if (pre) {
+    const int gx = gxo0 + w0 % nco, gz = gzo0 + w0 / nco;
+    const long long g0 = (long long)gz * S.pitch + gx;
+    p_v = vin[g0];
+    p_ix = __ldg(S.tx + gx); p_Rx = __ldg(S.tx + S.nxg + gx); p_dx = __ldg(S.tx + 2 * S.nxg + gx);
+    p_iz = __ldg(S.tz + gz); p_Rz = __ldg(S.tz + S.nzg + gz); p_dz = __ldg(S.tz + 2 * S.nzg + gz);
+    if (adj && t >= S.it0 && t < S.it1) p_g = S.grad[g0];
+  }
+  // the same for the misfit terms of each warp's first receiver (forward ticks)
+  const int rec_m = t - ((S.flags & F_SHIFT) ? 1 : 0);
+  const bool rec_tick = (act == A_FWD || act == A_FINAL) && rec_m >= 0 && rec_m < S.nt;
+  const bool mis_tick = rec_tick && (S.flags & F_MISFIT) && rec_m >= S.it0 && rec_m < S.it1 &&
+                        ((rec_m - S.it0) % S.decim) == 0;
+  double p_y = 0.0, p_mis = 0.0, p_rmax = 0.0;
+  if (mis_tick && lane == 0 && warp < S.rec_tile_off[lt + 1] - S.rec_tile_off[lt]) {
+    const int r = S.rec_tile_ids[S.rec_tile_off[lt] + warp];
+    p_y = S.yobs[(long long)((rec_m - S.it0) / S.decim) * S.nrec + r];
+    p_mis = S.misfit[r];
+    p_rmax = S.rmax[r];
+  }
+
+  // ---------------- stage operators and the haloed tile (one (row, column) item per
+  // thread and pass: a small tile's halo region takes a single pass)
   for (int i = threadIdx.x; i < NP * NP; i += nthr) sD[i] = S.D[i];
   for (int i = threadIdx.x; i < NP; i += nthr) sB[i] = S.beta[i];
   {
     const int r0 = max(gzs, 0), r1 = min(gzs + SH, S.nzg);
     const int c0 = max(gxs, 0), c1 = min(gxs + (ex1 - ex0 + 2) * N + 1, S.nxg);
     const bool need_c = (act != A_FINAL);
-    for (int r = r0 + warp; r < r1; r += nwarps) {
-      const long long grow = (long long)r * S.pitch;
-      float* du = su + (r - gzs) * SW - gxs;
-      float* dc = sc + (r - gzs) * SW - gxs;
-      float* dw = sw + (r - gzs) * SW - gxs;
-      for (int c = c0 + lane; c < c1; c += 32) {
-        du[c] = __ldg(cur + grow + c);
-        if (need_c) dc[c] = __ldg(S.c2 + grow + c);
-        if (adj) dw[c] = __ldg(fwdu + grow + c);
-      }
+    const int ncol = c1 - c0, tot = ncol * (r1 - r0);
+#pragma unroll 2
+    for (int i = threadIdx.x; i < tot; i += nthr) {
+      const int rr = i / ncol, r = r0 + rr, c = c0 + (i - rr * ncol);
+      const long long gi = (long long)r * S.pitch + c;
+      const int si = (r - gzs) * SW + (c - gxs);
+      su[si] = ld_xf<COH>(cur + gi);
+      if (need_c) sc[si] = __ldg(S.c2 + gi);
+      if (adj) sw[si] = ld_xf<COH>(fwdu + gi);
     }
   }
   __syncthreads();
 
   // ---------------- receivers: record R b_t (forward sweep only)
   if (act == A_FWD || act == A_FINAL) {
-    const int m = t - ((S.flags & F_SHIFT) ? 1 : 0);
-    if (m >= 0 && m < S.nt) {
+    const int m = rec_m;
+    if (rec_tick) {
       const int off = S.rec_tile_off[lt], cnt = S.rec_tile_off[lt + 1] - off;
       for (int q = warp; q < cnt; q += nwarps) {
         const int r = S.rec_tile_ids[off + q];
@@ -375,10 +392,12 @@ __global__ void __launch_bounds__(256) sem_tick_kernel(const SolveDev* __restric
         for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
         if (lane == 0) {
           S.rec_out[(long long)m * S.nrec + r] = acc;
-          if ((S.flags & F_MISFIT) && m >= S.it0 && m < S.it1 && ((m - S.it0) % S.decim) == 0) {
-            const double res = (double)acc - S.yobs[(long long)((m - S.it0) / S.decim) * S.nrec + r];
-            misfit_add(S.misfit + r, res);
-            S.rmax[r] = fmax(S.rmax[r], fabs(res));
+          if (mis_tick) {
+            const bool first = (q == warp);
+            const double res =
+                (double)acc - (first ? p_y : S.yobs[(long long)((m - S.it0) / S.decim) * S.nrec + r]);
+            S.misfit[r] = __dadd_rn(first ? p_mis : S.misfit[r], __dmul_rn(res, res));
+            S.rmax[r] = fmax(first ? p_rmax : S.rmax[r], fabs(res));
           }
         }
       }
@@ -396,12 +415,12 @@ __global__ void __launch_bounds__(256) sem_tick_kernel(const SolveDev* __restric
     have_inj = in_win && cnt > 0;
     if (have_inj) {
       float* sres = sacc + nrop_max * ncop_max;  // cnt <= kMaxInj floats
-      const double ascale = *S.adj_scale;
+      const double ascale = ld_xd<COH>(S.adj_scale);
       const long long yrow = (long long)((t - S.it0) / S.decim) * S.nrec;
       for (int i = threadIdx.x; i < nro * nco; i += nthr) sacc[i] = 0.f;
       for (int q = threadIdx.x; q < cnt; q += nthr) {
         const int r = S.inj_tile_ids[off + q];
-        const double res = (double)S.rec_out[(long long)t * S.nrec + r] - S.yobs[yrow + r];
+        const double res = (double)ld_xf<COH>(S.rec_out + (long long)t * S.nrec + r) - S.yobs[yrow + r];
         sres[q] = (float)(res * ascale);
       }
       __syncthreads();
@@ -540,18 +559,20 @@ __global__ void __launch_bounds__(256) sem_tick_kernel(const SolveDev* __restric
         if (adj) SZ = __fadd_rn(SZ, zs[o]);
       }
     }
-    const float ixv = __ldg(S.tx + gx), Rxv = __ldg(S.tx + S.nxg + gx);
-    const float izv = __ldg(S.tz + gz), Rzv = __ldg(S.tz + S.nzg + gz);
-    const float dxv = __ldg(S.tx + 2 * S.nxg + gx), dzv = __ldg(S.tz + 2 * S.nzg + gz);
+    const bool first = (w == w0);
+    const float ixv = first ? p_ix : __ldg(S.tx + gx), Rxv = first ? p_Rx : __ldg(S.tx + S.nxg + gx);
+    const float izv = first ? p_iz : __ldg(S.tz + gz), Rzv = first ? p_Rz : __ldg(S.tz + S.nzg + gz);
+    const float dxv = first ? p_dx : __ldg(S.tx + 2 * S.nxg + gx);
+    const float dzv = first ? p_dz : __ldg(S.tz + 2 * S.nzg + gz);
     const long long g = (long long)gz * S.pitch + gx;
     const float b = su[(gz - gzs) * SW + (gx - gxs)];
-    const float v = vin[g];
+    const float v = first ? p_v : vin[g];
     float extra = 0.f;
     if (!adj) {
       if (gx == S.src_gx && gz == S.src_gz) extra = S.src_term[t];
     } else {
       extra = have_inj ? sacc[r * nco + cc] : 0.f;
-      if (grad_on) S.grad[g] += sens_increment(Rzv, SX, Rxv, SZ);
+      if (grad_on) S.grad[g] = (first ? p_g : S.grad[g]) + sens_increment(Rzv, SX, Rxv, SZ);
     }
     float res, vres;
     advance_node(adj, damp, b, v, X, Z, ixv, Rxv, dxv, izv, Rzv, dzv, extra, res, vres);
@@ -560,6 +581,36 @@ __global__ void __launch_bounds__(256) sem_tick_kernel(const SolveDev* __restric
     bad |= !isfinite(res);
   }
   if (__any_sync(0xffffffffu, bad) && lane == 0) atomicOr(S.status, SEM_ERR_NONFINITE);
+}
+
+template <int N>
+__global__ void __launch_bounds__(256) sem_tick_kernel(const SolveDev* __restrict__ solves,
+                                                       const int* __restrict__ cta_solve,
+                                                       const int* __restrict__ tick_ptr,
+                                                       int tex, int tez, int tick_arg) {
+  extern __shared__ float smem[];
+  __shared__ SolveDev S;
+  __shared__ int s_act, s_t, s_seg;
+  grid_dep_launch();
+
+  const int sid = cta_solve[blockIdx.x];
+  {
+    static_assert(sizeof(SolveDev) % 8 == 0, "descriptor is copied as 8-byte words");
+    const unsigned long long* src = reinterpret_cast<const unsigned long long*>(solves + sid);
+    unsigned long long* dst = reinterpret_cast<unsigned long long*>(&S);
+    for (int i = threadIdx.x; i < (int)(sizeof(SolveDev) / 8); i += blockDim.x) dst[i] = src[i];
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int act, t, seg;
+    decode(S, (tick_ptr ? *tick_ptr : tick_arg) - S.start_tick, act, t, seg);
+    s_act = act; s_t = t; s_seg = seg;
+  }
+  __syncthreads();
+  grid_dep_wait();  // the previous tick's fields are complete from here on
+  const int act = s_act;
+  if (act == A_NONE) return;
+  tile_tick<N, false>(S, act, s_t, s_seg, tex, tez, smem);
 }
 
 // ----------------------------------------------------------------------------
@@ -1199,6 +1250,72 @@ __global__ void __launch_bounds__(kStripCols, (N <= 4) ? SEM_STRIP_MIN_BLOCKS : 
     strip_tick<N, false>(S, act, t, seg, smem, &s_abort);
 }
 
+// ----------------------------------------------------------------------------
+// persistent tile kernel: one cooperative launch runs the whole tick program of a
+// latency-bound group (small meshes, one solve at a time), with a grid barrier between
+// ticks instead of a kernel boundary
+// ----------------------------------------------------------------------------
+__device__ __forceinline__ unsigned long long ld_acquire_u64(const unsigned long long* p) {
+  unsigned long long v;
+  asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+  return v;
+}
+// Arrive at and wait on the grid barrier: `count` only grows (target = ticks done x CTAs),
+// thread 0 releases the CTA's writes (fence, then the arrival) and polls with acquire
+// loads.  Gives up after kWaitNs and returns false (every CTA is resident: cooperative
+// launch, so a late CTA is late, not absent).
+__device__ __forceinline__ bool grid_barrier(unsigned long long* count, unsigned long long target,
+                                             int* s_flag) {
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    atomicAdd(count, 1ull);
+    int ok = 1;
+    if (ld_acquire_u64(count) < target) {
+      const long long t0 = global_ns();
+      while (ld_acquire_u64(count) < target)
+        if (global_ns() - t0 > kWaitNs) { ok = 0; break; }
+    }
+    *s_flag = ok;
+  }
+  __syncthreads();
+  return *s_flag != 0;
+}
+
+template <int N>
+__global__ void __launch_bounds__(256) sem_persist_kernel(const SolveDev* __restrict__ solves,
+                                                          const int* __restrict__ cta_solve,
+                                                          int tick0, int tick1, int tex, int tez,
+                                                          unsigned long long* __restrict__ bar) {
+  extern __shared__ float smem[];
+  __shared__ SolveDev S;
+  __shared__ int s_act, s_t, s_seg, s_ok;
+  const int sid = cta_solve[blockIdx.x];
+  {
+    const unsigned long long* src = reinterpret_cast<const unsigned long long*>(solves + sid);
+    unsigned long long* dst = reinterpret_cast<unsigned long long*>(&S);
+    for (int i = threadIdx.x; i < (int)(sizeof(SolveDev) / 8); i += blockDim.x) dst[i] = src[i];
+  }
+  unsigned long long target = 0;
+  for (int tick = tick0; tick < tick1; ++tick) {
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      int act, t, seg;
+      decode(S, tick - S.start_tick, act, t, seg);
+      s_act = act; s_t = t; s_seg = seg;
+    }
+    __syncthreads();
+    const int act = s_act;
+    if (act != A_NONE) tile_tick<N, true>(S, act, s_t, s_seg, tex, tez, smem);
+    if (tick + 1 == tick1) break;
+    target += gridDim.x;
+    if (!grid_barrier(bar, target, &s_ok)) {
+      if (threadIdx.x == 0) atomicOr(S.status, SEM_ERR_TIMEOUT);
+      return;
+    }
+  }
+}
+
 __global__ void tick_advance_kernel(int* tick) { *tick += 1; }
 
 // c (float64, reference order) -> c^2 (float32, pitched grid)
@@ -1523,6 +1640,20 @@ KernelFn kernel_for(int N) {
     case 5: return sem_tick_kernel<5>;
     case 6: return sem_tick_kernel<6>;
     case 7: return sem_tick_kernel<7>;
+  }
+  return nullptr;
+}
+
+typedef void (*PersistFn)(const SolveDev*, const int*, int, int, int, int, unsigned long long*);
+PersistFn persist_kernel_for(int N) {
+  switch (N) {
+    case 1: return sem_persist_kernel<1>;
+    case 2: return sem_persist_kernel<2>;
+    case 3: return sem_persist_kernel<3>;
+    case 4: return sem_persist_kernel<4>;
+    case 5: return sem_persist_kernel<5>;
+    case 6: return sem_persist_kernel<6>;
+    case 7: return sem_persist_kernel<7>;
   }
   return nullptr;
 }
@@ -1937,8 +2068,38 @@ static int run_group(sem_batch_t* b, const sem_solve_t* solves, int32_t n,
   cudaEvent_t ev_begin = b->tick_ev[b->tick_ev_used], ev_end = b->tick_ev[b->tick_ev_used + 1];
   CUDA_TRY(cudaEventRecord(ev_begin, stream));
   const long long per_tick = (long long)launches.size() + 1;  // graphed: + counter kernel
-  bool graphed = false;
-  if (cfg.graph_chunk > 0 && stream != nullptr && stream != cudaStreamLegacy &&
+  bool graphed = false, persisted = false;
+  // persistent kernel: one cooperative launch for the whole tick program, when the group
+  // has one polynomial order and all its CTAs are resident at once (else per-tick launches)
+  if (cfg.kernel == 3 && launches.size() == 1) {
+    const Launch& Lc = launches[0];
+    PersistFn pf = persist_kernel_for(Lc.N);
+    int nb = 0;
+    if (pf && raise_smem_limit((const void*)pf, Lc.smem) == cudaSuccess &&
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, pf, cfg.threads, Lc.smem) == cudaSuccess &&
+        (long long)nb * sms >= Lc.ncta) {
+      unsigned long long* bar =
+          reinterpret_cast<unsigned long long*>(reinterpret_cast<char*>(b->d_tick) + 128);
+      CUDA_TRY(cudaMemsetAsync(bar, 0, sizeof(unsigned long long), stream));
+      cudaLaunchConfig_t lc = {};
+      lc.gridDim = dim3((unsigned)Lc.ncta);
+      lc.blockDim = dim3(cfg.threads);
+      lc.dynamicSmemBytes = Lc.smem;
+      lc.stream = stream;
+      cudaLaunchAttribute at[1];
+      at[0].id = cudaLaunchAttributeCooperative;
+      at[0].val.cooperative = 1;
+      lc.attrs = at;
+      lc.numAttrs = 1;
+      CUDA_TRY(cudaLaunchKernelEx(&lc, pf, gdesc[0], (const int*)(b->d_cta + Lc.cta0), 0, max_prog,
+                                  cfg.tile_ex, cfg.tile_ez, bar));
+      b->last_launches += 1;
+      persisted = true;
+    }
+    cudaGetLastError();  // a refused occupancy query leaves the per-tick path
+  }
+  b->last_kernel = persisted ? 3 : b->last_kernel;
+  if (!persisted && cfg.graph_chunk > 0 && stream != nullptr && stream != cudaStreamLegacy &&
       stream != cudaStreamPerThread) {
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
@@ -1957,7 +2118,7 @@ static int run_group(sem_batch_t* b, const sem_solve_t* solves, int32_t n,
     }
     cudaGetLastError();  // clear a failed capture
   }
-  if (!graphed) {
+  if (!graphed && !persisted) {
     for (int tick = 0; tick < max_prog; ++tick) CUDA_TRY(launch_tick_pdl(tick));
     b->last_launches += (long long)max_prog * (long long)launches.size();
   }
@@ -2111,7 +2272,8 @@ int sem_run(sem_batch_t* b, const sem_solve_t* solves, int32_t n, const sem_laun
   sem_launch_cfg_t cfg = cfg_in ? *cfg_in : sem_launch_cfg_t{0, 0, 256, 0, 0, 0, 0};
   if (!(cfg.tile_ex == 0 && cfg.tile_ez == 0) && (cfg.tile_ex < 1 || cfg.tile_ez < 1))
     return fail(SEM_ERR_ARG, "tile size must be >= 1 (or 0 x 0: automatic)");
-  if (cfg.kernel < 0 || cfg.kernel > 2) return fail(SEM_ERR_ARG, "kernel must be 0 (auto), 1 (tile), 2 (strip)");
+  if (cfg.kernel < 0 || cfg.kernel > 3)
+    return fail(SEM_ERR_ARG, "kernel must be 0 (auto), 1 (tile), 2 (strip), 3 (persistent tile)");
   if (cfg.threads < 32 || cfg.threads > 256 || cfg.threads % 32) cfg.threads = 256;
   if (cfg.memory_budget < 0) return fail(SEM_ERR_ARG, "memory_budget must be >= 0");
   if (cfg.strip_bands < 0) return fail(SEM_ERR_ARG, "strip_bands must be >= 0");
