@@ -57,6 +57,7 @@ namespace {
 
 constexpr int kMaxN = 7;       // supported polynomial orders 1..7
 constexpr int kMaxInj = 1024;  // receivers whose element touches one tile (checked on the host)
+constexpr int kInjCache = 8;   // adjoint-source receivers of a tile staged before the tile
 
 // ----------------------------------------------------------------------------
 // error plumbing
@@ -196,6 +197,7 @@ __host__ __device__ inline long long smem_floats(int N, int tex, int tez, bool a
   const long long xseg = (long long)(tex + 1) * NP * nro, zseg = (long long)(tez + 1) * NP * nco;
   long long f = 96 + 2 * reg + xseg + zseg;  // D, beta | u, c2 | K_x, K_z
   if (adj) f += reg + xseg + zseg + nro * nco + kMaxInj;  // forward field | S_x, S_z | injection
+  if (adj) f += kInjCache * (3 + 64);  // first receivers: id, element base, weights
   return f;
 }
 
@@ -345,12 +347,50 @@ __device__ __forceinline__ void tile_tick(const SolveDev& S, const int act, cons
   const bool rec_tick = (act == A_FWD || act == A_FINAL) && rec_m >= 0 && rec_m < S.nt;
   const bool mis_tick = rec_tick && (S.flags & F_MISFIT) && rec_m >= S.it0 && rec_m < S.it1 &&
                         ((rec_m - S.it0) % S.decim) == 0;
+  // and of this thread's first adjoint-source receiver (adjoint ticks in the window)
+  const bool in_win = adj && t >= S.it0 && t < S.it1 && ((t - S.it0) % S.decim) == 0;
+  float p_res = 0.f;
+  if (in_win && (int)threadIdx.x < S.inj_tile_off[lt + 1] - S.inj_tile_off[lt]) {
+    const int r = S.inj_tile_ids[S.inj_tile_off[lt] + threadIdx.x];
+    const long long yrow = (long long)((t - S.it0) / S.decim) * S.nrec;
+    const double res = (double)ld_xf<COH>(S.rec_out + (long long)t * S.nrec + r) - S.yobs[yrow + r];
+    p_res = (float)(res * ld_xd<COH>(S.adj_scale));
+  }
+  // the first receivers' ids, element bases and weights: a warp's first read-out receiver
+  // in registers, the first kInjCache adjoint-source receivers in shared memory
+  int* const s_ir = reinterpret_cast<int*>(sacc + nrop_max * ncop_max + kMaxInj);
+  int* const s_ibx = s_ir + kInjCache;
+  int* const s_ibz = s_ibx + kInjCache;
+  float* const s_iw = reinterpret_cast<float*>(s_ibz + kInjCache);
+  if (in_win) {
+    const int ioff = S.inj_tile_off[lt], icnt = min(S.inj_tile_off[lt + 1] - ioff, kInjCache);
+    if ((int)threadIdx.x < icnt) {
+      const int r = S.inj_tile_ids[ioff + threadIdx.x];
+      s_ir[threadIdx.x] = r;
+      s_ibx[threadIdx.x] = S.rec_base[2 * r];
+      s_ibz[threadIdx.x] = S.rec_base[2 * r + 1];
+    }
+    for (int k = threadIdx.x; k < icnt * NP * NP; k += nthr) {
+      const int q = k / (NP * NP), e = k - q * (NP * NP);
+      s_iw[q * 64 + e] = S.rec_w[(long long)S.inj_tile_ids[ioff + q] * NP * NP + e];
+    }
+  }
+  const bool rec_first = rec_tick && warp < S.rec_tile_off[lt + 1] - S.rec_tile_off[lt];
+  int p_r = 0, p_bx = 0, p_bz = 0;
+  float p_w0 = 0.f, p_w1 = 0.f;
+  if (rec_first) {
+    p_r = S.rec_tile_ids[S.rec_tile_off[lt] + warp];
+    p_bx = S.rec_base[2 * p_r];
+    p_bz = S.rec_base[2 * p_r + 1];
+    const float* wr = S.rec_w + (long long)p_r * NP * NP;
+    if (lane < NP * NP) p_w0 = wr[lane];
+    if (lane + 32 < NP * NP) p_w1 = wr[lane + 32];
+  }
   double p_y = 0.0, p_mis = 0.0, p_rmax = 0.0;
-  if (mis_tick && lane == 0 && warp < S.rec_tile_off[lt + 1] - S.rec_tile_off[lt]) {
-    const int r = S.rec_tile_ids[S.rec_tile_off[lt] + warp];
-    p_y = S.yobs[(long long)((rec_m - S.it0) / S.decim) * S.nrec + r];
-    p_mis = S.misfit[r];
-    p_rmax = S.rmax[r];
+  if (mis_tick && lane == 0 && rec_first) {
+    p_y = S.yobs[(long long)((rec_m - S.it0) / S.decim) * S.nrec + p_r];
+    p_mis = S.misfit[p_r];
+    p_rmax = S.rmax[p_r];
   }
 
   // ---------------- stage operators and the haloed tile (one (row, column) item per
@@ -380,13 +420,15 @@ __device__ __forceinline__ void tile_tick(const SolveDev& S, const int act, cons
     if (rec_tick) {
       const int off = S.rec_tile_off[lt], cnt = S.rec_tile_off[lt + 1] - off;
       for (int q = warp; q < cnt; q += nwarps) {
-        const int r = S.rec_tile_ids[off + q];
-        const int bx = S.rec_base[2 * r], bz = S.rec_base[2 * r + 1];
+        const bool pf = (q == warp);
+        const int r = pf ? p_r : S.rec_tile_ids[off + q];
+        const int bx = pf ? p_bx : S.rec_base[2 * r], bz = pf ? p_bz : S.rec_base[2 * r + 1];
         const float* wr = S.rec_w + (long long)r * NP * NP;
         float acc = 0.f;
         for (int e = lane; e < NP * NP; e += 32) {
           const int j = e / NP, i = e - j * NP;
-          acc = fmaf(wr[e], su[(bz + j - gzs) * SW + (bx + i - gxs)], acc);
+          const float we = !pf ? wr[e] : (e < 32 ? p_w0 : p_w1);
+          acc = fmaf(we, su[(bz + j - gzs) * SW + (bx + i - gxs)], acc);
         }
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
@@ -408,7 +450,6 @@ __device__ __forceinline__ void tile_tick(const SolveDev& S, const int act, cons
   // ---------------- adjoint source R^T r_it: residuals of this tile's receivers are
   // formed in parallel, then one warp adds them node by node in receiver order
   // (deterministic; receivers of one element never race)
-  const bool in_win = adj && t >= S.it0 && t < S.it1 && ((t - S.it0) % S.decim) == 0;
   bool have_inj = false;
   if (adj) {
     const int off = S.inj_tile_off[lt], cnt = S.inj_tile_off[lt + 1] - off;
@@ -419,6 +460,10 @@ __device__ __forceinline__ void tile_tick(const SolveDev& S, const int act, cons
       const long long yrow = (long long)((t - S.it0) / S.decim) * S.nrec;
       for (int i = threadIdx.x; i < nro * nco; i += nthr) sacc[i] = 0.f;
       for (int q = threadIdx.x; q < cnt; q += nthr) {
+        if (q == (int)threadIdx.x) {
+          sres[q] = p_res;
+          continue;
+        }
         const int r = S.inj_tile_ids[off + q];
         const double res = (double)ld_xf<COH>(S.rec_out + (long long)t * S.nrec + r) - S.yobs[yrow + r];
         sres[q] = (float)(res * ascale);
@@ -426,16 +471,19 @@ __device__ __forceinline__ void tile_tick(const SolveDev& S, const int act, cons
       __syncthreads();
       if (warp == 0) {
         for (int q = 0; q < cnt; ++q) {
-          const int r = S.inj_tile_ids[off + q];
+          const bool cached = q < kInjCache;
+          const int r = cached ? s_ir[q] : S.inj_tile_ids[off + q];
           const float rs = sres[q];
-          const int bx = S.rec_base[2 * r], bz = S.rec_base[2 * r + 1];
+          const int bx = cached ? s_ibx[q] : S.rec_base[2 * r];
+          const int bz = cached ? s_ibz[q] : S.rec_base[2 * r + 1];
           const float* wr = S.rec_w + (long long)r * NP * NP;
           for (int e = lane; e < NP * NP; e += 32) {
             const int j = e / NP, i = e - j * NP;
             const int gx = bx + i, gz = bz + j;
+            const float we = cached ? s_iw[q * 64 + e] : wr[e];
             if (gx >= gxo0 && gx < gxo1 && gz >= gzo0 && gz < gzo1)
               sacc[(gz - gzo0) * nco + (gx - gxo0)] =
-                  __fmaf_rn(wr[e], rs, sacc[(gz - gzo0) * nco + (gx - gxo0)]);
+                  __fmaf_rn(we, rs, sacc[(gz - gzo0) * nco + (gx - gxo0)]);
           }
           __syncwarp();
         }
