@@ -686,8 +686,10 @@ __global__ void __launch_bounds__(256) sem_tick_kernel(const SolveDev* __restric
 #ifndef SEM_STRIP_MIN_BLOCKS
 #define SEM_STRIP_MIN_BLOCKS 4
 #endif
+// suspend-time hint of the ring waits (ns); 0 = the instruction's own short suspend window,
+// measured 1-2 % faster per tick than a 20 us hint (the wait stays bounded either way)
 #ifndef SEM_WAIT_HINT_NS
-#define SEM_WAIT_HINT_NS 20000
+#define SEM_WAIT_HINT_NS 0
 #endif
 constexpr int kStripCols = 128;
 constexpr int kStages = 3;                   // ring slots of forward/replay ticks
