@@ -37,6 +37,7 @@
 // function, so a fixed launch sequence (capturable in a CUDA graph) drives any mix
 // of solves with different nt, checkpoint interval and polynomial order.
 
+#include <cuda.h>  // CUtensorMap and its encoder's types (the encoder is fetched at run time)
 #include <cuda_runtime.h>
 #include <stdint.h>
 #include <stdio.h>
@@ -124,6 +125,10 @@ struct SolveDev {
   double* rmax;       // [nrec] max |residual| (sizes the adjoint source)
   double* adj_scale;  // [1] power-of-two scale applied to the adjoint source
   int* status;
+  // strip kernel: the workspace base (its float fields start at multiples of fstride) and
+  // the tensor map of the band loads over it (device memory; null for the tile kernel)
+  const float* ws;
+  const void* tmap;
 };
 
 __device__ __forceinline__ void decode(const SolveDev& s, int sig, int& act, int& t, int& seg) {
@@ -666,7 +671,7 @@ __global__ void __launch_bounds__(256) sem_tick_kernel(const SolveDev* __restric
 //
 // Columns: N left-halo columns, the strip's owned columns and the shared column on its
 // right.  The CTA sweeps the strip one element row ("band", N+1 grid rows) at a time;
-// the band of every field the step reads is staged by TMA bulk copies (cp.async.bulk +
+// the band of every field the step reads is staged by TMA tensor copies (cp.async.bulk.tensor +
 // mbarrier) into a ring of slots, issued as many bands ahead as there are slots (3 for
 // forward/replay ticks, 2 for the larger adjoint bands so that four CTAs fit per SM).
 // Work per band: one thread per (band row, element segment) for the x-lines, one thread
@@ -756,19 +761,29 @@ __device__ __forceinline__ bool mbar_wait(unsigned long long* bar, unsigned pari
     if (global_ns() - t0 > kWaitNs) return false;
   return true;
 }
-__device__ __forceinline__ void bulk_load(void* dst, const void* src, unsigned bytes,
-                                          unsigned long long* bar) {
+
+// floats of one staged field of a band (N+1 rows of strip_bw columns), rounded up so that
+// every field's block starts 128-byte aligned (tensor-copy destinations)
+__host__ __device__ inline int strip_field_floats(int N) { return ((N + 1) * strip_bw(N) + 31) & ~31; }
+// one box of a 3-D tiled tensor map (column x, row y, field slot z) into shared memory;
+// x is a multiple of 4 floats (16 bytes), negative or past the edge reads zeros
+__device__ __forceinline__ void tensor_load_3d(void* dst, const void* tmap, int x, int y, int z,
+                                               unsigned long long* bar) {
   asm volatile(
-      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-          smem_addr(dst)),
-      "l"(src), "r"(bytes), "r"(smem_addr(bar))
+      "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];"
+      ::"r"(smem_addr(dst)), "l"(tmap), "r"(x), "r"(y), "r"(z), "r"(smem_addr(bar))
       : "memory");
+}
+// the map was written by the host through the generic proxy: make it visible to the
+// tensor-copy proxy before its first use in this launch
+__device__ __forceinline__ void tensormap_acquire(const void* tmap) {
+  asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"(tmap) : "memory");
 }
 
 __host__ __device__ inline long long strip_stage_floats(int N, bool adj) {
-  const int nfloat = adj ? 4 : 3;  // cur, c2, v (+ forward field)
-  const int ndouble = 0;  // the float64 gradient is loaded by its owner threads, not staged
-  return ((long long)(nfloat + 2 * ndouble) * (N + 1) * strip_bw(N) + 31) & ~31LL;
+  const int nfloat = adj ? 4 : 3;  // cur, c2, v (+ forward field); the float64 gradient is
+                                   // loaded by its owner threads, not staged
+  return (long long)nfloat * strip_field_floats(N);
 }
 // exchange arrays: x-segment results Xs[rows][segments][N+1] (+ sensitivity), z-segment
 // results stay in registers; injection rows and residuals
@@ -853,7 +868,6 @@ __device__ __forceinline__ void strip_tick(const SolveDev& S, const int act, con
   const int so1 = (e1 == nelx) ? nxg : e1 * N;              // owned columns [sx0, so1)
   const int X0 = (sx0 - N) & ~3;                            // 16-byte aligned copy origin
   const int off = (sx0 - N) - X0;                           // smem column of column sx0 - N
-  const int cs = max(X0, 0), ce = min(X0 + BW, pitch);      // copied columns
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int nseg = e1 - e0 + 1;                             // segments e0-1 .. e1-1
   const int seg0 = (e0 == 0) ? 1 : 0;                       // segment -1 does not exist
@@ -902,28 +916,25 @@ __device__ __forceinline__ void strip_tick(const SolveDev& S, const int act, con
   }
   __syncthreads();
 
-  // TMA: element row `ez` of every field into ring slot (ez - ezs) % NST (one warp: lane 0
-  // posts the expected bytes, then each lane issues row copies)
-  // The row copies of a band (field f, row a: nload * NP <= 4 * 8 < NT of them) are spread
-  // over all warps, one per thread at most (copy q = lane * NW + warp, so every warp
-  // issues a few): each thread fixes its copy's slot offset and source once per tick and
-  // adds the band's offset.  A copy may complete before lane 0 of warp 0 posts the
-  // expected bytes: the barrier's pending arrival keeps the phase open until then.
-  const unsigned rowb = (unsigned)(ce - cs) * 4u;
-  const int myq = lane * NW + warp;
-  const bool has_copy = myq < nload * NP;
-  int cp_dst = 0;
-  const float* cp_src = cur;
+  // TMA: element row `ez` of every field into ring slot (ez - ezs) % NST.  One tensor copy
+  // per staged field: the box of BW columns from X0 and N+1 rows from ez * N of the
+  // field's slot in the solve's workspace map (columns outside [0, pitch) read as zeros
+  // and are never used).  Field f is issued by lane 1 of warp f, so the copies are spread
+  // over the warps; thread 0 posts the expected bytes (a copy may complete first: the
+  // barrier's pending arrival keeps the phase open until then).
+  const bool has_copy = lane == 1 && warp < nload;
+  int cp_slot = 0;
   if (has_copy) {
-    const int f = myq / NP, a = myq - f * NP;
-    cp_src = ((f == 0) ? cur : (f == 1) ? c2p : (f == 2) ? vin : fwdu) + (long long)a * pitch + cs;
-    cp_dst = (f * NP + a) * BW + (cs - X0);
+    const float* fp = (warp == 0) ? cur : (warp == 1) ? c2p : (warp == 2) ? vin : fwdu;
+    cp_slot = (int)((fp - S.ws) / S.fstride);
+    tensormap_acquire(S.tmap);
   }
-  const long long band_floats = (long long)N * pitch;
+  constexpr int FBF = ((N + 1) * BW + 31) & ~31;  // floats per staged field block
+  const unsigned band_bytes = (unsigned)(nload * NP * BW) * 4u;
   auto issue = [&](int ez) {
     const int slot = (ez - ezs) % NST;
-    if (warp == 0 && lane == 0) mbar_expect_tx(bars + slot, (unsigned)(nload * NP) * rowb);
-    if (has_copy) bulk_load(stages + slot * stage_f + cp_dst, cp_src + ez * band_floats, rowb, bars + slot);
+    if (tid == 0) mbar_expect_tx(bars + slot, band_bytes);
+    if (has_copy) tensor_load_3d(stages + slot * stage_f + warp * FBF, S.tmap, X0, ez * N, cp_slot, bars + slot);
   };
   for (int r = 0; r < min(NST, nbands); ++r) issue(ezs + r);
 
@@ -983,9 +994,9 @@ __device__ __forceinline__ void strip_tick(const SolveDev& S, const int act, con
     const bool halo = has_halo && rel == 0;
     const float* st = stages + slot * stage_f;
     const float* Bs = st;
-    const float* Cs = st + NP * BW;
-    const float* Vs = st + 2 * NP * BW;
-    const float* Us = st + 3 * NP * BW;
+    const float* Cs = st + FBF;
+    const float* Vs = st + 2 * FBF;
+    const float* Us = st + 3 * FBF;
     float* const Xs = xs0 + (ez & 1) * XSZ;
     float* const SXs = Xs + NP * SEGS * NP;
     float* const tzb = sTz + (ez & 1) * 24;
@@ -1713,6 +1724,43 @@ struct Workspace {
   long long bytes;
 };
 
+// The strip kernel's band loads: one tiled tensor map per solve over its workspace seen as
+// [field slot][row][column] floats (c2, W, V, checkpoints, ring, L and Mu all start at
+// multiples of the field stride), box = strip_bw columns x N+1 rows of one field.
+typedef CUresult (*TensorMapEncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*,
+                                           const cuuint64_t*, const cuuint64_t*, const cuuint32_t*,
+                                           const cuuint32_t*, CUtensorMapInterleave, CUtensorMapSwizzle,
+                                           CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+TensorMapEncodeTiledFn tensor_map_encoder() {
+  static TensorMapEncodeTiledFn fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<TensorMapEncodeTiledFn>(f);
+    cudaGetLastError();
+  });
+  return fn;
+}
+int encode_band_map(CUtensorMap* m, char* ws_base, const sem_plan_s* p, long long nslots) {
+  TensorMapEncodeTiledFn enc = tensor_map_encoder();
+  if (!enc) return fail(SEM_ERR_CUDA, "cuTensorMapEncodeTiled unavailable");
+  const cuuint64_t dims[3] = {(cuuint64_t)p->pitch, (cuuint64_t)p->nzg, (cuuint64_t)nslots};
+  const cuuint64_t strides[2] = {(cuuint64_t)p->pitch * 4, (cuuint64_t)p->fstride * 4};
+  const cuuint32_t box[3] = {(cuuint32_t)strip_bw(p->npol), (cuuint32_t)(p->npol + 1), 1};
+  const cuuint32_t estr[3] = {1, 1, 1};
+  const CUresult r = enc(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, ws_base, dims, strides, box, estr,
+                         CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                         CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS ? SEM_OK : fail(SEM_ERR_CUDA, "tensor map encoding failed");
+}
+// float-field slots of a workspace (everything before the float64 gradient / the misfit)
+long long field_slots(const Workspace& w, const sem_plan_s* p, bool adj) {
+  return (adj ? w.grad : w.misfit) / (p->fstride * 4);
+}
+
 Workspace layout(const sem_plan_s* p, int flags, int k, int* nseg_out) {
   Workspace w{};
   const long long F = p->fstride * 4;  // bytes per float field (multiple of 256)
@@ -1760,6 +1808,9 @@ struct sem_batch_s {
   int tick_ev_used = 0;
   std::vector<SolveDev> h_solves;
   std::vector<int> h_cta;
+  CUtensorMap* d_tmaps = nullptr;       // strip kernel: band-load tensor map of each solve
+  int tmaps_cap = 0;
+  std::vector<CUtensorMap> h_tmaps;
 };
 
 extern "C" {
@@ -1856,7 +1907,7 @@ int sem_batch_destroy(sem_batch_t* b) {
   if (!b) return SEM_OK;
   for (cudaEvent_t e : b->tick_ev) cudaEventDestroy(e);
   cudaFree(b->d_io);
-  cudaFree(b->arena); cudaFree(b->d_tick); cudaFree(b->d_solves); cudaFree(b->d_cta);
+  cudaFree(b->arena); cudaFree(b->d_tick); cudaFree(b->d_solves); cudaFree(b->d_cta); cudaFree(b->d_tmaps);
   delete b;
   return SEM_OK;
 }
@@ -1924,6 +1975,14 @@ static int run_group(sem_batch_t* b, const sem_solve_t* solves, int32_t n,
   std::stable_sort(order.begin(), order.end(),
                    [&](int x, int y) { return solves[x].plan->npol < solves[y].plan->npol; });
   b->h_solves.assign(n, SolveDev{});
+  if (use_strip && n > b->tmaps_cap) {
+    cudaFree(b->d_tmaps);
+    b->d_tmaps = nullptr;
+    b->tmaps_cap = 0;
+    CUDA_TRY(cudaMalloc((void**)&b->d_tmaps, sizeof(CUtensorMap) * n));
+    b->tmaps_cap = n;
+  }
+  if (use_strip) b->h_tmaps.resize(n);
   b->h_cta.clear();
   struct Group { int N; long long cta0, ncta; bool adj; };
   std::vector<Group> groups;
@@ -1978,6 +2037,13 @@ static int run_group(sem_batch_t* b, const sem_solve_t* solves, int32_t n,
     d.rmax = d.misfit + p->nrec;
     d.adj_scale = d.misfit + 2 * p->nrec;
     d.status = (int*)(a + ws[i].status);
+    d.ws = (const float*)a;
+    d.tmap = nullptr;
+    if (use_strip) {
+      rc = encode_band_map(&b->h_tmaps[oi], a, p, field_slots(ws[i], p, s.flags & SEM_F_ADJOINT));
+      if (rc) return rc;
+      d.tmap = b->d_tmaps + oi;
+    }
     for (int c = 0; c < ntiles; ++c) b->h_cta.push_back(oi - 0);
     G.ncta += ntiles;
     max_prog = std::max(max_prog, prog[i]);
@@ -2002,6 +2068,9 @@ static int run_group(sem_batch_t* b, const sem_solve_t* solves, int32_t n,
   }
   CUDA_TRY(cudaMemcpyAsync(b->d_solves, b->h_solves.data(), sizeof(SolveDev) * n,
                            cudaMemcpyHostToDevice, stream));
+  if (use_strip)
+    CUDA_TRY(cudaMemcpyAsync(b->d_tmaps, b->h_tmaps.data(), sizeof(CUtensorMap) * n,
+                             cudaMemcpyHostToDevice, stream));
   CUDA_TRY(cudaMemcpyAsync(b->d_cta, b->h_cta.data(), sizeof(int) * b->h_cta.size(),
                            cudaMemcpyHostToDevice, stream));
 
@@ -2515,6 +2584,8 @@ struct EngineJob {
   long long start = 0, off = -1;
   Workspace ws{};
   cudaEvent_t ev = nullptr;
+  CUtensorMap tmap{};     // strip kernel: band-load map of its workspace (fixed while running)
+  bool has_tmap = false;
 };
 
 struct sem_engine_s {
@@ -2539,6 +2610,9 @@ struct sem_engine_s {
   std::vector<int> h_cta;
   SolveIo* d_io = nullptr;  // [2 * max_solves]: outputs of retiring solves | set-up of admitted
   std::vector<SolveIo> h_io;
+  CUtensorMap* d_tmaps = nullptr;
+  int tmaps_cap = 0;
+  std::vector<CUtensorMap> h_tmaps;
 };
 
 namespace {
@@ -2641,7 +2715,7 @@ int sem_engine_destroy(sem_engine_t* e) {
     if (kv.second->ev) cudaEventDestroy(kv.second->ev);
     delete kv.second;
   }
-  cudaFree(e->arena); cudaFree(e->d_tick); cudaFree(e->d_solves); cudaFree(e->d_cta);
+  cudaFree(e->arena); cudaFree(e->d_tick); cudaFree(e->d_solves); cudaFree(e->d_cta); cudaFree(e->d_tmaps);
   cudaFree(e->d_io);
   delete e;
   return SEM_OK;
@@ -2795,6 +2869,15 @@ int sem_engine_step(sem_engine_t* e, void* stream_v) {
   const int n = (int)order.size();
   e->h_solves.assign(n, SolveDev{});
   e->h_cta.clear();
+  if (use_strip && n > e->tmaps_cap) {
+    cudaFree(e->d_tmaps);
+    e->d_tmaps = nullptr;
+    e->tmaps_cap = 0;
+    const int cap = std::max(n, e->cfg.max_solves);
+    CUDA_TRY(cudaMalloc((void**)&e->d_tmaps, sizeof(CUtensorMap) * cap));
+    e->tmaps_cap = cap;
+  }
+  if (use_strip) e->h_tmaps.resize(n);
   struct Group { int N; long long cta0, ncta; bool adj; int first; };
   std::vector<Group> groups;
   for (int oi = 0; oi < n; ++oi) {
@@ -2844,6 +2927,17 @@ int sem_engine_step(sem_engine_t* e, void* stream_v) {
     d.rmax = d.misfit + p->nrec;
     d.adj_scale = d.misfit + 2 * p->nrec;
     d.status = (int*)(a + j->ws.status);
+    d.ws = (const float*)a;
+    d.tmap = nullptr;
+    if (use_strip) {
+      if (!j->has_tmap) {
+        rc = encode_band_map(&j->tmap, a, p, field_slots(j->ws, p, adj));
+        if (rc) return rc;
+        j->has_tmap = true;
+      }
+      e->h_tmaps[oi] = j->tmap;
+      d.tmap = e->d_tmaps + oi;
+    }
     for (int c = 0; c < ntiles; ++c) e->h_cta.push_back(oi - G.first);
     G.ncta += ntiles;
   }
@@ -2862,6 +2956,9 @@ int sem_engine_step(sem_engine_t* e, void* stream_v) {
   }
   CUDA_TRY(cudaMemcpyAsync(e->d_solves, e->h_solves.data(), sizeof(SolveDev) * n,
                            cudaMemcpyHostToDevice, stream));
+  if (use_strip)
+    CUDA_TRY(cudaMemcpyAsync(e->d_tmaps, e->h_tmaps.data(), sizeof(CUtensorMap) * n,
+                             cudaMemcpyHostToDevice, stream));
   CUDA_TRY(cudaMemcpyAsync(e->d_cta, e->h_cta.data(), sizeof(int) * e->h_cta.size(),
                            cudaMemcpyHostToDevice, stream));
   // ---- ticks: the tick number is passed; launches chain by programmatic dependent launch

@@ -93,13 +93,18 @@ def audit(N, nelx, nelz):
 STAGES, STAGES_ADJ, INJ, HDR, NBUF = 3, 3, 256, 192, 2
 
 
+def field_floats(N):
+    """strip_field_floats: one staged field of a band, rounded to 32 floats (128 bytes)."""
+    return ((N + 1) * bw(N) + 31) & ~31
+
+
 def smem_bytes(N, adj):
     """strip_smem_floats(N, adj) * 4: header, ring slots, exchange buffers, injection.
     The float64 gradient is not staged (owner threads load their rows)."""
     NP, segs = N + 1, ew_max(N) + 1
 
     def stage(a):
-        return ((4 if a else 3) * NP * bw(N) + 31) & ~31
+        return (4 if a else 3) * field_floats(N)
 
     def xch(a):
         f = NBUF * (2 if a else 1) * NP * segs * NP + ((NP * THREADS + INJ) if a else 0)
@@ -215,10 +220,34 @@ def test_strip_chunks_partition_and_ring(nelz, zch):
 
 
 @pytest.mark.parametrize("N", [1, 2, 3, 4, 5, 6, 7])
-def test_ring_copies_one_per_thread(N):
-    # copy q = lane * NW + warp of each band: every (field, row) copy exactly once
-    NP, NW = N + 1, THREADS // 32
-    for nload in (1, 3, 4):
-        qs = [lane * NW + warp for tid in range(THREADS) for warp, lane in [divmod(tid, 32)]]
-        mine = [q for q in qs if q < nload * NP]
-        assert sorted(mine) == list(range(nload * NP))
+def test_band_tensor_copies(N):
+    """One tensor copy per staged field and band: box of bw(N) columns from X0 and N+1 rows
+    from ez*N in the field's slot of the solve's workspace map, issued by lane 1 of warp f."""
+    NP, NW, BW = N + 1, THREADS // 32, bw(N)
+    assert BW <= 256 and NP <= 256 and (BW * 4) % 16 == 0      # box limits, 16-byte inner extent
+    FB = field_floats(N)
+    assert FB >= NP * BW and (FB * 4) % 128 == 0               # field blocks 128-byte aligned
+    for adj in (False, True):
+        nload = 4 if adj else 3
+        assert nload <= NW                                     # one issuing warp per field
+        issuers = [tid for tid in range(THREADS) if tid % 32 == 1 and tid // 32 < nload]
+        assert [t // 32 for t in issuers] == list(range(nload))
+        assert (nload * FB) % 32 == 0                          # ring slots stay aligned
+    for nelx, nelz in ((100, 50), (400, 200), (7, 3), (40, 20)):
+        nxg, nzg = nelx * N + 1, nelz * N + 1
+        pitch = pitch_of(nxg)
+        assert (pitch * 4) % 16 == 0                           # row stride of the map
+        fstride = -(-(pitch * nzg) // 64) * 64                 # floats per field (256-byte multiple)
+        assert (fstride * 4) % 16 == 0                         # slot stride of the map
+        ns, EW = strips_of(nelx, N)
+        for strip in range(ns):
+            X0 = ((strip * EW) * N - N) & ~3
+            assert X0 % 4 == 0 and -BW < X0 < pitch            # x * 4 bytes on a 16-byte boundary
+        for ez in range(nelz):
+            assert 0 <= ez * N and ez * N + N <= nzg - 1       # the band's rows are in the map
+        # workspace slots: c2 | W W | V | ckpt (2 nseg) | ring (k+1) | L L | Mu, then the
+        # float64 gradient; every staged field is slot (ptr - ws) / fstride < slots
+        k, nt = 7, 50
+        nseg = -(-nt // k)
+        slots = 1 + 2 + 1 + 2 * nseg + (k + 1) + 2 + 1
+        assert slots * fstride < 2 ** 40 and slots < 2 ** 32
