@@ -672,8 +672,8 @@ __global__ void __launch_bounds__(256) sem_tick_kernel(const SolveDev* __restric
 // Columns: N left-halo columns, the strip's owned columns and the shared column on its
 // right.  The CTA sweeps the strip one element row ("band", N+1 grid rows) at a time;
 // the band of every field the step reads is staged by TMA tensor copies (cp.async.bulk.tensor +
-// mbarrier) into a ring of slots, issued as many bands ahead as there are slots (3 for
-// forward/replay ticks, 2 for the larger adjoint bands so that four CTAs fit per SM).
+// mbarrier; one box per field from a tiled tensor map over the solve's workspace) into a
+// ring of 3 slots, issued as many bands ahead as there are slots.
 // Work per band: one thread per (band row, element segment) for the x-lines, one thread
 // per owned column for the z-line segment of the band, D and beta in registers; then
 // one thread per owned column combines the segment results and advances the band's
