@@ -700,6 +700,7 @@ constexpr int kStripCols = 128;
 constexpr int kStages = 3;                   // ring slots of forward/replay ticks
 constexpr int kStagesAdj = SEM_STAGES_ADJ;   // ring slots of adjoint ticks (bigger bands)
 constexpr int kStripInj = 256;               // receivers per band of one strip (host-checked)
+constexpr int kMapBands = 8;                 // strip chunks this tall load bands by tensor map
 constexpr long long kWaitNs = 2000000000LL;  // bounded mbarrier waits: 2 s
 // floats ahead of the ring: mbarriers (64), D (64), beta (16), the band's z-table rows (48)
 constexpr int kStripHdr = 192;
@@ -765,6 +766,14 @@ __device__ __forceinline__ bool mbar_wait(unsigned long long* bar, unsigned pari
 // floats of one staged field of a band (N+1 rows of strip_bw columns), rounded up so that
 // every field's block starts 128-byte aligned (tensor-copy destinations)
 __host__ __device__ inline int strip_field_floats(int N) { return ((N + 1) * strip_bw(N) + 31) & ~31; }
+__device__ __forceinline__ void bulk_load(void* dst, const void* src, unsigned bytes,
+                                          unsigned long long* bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+          smem_addr(dst)),
+      "l"(src), "r"(bytes), "r"(smem_addr(bar))
+      : "memory");
+}
 // one box of a 3-D tiled tensor map (column x, row y, field slot z) into shared memory;
 // x is a multiple of 4 floats (16 bytes), negative or past the edge reads zeros
 __device__ __forceinline__ void tensor_load_3d(void* dst, const void* tmap, int x, int y, int z,
@@ -916,25 +925,47 @@ __device__ __forceinline__ void strip_tick(const SolveDev& S, const int act, con
   }
   __syncthreads();
 
-  // TMA: element row `ez` of every field into ring slot (ez - ezs) % NST.  One tensor copy
-  // per staged field: the box of BW columns from X0 and N+1 rows from ez * N of the
-  // field's slot in the solve's workspace map (columns outside [0, pitch) read as zeros
-  // and are never used).  Field f is issued by lane 1 of warp f, so the copies are spread
-  // over the warps; thread 0 posts the expected bytes (a copy may complete first: the
-  // barrier's pending arrival keeps the phase open until then).
-  const bool has_copy = lane == 1 && warp < nload;
-  int cp_slot = 0;
-  if (has_copy) {
-    const float* fp = (warp == 0) ? cur : (warp == 1) ? c2p : (warp == 2) ? vin : fwdu;
-    cp_slot = (int)((fp - S.ws) / S.fstride);
-    tensormap_acquire(S.tmap);
-  }
+  // TMA: element row `ez` of every field into ring slot (ez - ezs) % NST; thread 0 posts
+  // the expected bytes (a copy may complete first: the barrier's pending arrival keeps
+  // the phase open until then).  Field f of a band lands in the slot's block f.
+  //  * chunks of at least kMapBands bands: one tensor copy per field, the box of BW
+  //    columns from X0 and N+1 rows from ez * N of the field's slot in the solve's
+  //    workspace map (columns outside [0, pitch) read as zeros and are never used),
+  //    issued by lane 1 of warp f.  Fewer, larger copies; the map's acquire and first
+  //    fetch cost a little per CTA and tick, which short chunks do not amortise.
+  //  * shorter chunks: one bulk copy per (field, row), spread over all warps (copy
+  //    q = lane * NW + warp), each thread fixing its source and destination once per tick.
   constexpr int FBF = ((N + 1) * BW + 31) & ~31;  // floats per staged field block
-  const unsigned band_bytes = (unsigned)(nload * NP * BW) * 4u;
+  const bool by_map = S.tmap != nullptr && nbands >= kMapBands;
+  const int cs = max(X0, 0), ce = min(X0 + BW, pitch);  // columns inside the field
+  const unsigned rowb = (unsigned)(ce - cs) * 4u;
+  const int myq = by_map ? (lane == 1 && warp < nload ? warp : NT) : lane * NW + warp;
+  const bool has_copy = by_map ? myq < nload : myq < nload * NP;
+  int cp_dst = 0, cp_slot = 0;
+  const float* cp_src = cur;
+  if (has_copy) {
+    const int f = by_map ? myq : myq / NP, a = by_map ? 0 : myq - f * NP;
+    const float* fp = (f == 0) ? cur : (f == 1) ? c2p : (f == 2) ? vin : fwdu;
+    if (by_map) {
+      cp_slot = (int)((fp - S.ws) / S.fstride);
+      cp_dst = f * FBF;
+      tensormap_acquire(S.tmap);
+    } else {
+      cp_src = fp + (long long)a * pitch + cs;
+      cp_dst = f * FBF + a * BW + (cs - X0);
+    }
+  }
+  const long long band_floats = (long long)N * pitch;
+  const unsigned band_bytes = by_map ? (unsigned)(nload * NP * BW) * 4u : (unsigned)(nload * NP) * rowb;
   auto issue = [&](int ez) {
     const int slot = (ez - ezs) % NST;
     if (tid == 0) mbar_expect_tx(bars + slot, band_bytes);
-    if (has_copy) tensor_load_3d(stages + slot * stage_f + warp * FBF, S.tmap, X0, ez * N, cp_slot, bars + slot);
+    if (has_copy) {
+      if (by_map)
+        tensor_load_3d(stages + slot * stage_f + cp_dst, S.tmap, X0, ez * N, cp_slot, bars + slot);
+      else
+        bulk_load(stages + slot * stage_f + cp_dst, cp_src + ez * band_floats, rowb, bars + slot);
+    }
   };
   for (int r = 0; r < min(NST, nbands); ++r) issue(ezs + r);
 
