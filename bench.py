@@ -37,7 +37,7 @@ BYTES_PER_NODE_ADJ_TICK = 40
 # DRAM bytes per node and tick of the strip kernel from one ncu capture (dram__bytes_read +
 # dram__bytes_write of one forward and one adjoint tick over 128 models, 10.3 M nodes;
 # profiles/sem_strip_kernel_N4_128models.md), scaled to a launch by its nodes
-TRAFFIC_B_PER_NODE = {"fwd": 16.6, "adj": 36.7}
+TRAFFIC_B_PER_NODE = {"fwd": 16.9, "adj": 37.1}
 
 
 def workload(nmodels=256, nelx=100, nelz=50, nt=3000, nrec=100, seed0=0):
