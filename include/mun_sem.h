@@ -158,6 +158,13 @@ int sem_forward_adjoint(sem_batch_t* batch, const sem_plan_t* plan, const double
                         int32_t ckpt_k, float* clean_out, double* loglik_out,
                         double* grad_out, void* stream);
 
+/* Diagnostics (no counterpart in the reference): exercise the time limit of the device
+ * waits without any fault.  which = 0: an mbarrier wait whose bytes never arrive (the
+ * strip kernel's ring wait); 1: a grid barrier one arrival short (the persistent
+ * kernel's tick barrier); 2: a grid barrier that completes.  Blocks about 2 s for
+ * 0 and 1; *status_out = SEM_ERR_TIMEOUT for 0 and 1, SEM_OK for 2. */
+int sem_selftest_wait(int32_t which, int32_t* status_out);
+
 /* Allocation-free forward solve (receivers in the run() convention), for callers that
  * cannot allocate device memory while they run: a caller inside a memory pool that owns
  * the whole device, a real-time loop that must not hit cudaMalloc's implicit device

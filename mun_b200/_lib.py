@@ -55,7 +55,7 @@ EXPORTS = ["sem_plan_create", "sem_plan_destroy", "sem_plan_workspace_bytes", "s
            "sem_batch_destroy", "sem_run", "sem_batch_last_launches", "sem_batch_last_kernel",
            "sem_batch_last_groups", "sem_batch_last_shape", "sem_batch_last_ticks",
            "sem_batch_last_tick_ms", "sem_forward",
-           "sem_forward_adjoint", "sem_forward_noalloc", "sem_engine_create", "sem_engine_destroy",
+           "sem_forward_adjoint", "sem_forward_noalloc", "sem_selftest_wait", "sem_engine_create", "sem_engine_destroy",
            "sem_engine_submit", "sem_engine_step", "sem_engine_status", "sem_engine_release",
            "sem_engine_stats", "sem_velocity_from_curve", "sem_project_from_curve",
            "sem_velocity_last_error", "sem_last_error"]
@@ -100,6 +100,7 @@ def load(path=None):
     lib.sem_forward.argtypes = [vp, vp, vp, vp, vp]
     lib.sem_forward_adjoint.argtypes = [vp, vp, vp, vp, dbl, i32, i32, vp, vp, vp, vp]
     lib.sem_forward_noalloc.argtypes = [vp, vp, vp, vp, vp]
+    lib.sem_selftest_wait.argtypes = [i32, vp]
     lib.sem_engine_create.argtypes = [C.POINTER(EngineCfg), C.POINTER(vp)]
     lib.sem_engine_destroy.argtypes = [vp]
     lib.sem_engine_submit.argtypes = [vp, C.POINTER(Solve), C.POINTER(i64)]

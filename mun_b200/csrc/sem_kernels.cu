@@ -1408,6 +1408,27 @@ __global__ void __launch_bounds__(256) sem_persist_kernel(const SolveDev* __rest
   }
 }
 
+// Diagnostics of the device waits' time limits, without any fault: which = 0 waits on an
+// mbarrier whose expected bytes never arrive (no copy is issued), 1 on a grid barrier one
+// arrival short of its target (cooperative launch of 2 CTAs), 2 on a grid barrier that
+// completes.  A wait that gives up sets SEM_ERR_TIMEOUT in *status.
+__global__ void wait_probe_kernel(int which, unsigned long long* bar, int* status) {
+  __shared__ unsigned long long mb;
+  __shared__ int s_ok;
+  if (which == 0) {
+    if (threadIdx.x == 0) {
+      mbar_init(&mb, 1);
+      asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+      mbar_expect_tx(&mb, 16u);  // the only arrival, and 16 bytes that never come
+    }
+    __syncthreads();
+    if (!mbar_wait(&mb, 0) && threadIdx.x == 0) atomicOr(status, SEM_ERR_TIMEOUT);
+    return;
+  }
+  const unsigned long long target = gridDim.x + (which == 1 ? 1ull : 0ull);
+  if (!grid_barrier(bar, target, &s_ok) && threadIdx.x == 0) atomicOr(status, SEM_ERR_TIMEOUT);
+}
+
 __global__ void tick_advance_kernel(int* tick) { *tick += 1; }
 
 // c (float64, reference order) -> c^2 (float32, pitched grid)
@@ -2493,6 +2514,34 @@ int sem_batch_last_tick_ms(const sem_batch_t* b, double* ms_out) {
   }
   *ms_out = tot;
   return SEM_OK;
+}
+
+int sem_selftest_wait(int32_t which, int32_t* status_out) {
+  if (!status_out || which < 0 || which > 2) return fail(SEM_ERR_ARG, "which must be 0, 1 or 2");
+  char* buf = nullptr;
+  CUDA_TRY(cudaMalloc((void**)&buf, 256));
+  int rc = SEM_OK;
+  unsigned long long* bar = reinterpret_cast<unsigned long long*>(buf);
+  int* st = reinterpret_cast<int*>(buf + 128);
+  cudaError_t e = cudaMemset(buf, 0, 256);
+  if (e == cudaSuccess) {
+    cudaLaunchConfig_t lc = {};
+    lc.gridDim = dim3(which == 0 ? 1u : 2u);
+    lc.blockDim = dim3(32);
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeCooperative;
+    at[0].val.cooperative = 1;
+    lc.attrs = at;
+    lc.numAttrs = which == 0 ? 0 : 1;
+    e = cudaLaunchKernelEx(&lc, wait_probe_kernel, (int)which, bar, st);
+  }
+  if (e == cudaSuccess) e = cudaDeviceSynchronize();
+  int h = 0;
+  if (e == cudaSuccess) e = cudaMemcpy(&h, st, sizeof(int), cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess) rc = fail(SEM_ERR_CUDA, cudaGetErrorString(e));
+  cudaFree(buf);
+  *status_out = h;
+  return rc;
 }
 
 int sem_forward_noalloc(const sem_plan_t* p, const double* velocity, float* rec_out,
