@@ -1,8 +1,9 @@
 """Launch-configuration autotuner.
 
-Picks the kernel variant (tile kernel with a tile shape, or strip kernel) and the
-CUDA-graph chunk for a batch by timing candidates on a short proxy of the batch (the
-checkpoint interval and group split stay with the library's memory-budget schedule): the same meshes, orders, receivers and velocities with a few dozen time steps.
+Picks the kernel variant (tile kernel with a tile shape, persistent tile kernel, or strip
+kernel) and the CUDA-graph chunk for a batch by timing candidates on a short proxy of the
+batch: the same meshes, orders, receivers and velocities with a few dozen time steps.
+The checkpoint interval and group split stay with the library's memory-budget schedule.
 The choice is cached per batch signature (mesh sizes, orders, solve count, adjoint or
 not).  Results never depend on the choice: every variant computes bitwise the same
 numbers, so tuning only moves time.
@@ -16,7 +17,7 @@ import torch
 from .plan import SEMPlan
 from .solver import Batch, SolveSpec
 
-TILE_CANDIDATES = [(8, 8), (16, 8), (8, 4), (16, 4), (4, 4)]
+TILE_CANDIDATES = [(0, 0), (8, 8), (16, 8), (8, 4), (16, 4), (4, 4), (2, 2)]  # (0, 0): automatic
 GRAPH_CANDIDATES = [0, 32]
 
 _cache = {}
@@ -53,12 +54,15 @@ def tune(specs, nt_proxy=48, repeats=2, candidates=None, verbose=False):
                                  misfit=s.misfit, y_obs=y, inv_sigma2=s.inv_sigma2, ckpt_k=p.nt))
         return out
 
+    # the persistent kernel is one launch per run (graphs do not apply); it falls back to
+    # per-tick tile launches by itself when the tiles are not all resident
     cands = candidates or ([(1, t, g) for t in TILE_CANDIDATES for g in GRAPH_CANDIDATES]
+                           + [(3, t, 0) for t in TILE_CANDIDATES]
                            + [(2, (0, 0), g) for g in GRAPH_CANDIDATES])
     best, best_t = None, float("inf")
     stream = torch.cuda.Stream()
     for kernel, tile, chunk in cands:
-        b = Batch(tile=tile if kernel == 1 else (8, 8), graph_chunk=chunk, kernel=kernel)
+        b = Batch(tile=tile if kernel in (1, 3) else (8, 8), graph_chunk=chunk, kernel=kernel)
         try:
             with torch.cuda.stream(stream):
                 b.run(proxy_specs())  # warm-up (plan lists, graph instantiation)
@@ -88,5 +92,5 @@ def tune(specs, nt_proxy=48, repeats=2, candidates=None, verbose=False):
 def tuned_batch(specs, **kw):
     """A ``Batch`` configured by ``tune`` (checkpointing stays automatic)."""
     cfg = tune(specs, **kw)
-    return Batch(tile=cfg["tile"] if cfg["kernel"] == 1 else (8, 8), graph_chunk=cfg["graph_chunk"],
+    return Batch(tile=cfg["tile"] if cfg["kernel"] in (1, 3) else (8, 8), graph_chunk=cfg["graph_chunk"],
                  kernel=cfg["kernel"]), cfg
