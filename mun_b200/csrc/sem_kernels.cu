@@ -715,8 +715,8 @@ __constant__ float2 c_D2[kMaxN + 1][64];
 __constant__ float2 c_B2[kMaxN + 1][8];
 
 __host__ __device__ inline int strip_ew_max(int N) { return (kStripCols - N - 1) / N; }
-__host__ __device__ inline int strip_bw(int N) { return (kStripCols + 3 + 3) & ~3; }  // smem row
-__host__ __device__ inline int strip_threads(int N) { return kStripCols; }
+__host__ __device__ inline int strip_bw(int /*N*/) { return (kStripCols + 3 + 3) & ~3; }  // smem row
+__host__ __device__ inline int strip_threads(int /*N*/) { return kStripCols; }
 
 __device__ __forceinline__ uint32_t smem_addr(const void* p) {
   return (uint32_t)__cvta_generic_to_shared(p);
