@@ -737,8 +737,9 @@ def main():
                          "launch_us_avg": 1e3 * tick_loop_ms / ticks_per_step,
                          "ticks_per_step": ticks_per_step, "forward_like_ticks": fwd_like,
                          "note": "algorithmic bytes of the step's tick launches over the CUDA-"
-                                 "event time of the tick loops (tick kernel + 1-thread tick "
-                                 "counter kernel per tick); traffic = ncu DRAM bytes per launch",
+                                 "event time of the tick loops (one tick-kernel launch per tick, "
+                                 "chained by programmatic dependent launch); traffic = ncu DRAM "
+                                 "bytes per launch",
                          "step_level": {"bytes_per_node_step": BYTES_PER_NODE_STEP_FWDADJ,
                                         "achieved": step_achieved,
                                         "frac": step_achieved / peak}},
