@@ -5,7 +5,7 @@ order-4 mesh over 2000x1000 m (80,601 nodes), each the three-layer 1500/2200/300
 base (interfaces at 300/650 m) plus a cubic tensor B-spline perturbation on a 10x6
 node grid with N(0, 100^2) m/s node values drawn from a seed; Ricker 10 Hz at
 (1000, 20), 100 receivers at 10 m depth, 3000 steps at the CFL limit, sponge 200 m on
-all sides, float32 wavefields, float64 misfit and gradient accumulation.  Observed data
+all sides, float32 wavefields and gradient accumulation, float64 misfit.  Observed data
 come from a seeded "true" perturbation.  Inputs are synthetic (no dataset involved).
 
 A step = one batched forward+adjoint pass over all 256 models.  ``value`` is
@@ -28,16 +28,18 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, HERE)
 
-BYTES_PER_NODE_STEP_FWDADJ = 56  # algorithmic bytes (float32 state, float64 gradient RMW)
+# algorithmic bytes per node and fwd+adj step: forward 16, forward-state store/load 8,
+# adjoint 16, float32 gradient read-modify-write 8
+BYTES_PER_NODE_STEP_FWDADJ = 48
 # bytes one tick moves per node in the strip kernel: forward / replay tick reads b, v, c^2
-# and writes b, v; adjoint tick reads lambda, mu, c^2, the forward b and the float64
-# gradient and writes lambda, mu and the gradient
+# and writes b, v; adjoint tick reads lambda, mu, c^2, the forward b and the float32
+# gradient accumulator and writes lambda, mu and the accumulator
 BYTES_PER_NODE_FWD_TICK = 20
-BYTES_PER_NODE_ADJ_TICK = 40
+BYTES_PER_NODE_ADJ_TICK = 32
 # DRAM bytes per node and tick of the strip kernel from one ncu capture (dram__bytes_read +
 # dram__bytes_write of one forward and one adjoint tick over 128 models, 10.3 M nodes;
 # profiles/sem_strip_kernel_N4_128models.md), scaled to a launch by its nodes
-TRAFFIC_B_PER_NODE = {"fwd": 16.9, "adj": 37.1}
+TRAFFIC_B_PER_NODE = {"fwd": 16.8, "adj": 29.2}
 
 
 def workload(nmodels=256, nelx=100, nelz=50, nt=3000, nrec=100, seed0=0):
@@ -712,7 +714,7 @@ def main():
             "metric": "SEM fwd+adjoint solves/s (batched vs plain, same GPU, <=1e-4 rel); p50/p99 ms",
             "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f32 state / f64 misfit+gradient", "data": "synthetic",
+            "vs_baseline": None, "dtype": "f32 state and gradient accumulation / f64 misfit", "data": "synthetic",
             "config": {"workload": "batched ELBO sampling (256 models, 100x50 el, N=4, 80601 nodes, "
                                    "3000 steps, 100 receivers)",
                        "models_per_gpu": n, "nodes": W["npoints"], "nt": W["nt"],

@@ -12,7 +12,7 @@
 //   1/(omega dt) (about 10-20x larger seismogram error, measured).
 //   Adjoint step (core.py:1252-1275): the same recurrence run backwards with the
 //   source R^T r_it / sigma^2, no sponge (or the sponge, in exact mode), and the
-//   per-step sensitivity of core.py:49-85 accumulated in float64.
+//   per-step sensitivity of core.py:49-85 accumulated in float32 (see sens_increment).
 //
 // Operator structure used here.  With rectangular affine elements and GLL
 // collocation, Gx = (2/dx) kron(L,D), Gz = (2/dz) kron(D,L) with L diagonal
@@ -105,7 +105,7 @@ struct SolveDev {
   float* ring;  // k+1 fields: b at t = j*k .. j*k+k of the segment being replayed
   float* L;     // 2 fields: adjoint lambda ping-pong
   float* Mu;    // 1 field: adjoint increment (in place)
-  double* grad; // 1 field of doubles (dJ/dc^2 accumulated over time)
+  float* grad;  // 1 field: dJ/dc^2 (times the adjoint scale) accumulated over time
   // operators and tables
   const float* D;     // (N+1)^2
   const float* beta;  // N+1
@@ -208,9 +208,11 @@ __host__ __device__ inline long long smem_floats(int N, int tex, int tez, bool a
 
 
 // The zero-lag sensitivity increment of one node, R_z S_x + R_x S_z, rounded the same way
-// in every kernel.
-__device__ __forceinline__ double sens_increment(float Rzv, float SX, float Rxv, float SZ) {
-  return (double)__fmaf_rn(Rzv, SX, __fmul_rn(Rxv, SZ));
+// in every kernel.  It is summed over the adjoint ticks in float32 (__fadd_rn in both
+// kernels): against float64 accumulation of the same increments that adds 1e-8 to 1e-6
+// relative error over 200 to 2000 ticks, far below the float32 wavefield's own.
+__device__ __forceinline__ float sens_increment(float Rzv, float SX, float Rxv, float SZ) {
+  return __fmaf_rn(Rzv, SX, __fmul_rn(Rxv, SZ));
 }
 // Sensitivity of one segment node, beta_a (D w)_a (D lambda)_a, multiplied left to right.
 __device__ __forceinline__ float sens_product(float beta, float dw, float du) {
@@ -338,7 +340,7 @@ __device__ __forceinline__ void tile_tick(const SolveDev& S, const int act, cons
   const int w0 = threadIdx.x;
   const bool pre = (act != A_FINAL) && w0 < nro * nco;
   float p_v = 0.f, p_ix = 0.f, p_Rx = 0.f, p_dx = 0.f, p_iz = 0.f, p_Rz = 0.f, p_dz = 0.f;
-  double p_g = 0.0;
+  float p_g = 0.f;
   if (pre) {
     const int gx = gxo0 + w0 % nco, gz = gzo0 + w0 / nco;
     const long long g0 = (long long)gz * S.pitch + gx;
@@ -625,7 +627,7 @@ __device__ __forceinline__ void tile_tick(const SolveDev& S, const int act, cons
       if (gx == S.src_gx && gz == S.src_gz) extra = S.src_term[t];
     } else {
       extra = have_inj ? sacc[r * nco + cc] : 0.f;
-      if (grad_on) S.grad[g] = (first ? p_g : S.grad[g]) + sens_increment(Rzv, SX, Rxv, SZ);
+      if (grad_on) S.grad[g] = __fadd_rn(first ? p_g : S.grad[g], sens_increment(Rzv, SX, Rxv, SZ));
     }
     float res, vres;
     advance_node(adj, damp, b, v, X, Z, ixv, Rxv, dxv, izv, Rzv, dzv, extra, res, vres);
@@ -790,7 +792,7 @@ __device__ __forceinline__ void tensormap_acquire(const void* tmap) {
 }
 
 __host__ __device__ inline long long strip_stage_floats(int N, bool adj) {
-  const int nfloat = adj ? 4 : 3;  // cur, c2, v (+ forward field); the float64 gradient is
+  const int nfloat = adj ? 4 : 3;  // cur, c2, v (+ forward field); the gradient is
                                    // loaded by its owner threads, not staged
   return (long long)nfloat * strip_field_floats(N);
 }
@@ -915,7 +917,7 @@ __device__ __forceinline__ void strip_tick(const SolveDev& S, const int act, con
     out = (float*)rep_b(S, seg, t + 1); vout = (float*)rep_v(S, seg, t + 1);
   }
   const float* const c2p = S.c2;
-  double* const gradp = S.grad;
+  float* const gradp = S.grad;
   const float* const tzp = S.tz;
   const int nload = final_only ? 1 : NF;
 
@@ -1043,7 +1045,7 @@ __device__ __forceinline__ void strip_tick(const SolveDev& S, const int act, con
     // a failed wait records the first band that failed; every thread tests "failed at or
     // before this band" after the band's barrier, so all threads leave at the same band
     // the owner's gradient rows of this band, loaded now and used in phase B
-    double gpre[N];
+    float gpre[N];
     if (ADJ && grad_on && owned && !halo) {
 #pragma unroll
       for (int a = 0; a < N; ++a) gpre[a] = gradp[gb + a * pitch];
@@ -1262,12 +1264,12 @@ __device__ __forceinline__ void strip_tick(const SolveDev& S, const int act, con
         const float izv = tzb[a], Rzv = tzb[8 + a], dzv = tzb[16 + a];
         const int g = gb + a * pitch;
         float extra;
-        double gnew = 0.0;
+        float gnew = 0.f;
         if (!ADJ) {
           extra = (ez * N + a == src_row) ? src_val : 0.f;
         } else {
           extra = in_win ? sacc[a * NT + tid] : 0.f;
-          if (grad_on) gnew = (a < N ? gpre[a < N ? a : 0] : gradp[g]) + sens_increment(Rzv, SX, Rxv, SZ);
+          if (grad_on) gnew = __fadd_rn(a < N ? gpre[a < N ? a : 0] : gradp[g], sens_increment(Rzv, SX, Rxv, SZ));
         }
         float res, vres;
         advance_node(ADJ, damp, Bs[a * BW + sc], Vs[a * BW + sc], X, Z, ixv, Rxv, dxv, izv, Rzv,
@@ -1454,7 +1456,7 @@ struct SolveIo {
   char* zp[8];            // workspace ranges that must start at zero (256-byte aligned,
   long long zb[8];        //   lengths multiples of 16 bytes)
   double* grad_out;       // or null
-  const double* gacc;     // float64 dJ/dc^2 accumulator
+  const float* gacc;      // dJ/dc^2 accumulator (float32, scaled)
   const double* adj_scale;
   double inv_sigma2;
   const double* misfit;   // [nrec]
@@ -1490,7 +1492,7 @@ __global__ void batch_output_kernel(const SolveIo* __restrict__ io, int s0) {
     const double scale = s.inv_sigma2 / *s.adj_scale;  // exact: adj_scale is a power of two
     for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < s.npoints;
          i += (long long)gridDim.x * blockDim.x)
-      s.grad_out[i] = 2.0 * s.vel[i] * s.gacc[s.pos[i]] * scale;
+      s.grad_out[i] = 2.0 * s.vel[i] * (double)s.gacc[s.pos[i]] * scale;
   }
   if (blockIdx.x == 0 && threadIdx.x == 0) {
     if (s.loglik_out) {
@@ -1808,7 +1810,7 @@ int encode_band_map(CUtensorMap* m, char* ws_base, const sem_plan_s* p, long lon
                          CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   return r == CUDA_SUCCESS ? SEM_OK : fail(SEM_ERR_CUDA, "tensor map encoding failed");
 }
-// float-field slots of a workspace (everything before the float64 gradient / the misfit)
+// float-field slots of a workspace (everything before the gradient / the misfit)
 long long field_slots(const Workspace& w, const sem_plan_s* p, bool adj) {
   return (adj ? w.grad : w.misfit) / (p->fstride * 4);
 }
@@ -1827,7 +1829,7 @@ Workspace layout(const sem_plan_s* p, int flags, int k, int* nseg_out) {
     w.ring = o; o += (long long)(k + 1) * F;
     w.L = o; o += 2 * F;
     w.Mu = o; o += F;
-    w.grad = o; o += 2 * F;
+    w.grad = o; o += F;
   }
   w.misfit = o; o += round_up((long long)(2 * p->nrec + 1) * 8, 256);  // misfit, rmax, scale
   w.status = o; o += 256;
@@ -2079,7 +2081,7 @@ static int run_group(sem_batch_t* b, const sem_solve_t* solves, int32_t n,
     d.ring = (s.flags & SEM_F_ADJOINT) ? (float*)(a + ws[i].ring) : nullptr;
     d.L = (s.flags & SEM_F_ADJOINT) ? (float*)(a + ws[i].L) : nullptr;
     d.Mu = (s.flags & SEM_F_ADJOINT) ? (float*)(a + ws[i].Mu) : nullptr;
-    d.grad = (s.flags & SEM_F_ADJOINT) ? (double*)(a + ws[i].grad) : nullptr;
+    d.grad = (s.flags & SEM_F_ADJOINT) ? (float*)(a + ws[i].grad) : nullptr;
     d.D = p->D; d.beta = p->beta; d.tx = p->tx; d.tz = p->tz; d.src_term = p->src_term;
     d.rec_base = p->rec_base; d.rec_w = p->rec_w;
     d.rec_tile_off = L.rec_off; d.rec_tile_ids = L.rec_ids;
@@ -2148,11 +2150,11 @@ static int run_group(sem_batch_t* b, const sem_solve_t* solves, int32_t n,
       zero(ws[i].ckpt, 2 * F);
       zero(ws[i].ring, F);
       zero(ws[i].L, 3 * F);      // L[0], L[1], Mu
-      zero(ws[i].grad, 2 * F);
+      zero(ws[i].grad, F);
     }
     zero(ws[i].misfit, ws[i].status - ws[i].misfit + 256);
     io.grad_out = ((s.flags & SEM_F_ADJOINT) && s.grad_out) ? s.grad_out : nullptr;
-    io.gacc = (const double*)(a + ws[i].grad);
+    io.gacc = (const float*)(a + ws[i].grad);
     io.adj_scale = (const double*)(a + ws[i].misfit) + 2 * p->nrec;
     io.inv_sigma2 = s.inv_sigma2;
     io.misfit = (const double*)(a + ws[i].misfit);
@@ -2711,11 +2713,11 @@ SolveIo solve_io(const sem_solve_t& s, const Workspace& ws, char* a) {
     zero(ws.ckpt, 2 * F);
     zero(ws.ring, F);
     zero(ws.L, 3 * F);  // L[0], L[1], Mu
-    zero(ws.grad, 2 * F);
+    zero(ws.grad, F);
   }
   zero(ws.misfit, ws.status - ws.misfit + 256);
   io.grad_out = ((s.flags & SEM_F_ADJOINT) && s.grad_out) ? s.grad_out : nullptr;
-  io.gacc = (const double*)(a + ws.grad);
+  io.gacc = (const float*)(a + ws.grad);
   io.adj_scale = (const double*)(a + ws.misfit) + 2 * p->nrec;
   io.inv_sigma2 = s.inv_sigma2;
   io.misfit = (const double*)(a + ws.misfit);
@@ -2997,7 +2999,7 @@ int sem_engine_step(sem_engine_t* e, void* stream_v) {
     d.ring = adj ? (float*)(a + j->ws.ring) : nullptr;
     d.L = adj ? (float*)(a + j->ws.L) : nullptr;
     d.Mu = adj ? (float*)(a + j->ws.Mu) : nullptr;
-    d.grad = adj ? (double*)(a + j->ws.grad) : nullptr;
+    d.grad = adj ? (float*)(a + j->ws.grad) : nullptr;
     d.D = p->D; d.beta = p->beta; d.tx = p->tx; d.tz = p->tz; d.src_term = p->src_term;
     d.rec_base = p->rec_base; d.rec_w = p->rec_w;
     d.rec_tile_off = L.rec_off; d.rec_tile_ids = L.rec_ids;
