@@ -5,22 +5,29 @@ order-4 mesh over 2000x1000 m (80,601 nodes), each the three-layer 1500/2200/300
 base (interfaces at 300/650 m) plus a cubic tensor B-spline perturbation on a 10x6
 node grid with N(0, 100^2) m/s node values drawn from a seed; Ricker 10 Hz at
 (1000, 20), 100 receivers at 10 m depth, 3000 steps at the CFL limit, sponge 200 m on
-all sides, float32 wavefields and gradient accumulation, float64 misfit.  Observed data
-come from a seeded "true" perturbation.  Inputs are synthetic (no dataset involved).
+all sides, float32 wavefields, float64 gradient time-sum (float32 partial sums of at
+most 16 ticks folded into float64) and float64 misfit.  Observed data come from a
+seeded "true" perturbation.  Inputs are synthetic (no dataset involved).
 
 A step = one batched forward+adjoint pass over all 256 models.  ``value`` is
 device-timed with CUDA events (inputs resident), ``e2e`` is the same step through the
 public API with host arrays copied in and gradients/logliks copied out inside the
-timed region.  ``plain`` times one-at-a-time solves of the same models.
+timed region.  ``plain`` times one-at-a-time solves of the same models.  Outside the
+timed region, two of the models are solved again by the float64 oracle on the host
+(``parity``), and compact runs of the single large solve, the uneven batch and the
+serving mix are added as ``single``, ``uneven`` and ``serving``.
 
 ``--impl reference`` times the oracle restatement of MUN's CPU path (torch-CPU float64,
-same library calls as the reference) on a bounded sample of the same workload.
+same library calls as the reference) on the host cores: one full 3000-step solve of
+one model per step (``--ref-nt N`` fits set-up + per-step cost from N- and 2N-step runs
+instead).
 """
 import argparse
 import json
 import os
 import subprocess
 import sys
+import tempfile
 import time
 
 import numpy as np
@@ -28,18 +35,26 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, HERE)
 
-# algorithmic bytes per node and fwd+adj step: forward 16, forward-state store/load 8,
-# adjoint 16, float32 gradient read-modify-write 8
-BYTES_PER_NODE_STEP_FWDADJ = 48
-# bytes one tick moves per node in the strip kernel: forward / replay tick reads b, v, c^2
-# and writes b, v; adjoint tick reads lambda, mu, c^2, the forward b and the float32
-# gradient accumulator and writes lambda, mu and the accumulator
+# the metric both arms report (the driver pairs the two lines by it)
+METRIC = "SEM fwd+adjoint solves/s (batched vs plain, same GPU, <=1e-4 rel); p50/p99 ms"
+# algorithmic bytes per node and fwd+adj step (float32 state): forward 16 (u_curr, u_prev
+# and c^2 read, u_next written), forward-state store/load 8, adjoint 16, float64 gradient
+# read-modify-write 16; a forward tick carries 20 of them, an adjoint tick 36
+BYTES_PER_NODE_STEP_FWDADJ = 56
 BYTES_PER_NODE_FWD_TICK = 20
-BYTES_PER_NODE_ADJ_TICK = 32
+BYTES_PER_NODE_ADJ_TICK = 36
+# bytes the strip kernel itself moves per node: forward tick 20 (reads b, v, c^2, writes
+# b, v); adjoint tick 32.5 (reads lambda, mu, c^2 and the forward b, writes lambda and mu,
+# float32 partial gradient read-modify-write, and a float64 fold every 16 ticks)
+IMPL_BYTES_PER_NODE = {"forward_tick": 20, "adjoint_tick": 32.5}
 # DRAM bytes per node and tick of the strip kernel from one ncu capture (dram__bytes_read +
-# dram__bytes_write of one forward and one adjoint tick over 128 models, 10.3 M nodes;
-# profiles/sem_strip_kernel_N4_128models.md), scaled to a launch by its nodes
+# dram__bytes_write of one forward and one adjoint tick of a 128-model group, 10.3 M nodes),
+# scaled to a launch by its nodes
 TRAFFIC_B_PER_NODE = {"fwd": 16.8, "adj": 29.2}
+
+
+WORKLOAD_ELBO = ("batched ELBO sampling (256 models, 100x50 el, N=4, 80601 nodes, 3000 steps, "
+                 "100 receivers)")
 
 
 def workload(nmodels=256, nelx=100, nelz=50, nt=3000, nrec=100, seed0=0):
@@ -260,12 +275,11 @@ def run_reference(args):
                   if nt_sample <= 0 or nt_sample >= W["nt"] else
                   f"1 model, {nt_sample}- and {2 * nt_sample}-step runs (of 3000) fitted to set-up + "
                   "per-step cost")
-    out = {"metric": "SEM fwd+adjoint solves/s", "value": val, "unit": "solves/s",
+    out = {"metric": METRIC, "value": val, "unit": "solves/s",
            "impl": "reference", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
            "ms_per_step": per * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
            "dtype": "f64", "data": "synthetic",
-           "config": {"workload": "batched ELBO sampling: 100x50 el, N=4, 80601 nodes, 3000 steps",
-                      "sample": sample_txt},
+           "config": {"workload": WORKLOAD_ELBO, "sample": sample_txt},
            "cpu_baseline": {"value": val, "unit": "solves/s", "cores": threads, "kind": "port",
                             "sample": sample_txt},
            "e2e": {"value": val, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
@@ -280,16 +294,14 @@ def _layered_plume(coords, cx, cz, ax, az, drop=0.08):
     return base * (1.0 - drop * w)
 
 
-def run_uneven(args):
-    """Uneven batch: 64 solves, meshes 40x20..200x100 (2:1), orders {3,4,5}, 8-20 Hz,
-    nt from each mesh's CFL for T=0.5 s clamped to [1500, 6000], layered base with a
-    seeded elliptical -8% plume; one batched launch sequence vs one solve at a time."""
-    import torch
-    from mun_b200 import Batch, SEMPlan, SolveSpec
+def uneven_specs(n=64, seed=3):
+    """Uneven batch: n solves, meshes 40x20..200x100 (2:1), orders {3,4,5}, 8-20 Hz, nt from
+    each mesh's CFL for T = 0.5 s clamped to [1500, 6000], layered base with a seeded
+    elliptical -8% plume; observations from each model's own forward at 2% lower velocity."""
     from mun_b200.mesh import create_global_mesh
-    rng = np.random.default_rng(3)
-    specs_args = []
-    for i in range(args.models if args.models != 256 else 64):
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(n):
         nelx = int(rng.integers(40, 201))
         nelz = max(1, nelx // 2)
         N = int(rng.choice([3, 4, 5]))
@@ -301,45 +313,65 @@ def run_uneven(args):
         dt = 0.35 * (h / (N + 1)) / (float(v.max()) * (N + 1) * np.sqrt(2.0))
         nt = int(min(6000, max(1500, np.ceil(0.5 / dt))))
         rec = np.stack([np.linspace(0.0, 2000.0, 100), np.full(100, 10.0)], 1)
-        specs_args.append(dict(plan=dict(xmin=0.0, xmax=2000.0, zmin=0.0, zmax=1000.0, nelx=nelx, nelz=nelz,
-                                         npol=N, dt=dt, nt=nt, src_xz=(1000.0, 20.0), f0=f0, amp=1.0,
-                                         receivers=rec, pml_thickness=200.0, sponge_cmax=3000.0,
-                                         coords=coords, node_grid=ng), v=v))
+        out.append(dict(plan=dict(xmin=0.0, xmax=2000.0, zmin=0.0, zmax=1000.0, nelx=nelx, nelz=nelz,
+                                  npol=N, dt=dt, nt=nt, src_xz=(1000.0, 20.0), f0=f0, amp=1.0,
+                                  receivers=rec, pml_thickness=200.0, sponge_cmax=3000.0,
+                                  coords=coords, node_grid=ng), v=v))
+    return out
+
+
+def run_uneven(args, steps=None, warmup=None, plain=None, cpu_sample=None, emit=True):
+    """Uneven batch (64 solves of uneven meshes, orders and step counts), batched through
+    the autotuned launch configuration vs one solve at a time."""
+    import torch
+    from mun_b200 import Batch, SEMPlan, SolveSpec
+    from mun_b200.autotune import tuned_batch
+    steps = args.steps if steps is None else steps
+    warmup = args.warmup if warmup is None else warmup
+    plain = args.plain if plain is None else plain
+    cpu_sample = args.cpu_sample if cpu_sample is None else cpu_sample
+    specs_args = uneven_specs(args.models if (emit and args.models != 256) else 64)
     plans = [SEMPlan(**a["plan"]) for a in specs_args]
     dev = torch.device("cuda")
     stream = torch.cuda.Stream()
-    # observations: each model's own forward with a 2% slower velocity
     ys = []
-    for p, a in zip(plans, specs_args):
-        s = SolveSpec(p, torch.as_tensor(a["v"] * 0.98, device=dev), shift=True)
-        with torch.cuda.stream(stream):
-            Batch().run([s])
-        ys.append(s.rec.double())
+    ob = Batch()
+    with torch.cuda.stream(stream):
+        for p, a in zip(plans, specs_args):
+            s = SolveSpec(p, torch.as_tensor(a["v"] * 0.98, device=dev), shift=True)
+            ob.run([s])
+            ys.append(s.rec.double())
     stream.synchronize()
     node_steps = sum(p.npoints * p.nt for p in plans)
 
     def specs():
         return [SolveSpec(p, torch.as_tensor(a["v"], device=dev), adjoint=True, y_obs=y, inv_sigma2=1e6,
                           ckpt_k=0) for p, a, y in zip(plans, specs_args, ys)]
-    b = Batch(kernel=args.kernel, graph_chunk=args.graph_chunk)
+    t0 = time.perf_counter()
+    if args.kernel == 0 and args.graph_chunk == 0:
+        b, tuned = tuned_batch(specs())
+    else:
+        b, tuned = Batch(kernel=args.kernel, graph_chunk=args.graph_chunk), None
+    tune_s = time.perf_counter() - t0
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     ms = []
-    for it in range(args.warmup + args.steps):
+    for it in range(warmup + steps):
         sp = specs()
         with torch.cuda.stream(stream):
             ev0.record(stream)
             b.run(sp)
             ev1.record(stream)
         ev1.synchronize()
-        if it >= args.warmup:
+        if it >= warmup:
             ms.append(ev0.elapsed_time(ev1))
+    status = max(int(s.status.item()) for s in sp)
     batched = len(plans) / (np.mean(ms) / 1e3)
     plain_ms = []
     pb = Batch()
-    for sp in specs()[: max(4, args.plain)]:
+    for sp1 in specs()[: max(4, plain)]:
         with torch.cuda.stream(stream):
             ev0.record(stream)
-            pb.run([sp])
+            pb.run([sp1])
             ev1.record(stream)
         ev1.synchronize()
         plain_ms.append(ev0.elapsed_time(ev1))
@@ -347,30 +379,36 @@ def run_uneven(args):
     sub = plans[: len(plain_ms)]
     plain_total = sum(plain_ms) * node_steps / sum(p.npoints * p.nt for p in sub)
     cpu = None
-    if args.cpu_sample > 0:
+    if cpu_sample > 0:
         threads = os.cpu_count() or 1
         per_ns, el = [], 0.0
         for p, a in list(zip(plans, specs_args))[:2]:
             kw_o = {k: a["plan"][k] for k in a["plan"] if k not in ("coords", "node_grid", "dt", "nt")}
-            per, e = cpu_estimate(kw_o, a["plan"]["dt"], p.nt, a["v"], args.cpu_sample, threads)
+            per, e = cpu_estimate(kw_o, a["plan"]["dt"], p.nt, a["v"], cpu_sample, threads)
             per_ns.append(per / (p.npoints * p.nt))
             el += e
         total = float(np.mean(per_ns)) * node_steps
         cpu = {"solves_per_s": len(plans) / total, "s_all": total, "cores": threads, "kind": "port",
-               "sample": f"first 2 solves, {args.cpu_sample}/{2 * args.cpu_sample}-step runs, per node-step "
+               "sample": f"first 2 solves, {cpu_sample}/{2 * cpu_sample}-step runs, per node-step "
                          f"cost scaled to all 64 ({el:.0f} s)"}
-    print(json.dumps({"workload": "uneven batch: 64 solves, 40x20..200x100 el, N in {3,4,5}, nt 1500-6000",
-                      "cpu": cpu,
-                      "metric": "SEM fwd+adjoint solves/s", "batched": batched, "unit": "solves/s",
-                      "batched_ms": float(np.mean(ms)), "kernel": b.last_kernel,
-                      "plain_estimated": len(plans) / (plain_total / 1e3), "plain_solves_timed": len(plain_ms),
-                      "mnode_steps_per_s": node_steps / (np.mean(ms) / 1e3) / 1e6,
-                      "orders": sorted(set(p.npol for p in plans)), "nt_range": [min(p.nt for p in plans),
-                                                                                   max(p.nt for p in plans)]}),
-          flush=True)
+    out = {"workload": "uneven batch: 64 solves, 40x20..200x100 el, N in {3,4,5}, nt 1500-6000",
+           "metric": "SEM fwd+adjoint solves/s", "unit": "solves/s", "batched": batched,
+           "batched_ms": float(np.mean(ms)), "kernel": b.last_kernel, "groups": b.last_groups,
+           "autotuned": None if tuned is None else {"kernel": tuned["kernel"], "tile": list(tuned["tile"]),
+                                                    "graph_chunk": tuned["graph_chunk"],
+                                                    "ckpt_k": "automatic schedule",
+                                                    "tuning_s": round(tune_s, 1)},
+           "plain_estimated": len(plans) / (plain_total / 1e3), "plain_solves_timed": len(plain_ms),
+           "batched_over_plain": batched / (len(plans) / (plain_total / 1e3)),
+           "mnode_steps_per_s": node_steps / (np.mean(ms) / 1e3) / 1e6,
+           "orders": sorted(set(p.npol for p in plans)),
+           "nt_range": [min(p.nt for p in plans), max(p.nt for p in plans)], "cpu": cpu, "status": status}
+    if emit:
+        print(json.dumps(out), flush=True)
+    return out
 
 
-def run_serving(args):
+def run_serving(args, requests=None, emit=True):
     """Serving: Poisson request stream of forward-only likelihoods from 16 random-walk MCMC
     chains (meshes 60x30..120x60, order 4) mixed with flow-trainer batches of 32
     forward+adjoint solves (100x50, order 4, 10x6 B-spline perturbations); continuous
@@ -407,7 +445,7 @@ def run_serving(args):
     reqs = []
     t = 0.0
     rate = args.serve_rate
-    n_req = args.serve_requests
+    n_req = args.serve_requests if requests is None else requests
     k_flow = 0
     while len(reqs) < n_req:
         t += rng.exponential(1.0 / rate)
@@ -423,7 +461,9 @@ def run_serving(args):
                                                  adjoint=True, y_obs=fy, inv_sigma2=1e6, ckpt_k=fplan.nt),
                                     "flow"))
             k_flow += 1
-    eng = Engine(max_solves=args.serve_slots, memory_cap_bytes=int(args.serve_cap_gb * (1 << 30)),
+    free, _ = torch.cuda.mem_get_info()
+    cap = min(int(args.serve_cap_gb * (1 << 30)), int(free) - (8 << 30))
+    eng = Engine(max_solves=args.serve_slots, memory_cap_bytes=cap,
                  ticks_per_step=args.serve_ticks, kernel=args.kernel)
     done, lat, wall = serve(eng, reqs)
     # serialized reference: the same requests one at a time, back to back
@@ -444,18 +484,19 @@ def run_serving(args):
            "p50_ms_mcmc": 1e3 * float(np.percentile(lat[kinds == "mcmc"], 50)),
            "p99_ms_mcmc": 1e3 * float(np.percentile(lat[kinds == "mcmc"], 99)),
            "p50_ms_flow": 1e3 * float(np.percentile(lat[kinds == "flow"], 50)) if (kinds == "flow").any() else None,
-           "serialized_solves_per_s": len(reqs) / serial, "engine": eng.stats()}
-    print(json.dumps(out), flush=True)
+           "serialized_solves_per_s": len(reqs) / serial, "served_over_serialized": (len(done) / wall) / (len(reqs) / serial),
+           "memory_cap_gb": cap / (1 << 30), "engine": eng.stats()}
+    if emit:
+        print(json.dumps(out), flush=True)
+    return out
 
 
-def run_single(args):
-    """Single large solve: 8000x4000 m, 400x200 elements, order 4 (1601x801 nodes), GRF
-    velocity (mean 2500, std 300, correlation 200 m, clipped [1500,4000], seed 1), Ricker
-    15 Hz at the surface centre, 400 surface receivers, 5000 steps, checkpoint every 250."""
-    import torch
-    from mun_b200 import Batch, SEMPlan, SolveSpec
+def single_model(nelx=400, nelz=200, N=4):
+    """Single large solve inputs: 8000x4000 m, order 4 (1601x801 nodes at 400x200), GRF
+    velocity (mean 2500, std 300, correlation 200 m, clipped [1500, 4000], seed 1), dt at
+    the CFL limit."""
     from mun_b200.mesh import create_global_mesh
-    nelx, nelz, N = 400, 200, 4
+    from mun_b200.sem_waveform.velocity import build_background_from_grid
     coords, _, ng = create_global_mesh(0.0, 8000.0, 0.0, 4000.0, nelx, nelz, N)
     rng = np.random.default_rng(1)
     nx, nz = 801, 401
@@ -466,10 +507,23 @@ def run_single(args):
     f = np.real(np.fft.ifft2(np.fft.fft2(w) * np.exp(-2 * (np.pi ** 2) * (200.0 ** 2) * K2)))
     f = (f - f.mean()) / f.std() * 300.0 + 2500.0
     grid = np.clip(f, 1500.0, 4000.0)
-    from mun_b200.sem_waveform.velocity import build_background_from_grid
     v = build_background_from_grid(coords, np.linspace(0, 8000, nx), np.linspace(0, 4000, nz), grid)
-    dt = 0.35 * (20.0 / 5) / (float(v.max()) * 5 * np.sqrt(2.0))
-    nt = args.nt if args.nt != 3000 else 5000
+    h = min(8000.0 / nelx, 4000.0 / nelz)
+    dt = 0.35 * (h / (N + 1)) / (float(v.max()) * (N + 1) * np.sqrt(2.0))
+    return coords, ng, v, dt
+
+
+def run_single(args, steps=None, warmup=None, cpu_sample=None, emit=True):
+    """Single large solve: 400x200 elements, order 4, GRF velocity, Ricker 15 Hz at the
+    surface centre, 400 surface receivers, 5000 steps, checkpoint every 250."""
+    import torch
+    from mun_b200 import Batch, SEMPlan, SolveSpec
+    steps = args.steps if steps is None else steps
+    warmup = args.warmup if warmup is None else warmup
+    cpu_sample = args.cpu_sample if cpu_sample is None else cpu_sample
+    nelx, nelz, N = 400, 200, 4
+    coords, ng, v, dt = single_model(nelx, nelz, N)
+    nt = args.nt if (emit and args.nt != 3000) else 5000
     rec = np.stack([np.linspace(0.0, 8000.0, 400), np.full(400, 1e-3)], 1)
     plan = SEMPlan(xmin=0.0, xmax=8000.0, zmin=0.0, zmax=4000.0, nelx=nelx, nelz=nelz, npol=N, dt=dt, nt=nt,
                    src_xz=(4000.0, 1e-3), f0=15.0, amp=1.0, receivers=rec, pml_thickness=400.0,
@@ -479,55 +533,88 @@ def run_single(args):
     Batch().run([obs])
     stream = torch.cuda.Stream()
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    ms = []
     b = Batch(kernel=args.kernel)
-    for it in range(args.warmup + args.steps):
-        s = SolveSpec(plan, torch.as_tensor(v, device=dev), adjoint=True, y_obs=obs.rec.double(), inv_sigma2=1e6,
-                      ckpt_k=250)
-        with torch.cuda.stream(stream):
-            ev0.record(stream)
-            b.run([s])
-            ev1.record(stream)
-        ev1.synchronize()
-        if it >= args.warmup:
-            ms.append(ev0.elapsed_time(ev1))
-    m = float(np.mean(ms))
-    ticks_k250 = b.last_ticks
+
+    def timed(k):
+        ms = []
+        for it in range(warmup + steps):
+            s = SolveSpec(plan, torch.as_tensor(v, device=dev), adjoint=True, y_obs=obs.rec.double(),
+                          inv_sigma2=1e6, ckpt_k=k)
+            with torch.cuda.stream(stream):
+                ev0.record(stream)
+                b.run([s])
+                ev1.record(stream)
+            ev1.synchronize()
+            if it >= warmup:
+                ms.append(ev0.elapsed_time(ev1))
+        return float(np.mean(ms)), s, b.last_ticks, b.last_tick_ms()
+    m, s, ticks_k250, tick_ms = timed(250)
     # the same solve under the automatic schedule: its float32 forward history (25.6 GB)
     # fits, so there is no replay
-    ms_auto = []
-    for it in range(args.warmup + args.steps):
-        s2 = SolveSpec(plan, torch.as_tensor(v, device=dev), adjoint=True, y_obs=obs.rec.double(),
-                       inv_sigma2=1e6, ckpt_k=0)
-        with torch.cuda.stream(stream):
-            ev0.record(stream)
-            b.run([s2])
-            ev1.record(stream)
-        ev1.synchronize()
-        if it >= args.warmup:
-            ms_auto.append(ev0.elapsed_time(ev1))
-    m_auto = float(np.mean(ms_auto))
+    m_auto, s2, ticks_auto, tick_ms_auto = timed(0)
     same = bool(torch.equal(s.grad, s2.grad) and torch.equal(s.rec, s2.rec))
-    auto = {"ms_per_solve": m_auto, "solves_per_s": 1e3 / m_auto, "ticks": b.last_ticks,
+    alg = BYTES_PER_NODE_STEP_FWDADJ * plan.npoints * nt
+    pk, pk_kind = peaks()
+    peak = float(pk.get("hbm_gbs", 6650.0))
+    auto = {"ms_per_solve": m_auto, "solves_per_s": 1e3 / m_auto, "ticks": ticks_auto,
             "groups": b.last_groups, "bitwise_equal_to_k250": same,
-            "achieved_gbs_56B": 56 * plan.npoints * nt / (m_auto / 1e3) / 1e9}
+            "achieved_gbs_56B": alg / (m_auto / 1e3) / 1e9,
+            "hbm_frac_56B": alg / (m_auto / 1e3) / 1e9 / peak,
+            "tick_loop_ms": tick_ms_auto}
     cpu = None
-    if args.cpu_sample > 0:
+    if cpu_sample > 0:
         kw_o = dict(xmin=0.0, xmax=8000.0, zmin=0.0, zmax=4000.0, nelx=nelx, nelz=nelz, npol=N,
                     src_xz=(4000.0, 1e-3), f0=15.0, amp=1.0, receivers=rec, pml_thickness=400.0,
                     sponge_cmax=4000.0)
         threads = os.cpu_count() or 1
-        per, el = cpu_estimate(kw_o, dt, nt, v, args.cpu_sample, threads)
+        per, el = cpu_estimate(kw_o, dt, nt, v, cpu_sample, threads)
         cpu = {"s_per_solve": per, "solves_per_s": 1.0 / per, "cores": threads, "kind": "port",
-               "sample": f"{args.cpu_sample}- and {2 * args.cpu_sample}-step runs of {nt}, linear fit "
+               "sample": f"{cpu_sample}- and {2 * cpu_sample}-step runs of {nt}, linear fit "
                          f"(float64 state, no checkpointing: {el:.0f} s)"}
-    print(json.dumps({"workload": "single large solve: 400x200 el, N=4, 1,282,401 nodes, 5000 steps, k=250",
-                      "cpu": cpu,
-                      "nt": nt, "ms_per_solve": m, "solves_per_s": 1e3 / m, "kernel": b.last_kernel,
-                      "mnode_steps_per_s": plan.npoints * nt / (m / 1e3) / 1e6,
-                      "achieved_gbs_56B": 56 * plan.npoints * nt / (m / 1e3) / 1e9, "ticks": ticks_k250,
-                      "auto_schedule": auto,
-                      "status": int(s.status.item()) | int(s2.status.item())}), flush=True)
+    out = {"workload": "single large solve: 400x200 el, N=4, 1,282,401 nodes, 5000 steps, k=250",
+           "nt": nt, "ms_per_solve": m, "solves_per_s": 1e3 / m, "kernel": b.last_kernel,
+           "shape (tile_ex, tile_ez, strip_bands)": list(b.last_shape),
+           "mnode_steps_per_s": plan.npoints * nt / (m / 1e3) / 1e6,
+           "achieved_gbs_56B": alg / (m / 1e3) / 1e9, "hbm_frac_56B": alg / (m / 1e3) / 1e9 / peak,
+           "peak_kind": pk_kind, "ticks": ticks_k250, "tick_loop_ms": tick_ms,
+           "auto_schedule": auto, "cpu": cpu,
+           "status": int(s.status.item()) | int(s2.status.item())}
+    if emit:
+        print(json.dumps(out), flush=True)
+    return out
+
+
+def parity_leg(W, specs, y, which):
+    """Relative errors of solves ``which`` of the timed batch (their last run) against the
+    float64 oracle on the host, same velocity and observations: seismogram (rel. L2),
+    gradient dJ/dv (rel. L2), log-likelihood (rel.).  Outside the timed region."""
+    import torch
+    from oracle import sem_oracle as so
+    torch.set_num_threads(os.cpu_count() or 1)
+    kw = W["plan_kw"]
+    cfg = {"domain": {"xmin": kw["xmin"], "xmax": kw["xmax"], "zmin": kw["zmin"],
+                      "zmax": kw["zmax"], "nelem_x": kw["nelx"], "nelem_z": kw["nelz"]},
+           "time": {"total_time": (W["nt"] - 0.5) * W["dt"], "dt": W["dt"]},
+           "source": {"position": kw["src_xz"], "frequency": kw["f0"], "amplitude": kw["amp"]},
+           "receivers": {"positions": kw["receivers"]},
+           "method": {"polynomial_order": kw["npol"], "pml_thickness": kw["pml_thickness"]},
+           "velocity": {"outside_velocity": kw["sponge_cmax"]}}
+    yy = y.cpu().numpy()
+    rel = lambda a, b: float(np.linalg.norm(a - b) / np.linalg.norm(b))  # noqa: E731
+    t0 = time.perf_counter()
+    rows = []
+    for i in which:
+        sim = so.build_sim(cfg, W["vels"][i], dt=W["dt"])
+        assert sim.nt == W["nt"]
+        ref = so.forward_adjoint(sim, yy, W["sigma"])
+        s = specs[i]
+        rows.append((rel(s.rec.cpu().numpy(), ref["clean"]), rel(s.grad.cpu().numpy(), ref["dJ_dv"]),
+                     abs(float(s.loglik.item()) - ref["loglik"]) / abs(ref["loglik"])))
+    e = np.array(rows).max(axis=0)
+    return {"models": list(which), "seis_rel_l2": float(e[0]), "grad_rel_l2": float(e[1]),
+            "loglik_rel": float(e[2]), "tolerance": 1e-4, "pass": bool((e <= 1e-4).all()),
+            "oracle": "float64 CPU restatement of the reference path, full 3000 steps",
+            "wall_s": time.perf_counter() - t0}
 
 
 def main():
@@ -555,6 +642,9 @@ def main():
     ap.add_argument("--serve-slots", type=int, default=256)
     ap.add_argument("--serve-cap-gb", type=float, default=150.0)
     ap.add_argument("--serve-ticks", type=int, default=32)
+    ap.add_argument("--clocks-log", default="", help="nvidia-smi clock samples (default: a temp file)")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="default workload: skip the parity, single, uneven and serving legs")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
@@ -616,8 +706,7 @@ def main():
     shape_used = batch.last_shape
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     step_ms, tick_ms = [], []
-    clocks = Clocks(os.path.join(HERE, "gpurun_out", f"clocks_r{rank}.csv") if os.path.isdir(
-        os.path.join(HERE, "gpurun_out")) else f"/tmp/clocks_r{rank}.csv")
+    clocks = Clocks(args.clocks_log or os.path.join(tempfile.gettempdir(), f"mun_b200_clocks_r{rank}.csv"))
     barrier()
     torch.cuda.synchronize()
     with clocks:
@@ -636,8 +725,9 @@ def main():
     # node-ticks of each kind per step: every group runs nt adjoint ticks, a read-out and
     # a scale tick; its remaining ticks are forward or replay ticks
     fwd_like = ticks_per_step - groups_used * (W["nt"] + 2)
-    kern_bytes = W["npoints"] * (n // groups_used) * (
-        BYTES_PER_NODE_FWD_TICK * fwd_like + BYTES_PER_NODE_ADJ_TICK * groups_used * W["nt"])
+    # algorithmic bytes of the step's tick launches: 56 B per node-step (replay ticks are
+    # overhead and carry none)
+    kern_bytes = BYTES_PER_NODE_STEP_FWDADJ * W["npoints"] * W["nt"] * n
     tick_loop_ms = float(np.mean(tick_ms))
     ms = max_over_ranks(ms, world, dev)
     status = torch.cat([s.status for s in specs]).max().item()
@@ -700,6 +790,24 @@ def main():
             TRAFFIC_B_PER_NODE["fwd"] * fwd_like + TRAFFIC_B_PER_NODE["adj"] * groups_used * W["nt"]
         ) / ticks_per_step
 
+    # ---------------- parity of two of the models against the float64 oracle (host)
+    parity = None
+    if rank == 0 and not args.no_extras:
+        parity = parity_leg(W, specs, y, [0, n - 1])
+
+    # ---------------- compact runs of the other workloads (device-timed, one solve set each)
+    extras = {}
+    # the batches' arenas (the 256-model step keeps ~128 GB) go back before the other legs
+    del batch, pbatch
+    import gc
+    gc.collect()
+    torch.cuda.synchronize()
+    torch.cuda.empty_cache()
+    if rank == 0 and not args.no_extras:
+        extras["single"] = run_single(args, steps=2, warmup=1, cpu_sample=0, emit=False)
+        extras["uneven"] = run_uneven(args, steps=1, warmup=1, plain=4, cpu_sample=0, emit=False)
+        extras["serving"] = run_serving(args, requests=100, emit=False)
+
     cpu = None
     if rank == 0 and not args.no_cpu:
         threads = os.cpu_count() or 1
@@ -714,9 +822,10 @@ def main():
             "metric": "SEM fwd+adjoint solves/s (batched vs plain, same GPU, <=1e-4 rel); p50/p99 ms",
             "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f32 state and gradient accumulation / f64 misfit", "data": "synthetic",
-            "config": {"workload": "batched ELBO sampling (256 models, 100x50 el, N=4, 80601 nodes, "
-                                   "3000 steps, 100 receivers)",
+            "vs_baseline": None,
+            "dtype": "f32 state / f64 gradient time-sum (f32 partials of <=16 ticks folded into f64) / f64 misfit",
+            "data": "synthetic",
+            "config": {"workload": WORKLOAD_ELBO,
                        "models_per_gpu": n, "nodes": W["npoints"], "nt": W["nt"],
                        "kernel": kernel_used, "shape (tile_ex, tile_ez, strip_bands)": shape_used,
                        "graph_chunk": args.graph_chunk,
@@ -734,18 +843,22 @@ def main():
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic, "peak_kind": pk_kind,
                          "kernel": f"sem_{kernel_used}_kernel<4>",
+                         "bytes_per_node_step": BYTES_PER_NODE_STEP_FWDADJ,
                          "bytes_per_node": {"forward_tick": BYTES_PER_NODE_FWD_TICK,
                                             "adjoint_tick": BYTES_PER_NODE_ADJ_TICK},
+                         "kernel_bytes_per_node": IMPL_BYTES_PER_NODE,
                          "launch_us_avg": 1e3 * tick_loop_ms / ticks_per_step,
                          "ticks_per_step": ticks_per_step, "forward_like_ticks": fwd_like,
-                         "note": "algorithmic bytes of the step's tick launches over the CUDA-"
-                                 "event time of the tick loops (one tick-kernel launch per tick, "
-                                 "chained by programmatic dependent launch); traffic = ncu DRAM "
-                                 "bytes per launch",
+                         "note": "algorithmic bytes (56 per fwd+adj node-step) of the step's tick "
+                                 "launches over the CUDA-event time of the tick loops (one "
+                                 "tick-kernel launch per tick, chained by programmatic dependent "
+                                 "launch); traffic = ncu DRAM bytes per launch",
                          "step_level": {"bytes_per_node_step": BYTES_PER_NODE_STEP_FWDADJ,
                                         "achieved": step_achieved,
                                         "frac": step_achieved / peak}},
             "cpu_baseline": cpu,
+            "parity": parity,
+            **extras,
             "gpu_launches": int(launches_per_step * args.steps),
             "status": int(status),
             "clocks": clocks.summary(local),

@@ -179,12 +179,12 @@ int sem_selftest_wait(int32_t which, int32_t* status_out);
  * receiver sums must fit in 32 MiB, about 1.9 million mesh nodes; larger meshes
  * return SEM_ERR_ARG with the required size in sem_last_error().
  *
- * The first call on a device looks up the array's device address
- * (cudaGetSymbolAddress) with that device current; make that first call before any
- * stream capture.  All calls share the one array and it keeps the last call's
- * contents (the call clears what must start at zero): calls that overlap on the GPU,
- * from different streams or threads, race and give wrong results.  status_out
- * (device, may be NULL) receives SEM_OK or SEM_ERR_NONFINITE. */
+ * sem_plan_create looks up the array's device address (cudaGetSymbolAddress) with
+ * the plan's device current and keeps it in the plan, so this call looks up and loads
+ * nothing.  All calls share the one array and it keeps the last call's contents (the
+ * call clears what must start at zero): calls that overlap on the GPU, from different
+ * streams or threads, race and give wrong results.  status_out (device, may be NULL)
+ * receives SEM_OK or SEM_ERR_NONFINITE. */
 int sem_forward_noalloc(const sem_plan_t* plan, const double* velocity, float* rec_out,
                         int32_t* status_out, void* stream);
 

@@ -12,7 +12,8 @@
 //   1/(omega dt) (about 10-20x larger seismogram error, measured).
 //   Adjoint step (core.py:1252-1275): the same recurrence run backwards with the
 //   source R^T r_it / sigma^2, no sponge (or the sponge, in exact mode), and the
-//   per-step sensitivity of core.py:49-85 accumulated in float32 (see sens_increment).
+//   per-step sensitivity of core.py:49-85 summed over time in float64 (float32 partial
+//   sums of at most 16 ticks folded into a float64 field; see kGradFold).
 //
 // Operator structure used here.  With rectangular affine elements and GLL
 // collocation, Gx = (2/dx) kron(L,D), Gz = (2/dz) kron(D,L) with L diagonal
@@ -105,7 +106,9 @@ struct SolveDev {
   float* ring;  // k+1 fields: b at t = j*k .. j*k+k of the segment being replayed
   float* L;     // 2 fields: adjoint lambda ping-pong
   float* Mu;    // 1 field: adjoint increment (in place)
-  float* grad;  // 1 field: dJ/dc^2 (times the adjoint scale) accumulated over time
+  float* grad;     // 1 field: float32 partial sum of dJ/dc^2 (times the adjoint scale)
+                   //   over at most kGradFold adjoint ticks
+  double* grad64;  // float64 field (2 float slots): the partial sums folded over time
   // operators and tables
   const float* D;     // (N+1)^2
   const float* beta;  // N+1
@@ -208,12 +211,23 @@ __host__ __device__ inline long long smem_floats(int N, int tex, int tez, bool a
 
 
 // The zero-lag sensitivity increment of one node, R_z S_x + R_x S_z, rounded the same way
-// in every kernel.  It is summed over the adjoint ticks in float32 (__fadd_rn in both
-// kernels): against float64 accumulation of the same increments that adds 1e-8 to 1e-6
-// relative error over 200 to 2000 ticks, far below the float32 wavefield's own.
+// in every kernel.
 __device__ __forceinline__ float sens_increment(float Rzv, float SX, float Rxv, float SZ) {
   return __fmaf_rn(Rzv, SX, __fmul_rn(Rxv, SZ));
 }
+// Time-sum of the gradient: the increments of at most kGradFold consecutive adjoint ticks
+// are added in a float32 partial sum (one __fadd_rn per node and tick), which is folded
+// into the float64 accumulator on the ticks with (t - it0) % kGradFold == 0 (__dadd_rn);
+// the last gradient tick, t = it0, is one of them.  A partial starts from zero on the
+// tick after a fold and on the first gradient tick (t = it1 - 1), so it is never read
+// there.  Per node and adjoint tick that moves 8 bytes plus a 16-byte float64
+// read-modify-write every kGradFold ticks, and adds a few 1e-8 relative error against
+// float64 accumulation of the same increments.
+constexpr int kGradFold = 16;
+__device__ __forceinline__ bool grad_partial_starts(const SolveDev& s, int t) {
+  return t == s.it1 - 1 || (t - s.it0) % kGradFold == kGradFold - 1;
+}
+__device__ __forceinline__ bool grad_folds(const SolveDev& s, int t) { return (t - s.it0) % kGradFold == 0; }
 // Sensitivity of one segment node, beta_a (D w)_a (D lambda)_a, multiplied left to right.
 __device__ __forceinline__ float sens_product(float beta, float dw, float du) {
   return __fmul_rn(__fmul_rn(beta, dw), du);
@@ -347,7 +361,7 @@ __device__ __forceinline__ void tile_tick(const SolveDev& S, const int act, cons
     p_v = vin[g0];
     p_ix = __ldg(S.tx + gx); p_Rx = __ldg(S.tx + S.nxg + gx); p_dx = __ldg(S.tx + 2 * S.nxg + gx);
     p_iz = __ldg(S.tz + gz); p_Rz = __ldg(S.tz + S.nzg + gz); p_dz = __ldg(S.tz + 2 * S.nzg + gz);
-    if (adj && t >= S.it0 && t < S.it1) p_g = S.grad[g0];
+    if (adj && t >= S.it0 && t < S.it1 && !grad_partial_starts(S, t)) p_g = S.grad[g0];
   }
   // the same for the misfit terms of each warp's first receiver (forward ticks)
   const int rec_m = t - ((S.flags & F_SHIFT) ? 1 : 0);
@@ -573,6 +587,8 @@ __device__ __forceinline__ void tile_tick(const SolveDev& S, const int act, cons
   // ---------------- owned nodes: assemble, Newmark, sponge, source / sensitivity
   const bool damp = (act != A_ADJ) || (S.flags & F_EXACT);
   const bool grad_on = adj && t >= S.it0 && t < S.it1;
+  const bool g_start = grad_on && grad_partial_starts(S, t);
+  const bool g_fold = grad_on && grad_folds(S, t);
   bool bad = false;
   for (int w = threadIdx.x; w < nro * nco; w += nthr) {
     const int cc = w % nco, r = w / nco;
@@ -627,7 +643,14 @@ __device__ __forceinline__ void tile_tick(const SolveDev& S, const int act, cons
       if (gx == S.src_gx && gz == S.src_gz) extra = S.src_term[t];
     } else {
       extra = have_inj ? sacc[r * nco + cc] : 0.f;
-      if (grad_on) S.grad[g] = __fadd_rn(first ? p_g : S.grad[g], sens_increment(Rzv, SX, Rxv, SZ));
+      if (grad_on) {
+        const float gprev = g_start ? 0.f : (first ? p_g : S.grad[g]);
+        const float gnew = __fadd_rn(gprev, sens_increment(Rzv, SX, Rxv, SZ));
+        if (g_fold)
+          S.grad64[g] = __dadd_rn(S.grad64[g], (double)gnew);
+        else
+          S.grad[g] = gnew;
+      }
     }
     float res, vres;
     advance_node(adj, damp, b, v, X, Z, ixv, Rxv, dxv, izv, Rzv, dzv, extra, res, vres);
@@ -998,6 +1021,9 @@ __device__ __forceinline__ void strip_tick(const SolveDev& S, const int act, con
 
   const bool damp = !ADJ || (S.flags & F_EXACT);
   const bool grad_on = ADJ && t >= S.it0 && t < S.it1;
+  const bool g_start = grad_on && grad_partial_starts(S, t);
+  const bool g_fold = grad_on && grad_folds(S, t);
+  double* const grad64p = S.grad64;
   const bool in_win = ADJ && t >= S.it0 && t < S.it1 && ((t - S.it0) % S.decim) == 0;
   const int ms = t - ((S.flags & F_SHIFT) ? 1 : 0);
   const bool rec_on = !ADJ && (act == A_FWD || act == A_FINAL) && ms >= 0 && ms < S.nt;
@@ -1046,7 +1072,7 @@ __device__ __forceinline__ void strip_tick(const SolveDev& S, const int act, con
     // before this band" after the band's barrier, so all threads leave at the same band
     // the owner's gradient rows of this band, loaded now and used in phase B
     float gpre[N];
-    if (ADJ && grad_on && owned && !halo) {
+    if (ADJ && grad_on && !g_start && owned && !halo) {
 #pragma unroll
       for (int a = 0; a < N; ++a) gpre[a] = gradp[gb + a * pitch];
     }
@@ -1269,14 +1295,22 @@ __device__ __forceinline__ void strip_tick(const SolveDev& S, const int act, con
           extra = (ez * N + a == src_row) ? src_val : 0.f;
         } else {
           extra = in_win ? sacc[a * NT + tid] : 0.f;
-          if (grad_on) gnew = __fadd_rn(a < N ? gpre[a < N ? a : 0] : gradp[g], sens_increment(Rzv, SX, Rxv, SZ));
+          if (grad_on) {
+            const float gprev = g_start ? 0.f : (a < N ? gpre[a < N ? a : 0] : gradp[g]);
+            gnew = __fadd_rn(gprev, sens_increment(Rzv, SX, Rxv, SZ));
+          }
         }
         float res, vres;
         advance_node(ADJ, damp, Bs[a * BW + sc], Vs[a * BW + sc], X, Z, ixv, Rxv, dxv, izv, Rzv,
                      dzv, extra, res, vres);
         out[g] = res;
         vout[g] = vres;
-        if (ADJ && grad_on) gradp[g] = gnew;
+        if (ADJ && grad_on) {
+          if (g_fold)
+            grad64p[g] = __dadd_rn(grad64p[g], (double)gnew);
+          else
+            gradp[g] = gnew;
+        }
         bad |= !isfinite(res);
       }
       zc = rz[N];
@@ -1456,7 +1490,7 @@ struct SolveIo {
   char* zp[8];            // workspace ranges that must start at zero (256-byte aligned,
   long long zb[8];        //   lengths multiples of 16 bytes)
   double* grad_out;       // or null
-  const float* gacc;      // dJ/dc^2 accumulator (float32, scaled)
+  const double* gacc;     // dJ/dc^2 accumulator (float64, scaled)
   const double* adj_scale;
   double inv_sigma2;
   const double* misfit;   // [nrec]
@@ -1492,7 +1526,7 @@ __global__ void batch_output_kernel(const SolveIo* __restrict__ io, int s0) {
     const double scale = s.inv_sigma2 / *s.adj_scale;  // exact: adj_scale is a power of two
     for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < s.npoints;
          i += (long long)gridDim.x * blockDim.x)
-      s.grad_out[i] = 2.0 * s.vel[i] * (double)s.gacc[s.pos[i]] * scale;
+      s.grad_out[i] = 2.0 * s.vel[i] * s.gacc[s.pos[i]] * scale;
   }
   if (blockIdx.x == 0 && threadIdx.x == 0) {
     if (s.loglik_out) {
@@ -1534,6 +1568,8 @@ struct sem_plan_s {
   int nelx, nelz, npol, nt, npoints, nxg, nzg, pitch, nrec, src_gx, src_gz, device;
   double dt;
   long long fstride;
+  char* noalloc_scratch = nullptr;  // device address of the allocation-free entry point's
+                                    // scratch array on this plan's device
   float* D = nullptr;
   float* beta = nullptr;
   float* tx = nullptr;
@@ -1774,7 +1810,7 @@ PersistFn persist_kernel_for(int N) {
 }
 
 struct Workspace {
-  long long c2, W, V, ckpt, ring, L, Mu, grad, misfit, status;  // byte offsets
+  long long c2, W, V, ckpt, ring, L, Mu, grad, grad64, misfit, status;  // byte offsets
   long long bytes;
 };
 
@@ -1830,6 +1866,7 @@ Workspace layout(const sem_plan_s* p, int flags, int k, int* nseg_out) {
     w.L = o; o += 2 * F;
     w.Mu = o; o += F;
     w.grad = o; o += F;
+    w.grad64 = o; o += 2 * F;  // float64 field
   }
   w.misfit = o; o += round_up((long long)(2 * p->nrec + 1) * 8, 256);  // misfit, rmax, scale
   w.status = o; o += 256;
@@ -1923,6 +1960,18 @@ int sem_plan_create(const sem_plan_desc_t* d, sem_plan_t** out) {
       sem_plan_destroy(p);
       return rc;
     }
+  }
+  {
+    // device address of sem_forward_noalloc's scratch array, taken here (set-up, this
+    // plan's device current) so that the entry point itself loads nothing and looks up
+    // nothing; the array's host-side name is not a device address
+    void* ptr = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
+    if (e != cudaSuccess) {
+      sem_plan_destroy(p);
+      return fail(SEM_ERR_CUDA, std::string("cudaGetSymbolAddress(scratch): ") + cudaGetErrorString(e));
+    }
+    p->noalloc_scratch = (char*)ptr;
   }
   *out = p;
   return SEM_OK;
@@ -2082,6 +2131,7 @@ static int run_group(sem_batch_t* b, const sem_solve_t* solves, int32_t n,
     d.L = (s.flags & SEM_F_ADJOINT) ? (float*)(a + ws[i].L) : nullptr;
     d.Mu = (s.flags & SEM_F_ADJOINT) ? (float*)(a + ws[i].Mu) : nullptr;
     d.grad = (s.flags & SEM_F_ADJOINT) ? (float*)(a + ws[i].grad) : nullptr;
+    d.grad64 = (s.flags & SEM_F_ADJOINT) ? (double*)(a + ws[i].grad64) : nullptr;
     d.D = p->D; d.beta = p->beta; d.tx = p->tx; d.tz = p->tz; d.src_term = p->src_term;
     d.rec_base = p->rec_base; d.rec_w = p->rec_w;
     d.rec_tile_off = L.rec_off; d.rec_tile_ids = L.rec_ids;
@@ -2150,11 +2200,11 @@ static int run_group(sem_batch_t* b, const sem_solve_t* solves, int32_t n,
       zero(ws[i].ckpt, 2 * F);
       zero(ws[i].ring, F);
       zero(ws[i].L, 3 * F);      // L[0], L[1], Mu
-      zero(ws[i].grad, F);
+      zero(ws[i].grad, 3 * F);   // float32 partial and float64 accumulator
     }
     zero(ws[i].misfit, ws[i].status - ws[i].misfit + 256);
     io.grad_out = ((s.flags & SEM_F_ADJOINT) && s.grad_out) ? s.grad_out : nullptr;
-    io.gacc = (const float*)(a + ws[i].grad);
+    io.gacc = (const double*)(a + ws[i].grad64);
     io.adj_scale = (const double*)(a + ws[i].misfit) + 2 * p->nrec;
     io.inv_sigma2 = s.inv_sigma2;
     io.misfit = (const double*)(a + ws[i].misfit);
@@ -2553,24 +2603,9 @@ int sem_forward_noalloc(const sem_plan_t* p, const double* velocity, float* rec_
   int dev = -1;
   CUDA_TRY(cudaGetDevice(&dev));
   if (dev != p->device) return fail(SEM_ERR_ARG, "plan was created on another device");
-  // device address of the scratch array, looked up once per device
-  static std::mutex mu;
-  static std::map<int, char*> base_of;
-  char* base = nullptr;
-  {
-    std::lock_guard<std::mutex> lk(mu);
-    auto it = base_of.find(dev);
-    if (it == base_of.end()) {
-      void* ptr = nullptr;
-      cudaError_t e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
-      if (e != cudaSuccess)
-        return fail(SEM_ERR_CUDA, std::string("cudaGetSymbolAddress(scratch): ") + cudaGetErrorString(e));
-      base_of[dev] = (char*)ptr;
-      base = (char*)ptr;
-    } else {
-      base = it->second;
-    }
-  }
+  // device address of the scratch array on this device, looked up when the plan was made
+  char* const base = p->noalloc_scratch;
+  if (!base) return fail(SEM_ERR_ARG, "plan has no scratch address");
   // receiver lists of the default tiles were built when the plan was created
   sem_plan_s::Lists L{};
   {
@@ -2598,6 +2633,7 @@ int sem_forward_noalloc(const sem_plan_t* p, const double* velocity, float* rec_
   SolveDev d{};
   d.nelx = p->nelx; d.nelz = p->nelz; d.nxg = p->nxg; d.nzg = p->nzg; d.pitch = p->pitch;
   d.tiles_x = ntx; d.tiles_z = ntz; d.tile_base = 0;
+  d.zchunk = p->nelz;
   d.nt = p->nt; d.k = 2; d.nseg = 1; d.flags = 0; d.start_tick = 0;
   d.it0 = 0; d.it1 = p->nt; d.decim = 1;
   d.src_gx = p->src_gx; d.src_gz = p->src_gz; d.nrec = p->nrec;
@@ -2623,10 +2659,22 @@ int sem_forward_noalloc(const sem_plan_t* p, const double* velocity, float* rec_
   KernelFn fn = kernel_for(p->npol);
   const size_t smem = (size_t)smem_floats(p->npol, kNoAllocTile, kNoAllocTile, false) * sizeof(float);
   CUDA_TRY(raise_smem_limit((const void*)fn, smem));
+  // ticks: the tick number is an argument and consecutive ticks chain by programmatic
+  // dependent launch, as on sem_run's plain-launch path
   for (int tick = 0; tick < p->nt; ++tick) {
-    fn<<<ntiles, 256, smem, stream>>>((const SolveDev*)(base + o_desc), (const int*)(base + o_cta),
-                                      (const int*)(base + o_tick), kNoAllocTile, kNoAllocTile, 0);
-    tick_advance_kernel<<<1, 1, 0, stream>>>((int*)(base + o_tick));
+    cudaLaunchConfig_t lc = {};
+    lc.gridDim = dim3((unsigned)ntiles);
+    lc.blockDim = dim3(256);
+    lc.dynamicSmemBytes = smem;
+    lc.stream = stream;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = SEM_PDL ? 1 : 0;
+    lc.attrs = at;
+    lc.numAttrs = 1;
+    const int* no_counter = nullptr;
+    CUDA_TRY(cudaLaunchKernelEx(&lc, fn, (const SolveDev*)(base + o_desc), (const int*)(base + o_cta),
+                                no_counter, kNoAllocTile, kNoAllocTile, tick));
   }
   if (status_out) copy_status_kernel<<<1, 32, 0, stream>>>((const int*)(base + o_st), status_out);
   CUDA_TRY(cudaGetLastError());
@@ -2713,11 +2761,11 @@ SolveIo solve_io(const sem_solve_t& s, const Workspace& ws, char* a) {
     zero(ws.ckpt, 2 * F);
     zero(ws.ring, F);
     zero(ws.L, 3 * F);  // L[0], L[1], Mu
-    zero(ws.grad, F);
+    zero(ws.grad, 3 * F);  // float32 partial and float64 accumulator
   }
   zero(ws.misfit, ws.status - ws.misfit + 256);
   io.grad_out = ((s.flags & SEM_F_ADJOINT) && s.grad_out) ? s.grad_out : nullptr;
-  io.gacc = (const float*)(a + ws.grad);
+  io.gacc = (const double*)(a + ws.grad64);
   io.adj_scale = (const double*)(a + ws.misfit) + 2 * p->nrec;
   io.inv_sigma2 = s.inv_sigma2;
   io.misfit = (const double*)(a + ws.misfit);
@@ -3000,6 +3048,7 @@ int sem_engine_step(sem_engine_t* e, void* stream_v) {
     d.L = adj ? (float*)(a + j->ws.L) : nullptr;
     d.Mu = adj ? (float*)(a + j->ws.Mu) : nullptr;
     d.grad = adj ? (float*)(a + j->ws.grad) : nullptr;
+    d.grad64 = adj ? (double*)(a + j->ws.grad64) : nullptr;
     d.D = p->D; d.beta = p->beta; d.tx = p->tx; d.tz = p->tz; d.src_term = p->src_term;
     d.rec_base = p->rec_base; d.rec_w = p->rec_w;
     d.rec_tile_off = L.rec_off; d.rec_tile_ids = L.rec_ids;

@@ -1,10 +1,9 @@
 """Generate golden fixtures by running MUN's own ``sem_waveform`` package.
 
-Run in a container that has the MUN sources (default location below, override with
-``MUN_REFERENCE=/path``); the fixtures it writes are committed so that nothing else
-needs the reference at run time:
+Run where the MUN sources are, with their root in ``MUN_REFERENCE``; the fixtures it
+writes are committed so that nothing else needs the reference at run time:
 
-    python tests/golden/make_golden.py
+    MUN_REFERENCE=/path/to/MUN python tests/golden/make_golden.py [case ...]
 
 ``matplotlib`` and ``imageio`` are not installed here.  The reference imports them at
 module level (``core.py:7,10``) but its solver never calls them; the only arithmetic
@@ -42,7 +41,6 @@ from pathlib import Path as _P
 
 import numpy as np
 
-REF = _P(os.environ.get("MUN_REFERENCE", "/root/reference"))
 OUT = _P(__file__).resolve().parent
 
 
@@ -284,6 +282,10 @@ def _save(name, cfg, data):
 
 
 def main():
+    global REF
+    if not os.environ.get("MUN_REFERENCE"):
+        sys.exit("set MUN_REFERENCE to the root of the MUN sources")
+    REF = _P(os.environ["MUN_REFERENCE"])
     _install_stubs()
     import torch
     torch.set_num_threads(max(1, os.cpu_count() or 1))

@@ -1,8 +1,11 @@
-"""The kernels accumulate the sensitivity in float32 (one __fadd_rn per node and adjoint
-tick).  This checks the numerical argument on the CPU: the float64 oracle's per-tick
-node increments, rounded to float32 as the kernels form them and summed in float32, stay
-within a few 1e-7 of float64 accumulation of the same increments (the parity tolerance
-is 1e-4, the float32 wavefield's own error about 1e-5)."""
+"""The kernels sum the sensitivity over the adjoint ticks in float64: each tick's node
+increment (float32, as the kernels form it) is added to a float32 partial sum, which is
+folded into a float64 accumulator on the ticks with (t - it0) % 16 == 0; a partial
+starts from zero after each fold and on the first gradient tick.  This checks the
+numerical argument on the CPU with the float64 oracle's increments: the folded sum stays
+within a few 1e-8 of float64 accumulation of the same increments (relative L2), and
+within a few 1e-6 node by node on the nodes that carry the gradient (the parity tolerance is 1e-4, the float32 wavefield's
+own error about 1e-5).  A plain float32 running sum is shown beside it for scale."""
 import numpy as np
 import pytest
 import torch
@@ -54,19 +57,45 @@ def _accumulations(name):
     lam_c = torch.zeros(P, dtype=torch.float64)
     acc64 = torch.zeros(P, dtype=torch.float64)
     acc32 = torch.zeros(P, dtype=torch.float32)
+    fold64 = torch.zeros(P, dtype=torch.float64)
+    part32 = torch.zeros(P, dtype=torch.float32)
+    it0, it1 = 0, nt
     for it in range(nt - 1, -1, -1):
         rhs = torch.matmul(RT, rs[:, it]) - torch.matmul(K, lam_c)
         lam_p = 2.0 * lam_c - lam_n + dt2 * (Minv * rhs)
         inc32 = (sensitivity_step(hist[it], lam_c, conn_t, Gx_t, Gz_t, S_t, w2D_t, P) * scale).float()
         acc64 += inc32.double()
         acc32 += inc32
+        if it == it1 - 1 or (it - it0) % FOLD == FOLD - 1:
+            part32 = inc32.clone()
+        else:
+            part32 = part32 + inc32
+        if (it - it0) % FOLD == 0:
+            fold64 += part32.double()
+            part32 = torch.zeros(P, dtype=torch.float32)
         lam_n, lam_c = lam_c, lam_p
-    return acc64.numpy(), acc32.double().numpy()
+    return acc64.numpy(), fold64.numpy(), acc32.double().numpy()
 
 
-@pytest.mark.parametrize("name", ["inject_n1", "inject_n3"])
-def test_float32_accumulation_error_is_negligible(name):
-    a64, a32 = _accumulations(name)
-    rel = float(np.linalg.norm(a32 - a64) / np.linalg.norm(a64))
-    print(f"{name}: float32 vs float64 accumulation of the same increments {rel:.2e}")
-    assert rel < 2e-6
+FOLD = 16
+
+
+def _errors(ref, got):
+    rel_l2 = float(np.linalg.norm(got - ref) / np.linalg.norm(ref))
+    # node by node, on the nodes carrying at least 1e-3 of the largest |gradient|
+    big = np.abs(ref) >= 1e-3 * np.abs(ref).max()
+    rel_node = float((np.abs(got - ref)[big] / np.abs(ref)[big]).max())
+    return rel_l2, rel_node
+
+
+@pytest.mark.parametrize("name", ["inject_n1", "inject_n3", "layered_cfg0"])
+def test_folded_float64_accumulation_error_is_negligible(name):
+    a64, fold, a32 = _accumulations(name)
+    l2, node = _errors(a64, fold)
+    l2_32, node_32 = _errors(a64, a32)
+    print(f"{name}: folded float64 vs float64 accumulation rel. L2 {l2:.2e}, max per node {node:.2e} "
+          f"(plain float32 running sum: {l2_32:.2e}, {node_32:.2e})")
+    # per node the error is set by cancellation in a node's time-sum (increments of both
+    # signs), which the plain float32 sum shows 2-8 times larger
+    assert l2 < 1e-7 and node < 2e-5
+    assert l2 < l2_32

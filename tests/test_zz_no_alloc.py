@@ -7,7 +7,11 @@ hit cudaMalloc's implicit device synchronisation, or an embedding that brings it
 allocator.  ``sem_forward_noalloc`` serves them from a fixed scratch array compiled
 into the library.  Both calls go through the C ABI.  Two calls in a row with different
 velocities must each match the allocating path, which shows that the second call does
-not see the state the first call left in the shared scratch.
+not see the state the first call left in the shared scratch.  The tile kernel's
+arithmetic per node does not depend on the tile shape, so the traces are bitwise those
+of the allocating call; they are also checked against the reference's own traces (the
+golden ``rec_run``) at the parity tolerance, and the device's free memory must not
+change across a call.
 """
 import ctypes as C
 
@@ -62,11 +66,33 @@ def test_no_alloc_forward_matches_allocating_entry_point_twice():
                 assert torch.isfinite(a).all()
                 err = rel_l2(a.cpu().numpy(), b.cpu().numpy())
                 assert err <= TOL, (name, err)
+                assert torch.equal(a, b), name
+            # the reference's own traces of the first model
+            err_ref = rel_l2(_noalloc(lib, plan, v1).cpu().numpy(), g["rec_run"])
+            assert err_ref <= TOL, (name, err_ref)
             # and the traces of the two models differ (the test would notice stale state)
             assert rel_l2(_noalloc(lib, plan, v1).cpu().numpy(),
                           _noalloc(lib, plan, v2).cpu().numpy()) > 1e-3
     finally:
         lib.sem_batch_destroy(batch)
+
+
+def test_no_alloc_call_takes_no_device_memory():
+    lib = _lib.load()
+    g = load("inject_n3")
+    plan = plan_for(g["config"], g["dt_run"], g["nt_run"])
+    v = dev(g["velocity"])
+    rec = torch.empty((plan.nt, plan.nrec), dtype=torch.float32, device="cuda")
+    st = torch.empty((1,), dtype=torch.int32, device="cuda")
+    args = (plan.handle, C.c_void_p(v.data_ptr()), C.c_void_p(rec.data_ptr()), C.c_void_p(st.data_ptr()))
+    _lib.check(lib.sem_forward_noalloc(*args, _stream()))  # warm-up: kernels loaded
+    torch.cuda.synchronize()
+    free0 = torch.cuda.mem_get_info()[0]
+    for _ in range(2):
+        _lib.check(lib.sem_forward_noalloc(*args, _stream()))
+    torch.cuda.synchronize()
+    assert torch.cuda.mem_get_info()[0] == free0
+    assert int(st.item()) == 0
 
 
 def test_no_alloc_rejects_meshes_beyond_the_scratch():
