@@ -71,6 +71,22 @@ typedef struct {
   int32_t nrec;
   const int32_t* rec_base;  /* [nrec*2] (gx0,gz0) first node of the receiver element  */
   const double* rec_w;      /* [nrec*(npol+1)^2] Lagrange weights, index j*(npol+1)+i */
+  /* Boundary mode.  0: the reference's sponge (its decay is the third row of tab_x and
+   * tab_z).  1: an extension without counterpart in the reference: first-order Stacey
+   * absorbing edges on the sides and the bottom and a free surface (u = 0) on the top row;
+   * tab_x / tab_z then carry no decay (third rows 1).  The forward becomes
+   *   (1 + a) u+ = 2 u - (1 - a) u- + dt^2 M^-1 (f - K u),  a = c alpha on the absorbing
+   * edges, and the adjoint is its exact discrete adjoint: the same recurrence run
+   * backwards, with a boundary-impedance term in the gradient (from d a / d c): at each
+   * adjoint step the node of slot i adds (gamma_i / c_i) lambda_i (u_i(t+1) - u_i(t-1))
+   * to the sensitivity of c_i^2.
+   * Slots: (gx = 0, gz) -> gz, (gx = nxg-1, gz) -> nzg + gz, (gx, gz = nzg-1) -> 2 nzg + gx;
+   * bnd_n = 2 nzg + nxg.  Ignored in mode 0. */
+  int32_t boundary_mode;
+  int32_t bnd_n;
+  const int32_t* bnd_ref;   /* [bnd_n] reference node index of the slot's node, or -1   */
+  const double* bnd_alpha;  /* [bnd_n] dt beta / (2 M): a = c alpha                     */
+  const double* bnd_gamma;  /* [bnd_n] beta / (4 dt): impedance-term factor g = gamma/c */
 } sem_plan_desc_t;
 
 /* One solve inside sem_run.  Device pointers unless stated. */

@@ -22,7 +22,9 @@ class PlanDesc(C.Structure):
                 ("gll_beta", C.POINTER(C.c_double)), ("tab_x", C.POINTER(C.c_double)),
                 ("tab_z", C.POINTER(C.c_double)), ("src_term", C.POINTER(C.c_double)),
                 ("src_gx", C.c_int32), ("src_gz", C.c_int32), ("nrec", C.c_int32),
-                ("rec_base", C.POINTER(C.c_int32)), ("rec_w", C.POINTER(C.c_double))]
+                ("rec_base", C.POINTER(C.c_int32)), ("rec_w", C.POINTER(C.c_double)),
+                ("boundary_mode", C.c_int32), ("bnd_n", C.c_int32), ("bnd_ref", C.POINTER(C.c_int32)),
+                ("bnd_alpha", C.POINTER(C.c_double)), ("bnd_gamma", C.POINTER(C.c_double))]
 
 
 class Solve(C.Structure):

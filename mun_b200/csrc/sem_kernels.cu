@@ -97,6 +97,8 @@ struct SolveDev {
   int it0, it1, decim;
   int src_gx, src_gz;
   int nrec;
+  int bnd_n;          // Stacey / free-surface mode: boundary slots (0: the sponge)
+  int bnd_pitch;      // floats per row of the boundary tables (bnd_n rounded up to 64)
   long long fstride;  // floats per state field
   // fields
   const float* c2;
@@ -132,6 +134,11 @@ struct SolveDev {
   // the tensor map of the band loads over it (device memory; null for the tile kernel)
   const float* ws;
   const void* tmap;
+  // Stacey mode: per slot e1 = (1 - a) / (1 + a), e2 = 1 / (1 + a) and the impedance-term
+  // factor g (rows of bnd_pitch floats), and, for adjoint solves, the boundary nodes' b_t
+  // for t = 0 .. nt (row t), written by forward and replay ticks
+  const float* bnd_coef;
+  float* bnd_hist;
 };
 
 __device__ __forceinline__ void decode(const SolveDev& s, int sig, int& act, int& t, int& seg) {
@@ -261,6 +268,37 @@ __device__ __forceinline__ void advance_node(bool adj, bool damp, float b, float
     vout = wv;
     bout = __fadd_rn(b, wv);
   }
+}
+
+// Stacey / free-surface mode (an extension; the reference has only the sponge).  Slot of a
+// node of the absorbing edges (x = xmin, x = xmax, z = zmax) in the boundary tables, or -1.
+__device__ __forceinline__ int bnd_slot(const SolveDev& s, int gx, int gz) {
+  if (gx == 0) return gz;
+  if (gx == s.nxg - 1) return s.nzg + gz;
+  if (gz == s.nzg - 1) return 2 * s.nzg + gx;
+  return -1;
+}
+// One node of an absorbing edge: (1 + a) u+ = 2 u - (1 - a) u- + F in the (b, v) state,
+//   w = e1 v + e2 F,  v' = w,  b' = b + w   (e1 = (1 - a) / (1 + a), e2 = 1 / (1 + a)),
+// F = extra - P K (forward) or P (extra - K) (adjoint, the same recurrence run backwards);
+// there is no sponge in this mode.  Shared by both kernels.
+__device__ __forceinline__ void advance_node_stacey(bool adj, float b, float v, float X, float Z,
+                                                    float ixv, float Rxv, float izv, float Rzv,
+                                                    float extra, float e1, float e2, float& bout,
+                                                    float& vout) {
+  const float P = __fmul_rn(ixv, izv);
+  const float Kv = __fmaf_rn(Rzv, X, __fmul_rn(Rxv, Z));
+  const float F = !adj ? __fmaf_rn(-P, Kv, extra) : __fmul_rn(P, __fsub_rn(extra, Kv));
+  const float w = __fmaf_rn(e1, v, __fmul_rn(e2, F));
+  vout = w;
+  bout = __fadd_rn(b, w);
+}
+// The gradient's boundary-impedance increment (from d a / d c) of slot k at adjoint tick
+// t <= nt - 2, added to the sensitivity of c^2:  g lambda (b_{t+2} - b_t).
+__device__ __forceinline__ float bnd_sens(const SolveDev& s, int k, int t, float lam) {
+  const long long BP = s.bnd_pitch;
+  const float du = __fsub_rn(s.bnd_hist[(long long)(t + 2) * BP + k], s.bnd_hist[(long long)t * BP + k]);
+  return __fmul_rn(__fmul_rn(s.bnd_coef[2 * BP + k], lam), du);
 }
 
 // ----------------------------------------------------------------------------
@@ -589,6 +627,7 @@ __device__ __forceinline__ void tile_tick(const SolveDev& S, const int act, cons
   const bool grad_on = adj && t >= S.it0 && t < S.it1;
   const bool g_start = grad_on && grad_partial_starts(S, t);
   const bool g_fold = grad_on && grad_folds(S, t);
+  const bool stc = S.bnd_n > 0;
   bool bad = false;
   for (int w = threadIdx.x; w < nro * nco; w += nthr) {
     const int cc = w % nco, r = w / nco;
@@ -638,6 +677,7 @@ __device__ __forceinline__ void tile_tick(const SolveDev& S, const int act, cons
     const long long g = (long long)gz * S.pitch + gx;
     const float b = su[(gz - gzs) * SW + (gx - gxs)];
     const float v = first ? p_v : vin[g];
+    const int bk = (stc && gz > 0) ? bnd_slot(S, gx, gz) : -1;
     float extra = 0.f;
     if (!adj) {
       if (gx == S.src_gx && gz == S.src_gz) extra = S.src_term[t];
@@ -645,7 +685,9 @@ __device__ __forceinline__ void tile_tick(const SolveDev& S, const int act, cons
       extra = have_inj ? sacc[r * nco + cc] : 0.f;
       if (grad_on) {
         const float gprev = g_start ? 0.f : (first ? p_g : S.grad[g]);
-        const float gnew = __fadd_rn(gprev, sens_increment(Rzv, SX, Rxv, SZ));
+        float inc = sens_increment(Rzv, SX, Rxv, SZ);
+        if (bk >= 0 && t <= S.nt - 2) inc = __fadd_rn(inc, bnd_sens(S, bk, t, b));
+        const float gnew = __fadd_rn(gprev, inc);
         if (g_fold)
           S.grad64[g] = __dadd_rn(S.grad64[g], (double)gnew);
         else
@@ -653,7 +695,17 @@ __device__ __forceinline__ void tile_tick(const SolveDev& S, const int act, cons
       }
     }
     float res, vres;
-    advance_node(adj, damp, b, v, X, Z, ixv, Rxv, dxv, izv, Rzv, dzv, extra, res, vres);
+    if (stc && gz == 0) {  // free surface
+      res = 0.f;
+      vres = 0.f;
+    } else if (bk >= 0) {
+      const long long BP = S.bnd_pitch;
+      advance_node_stacey(adj, b, v, X, Z, ixv, Rxv, izv, Rzv, extra, S.bnd_coef[bk], S.bnd_coef[BP + bk],
+                          res, vres);
+      if (!adj && (S.flags & F_ADJ)) S.bnd_hist[(long long)(t + 1) * BP + bk] = res;
+    } else {
+      advance_node(adj, damp, b, v, X, Z, ixv, Rxv, dxv, izv, Rzv, dzv, extra, res, vres);
+    }
     vout[g] = vres;
     out[g] = res;
     bad |= !isfinite(res);
@@ -1024,6 +1076,7 @@ __device__ __forceinline__ void strip_tick(const SolveDev& S, const int act, con
   const bool g_start = grad_on && grad_partial_starts(S, t);
   const bool g_fold = grad_on && grad_folds(S, t);
   double* const grad64p = S.grad64;
+  const bool stc = S.bnd_n > 0;  // Stacey / free-surface mode
   const bool in_win = ADJ && t >= S.it0 && t < S.it1 && ((t - S.it0) % S.decim) == 0;
   const int ms = t - ((S.flags & F_SHIFT) ? 1 : 0);
   const bool rec_on = !ADJ && (act == A_FWD || act == A_FINAL) && ms >= 0 && ms < S.nt;
@@ -1289,20 +1342,34 @@ __device__ __forceinline__ void strip_tick(const SolveDev& S, const int act, con
         }
         const float izv = tzb[a], Rzv = tzb[8 + a], dzv = tzb[16 + a];
         const int g = gb + a * pitch;
+        const int gz = ez * N + a;
+        const int bk = (stc && gz > 0) ? bnd_slot(S, gx, gz) : -1;
         float extra;
         float gnew = 0.f;
         if (!ADJ) {
-          extra = (ez * N + a == src_row) ? src_val : 0.f;
+          extra = (gz == src_row) ? src_val : 0.f;
         } else {
           extra = in_win ? sacc[a * NT + tid] : 0.f;
           if (grad_on) {
             const float gprev = g_start ? 0.f : (a < N ? gpre[a < N ? a : 0] : gradp[g]);
-            gnew = __fadd_rn(gprev, sens_increment(Rzv, SX, Rxv, SZ));
+            float inc = sens_increment(Rzv, SX, Rxv, SZ);
+            if (bk >= 0 && t <= S.nt - 2) inc = __fadd_rn(inc, bnd_sens(S, bk, t, Bs[a * BW + sc]));
+            gnew = __fadd_rn(gprev, inc);
           }
         }
         float res, vres;
-        advance_node(ADJ, damp, Bs[a * BW + sc], Vs[a * BW + sc], X, Z, ixv, Rxv, dxv, izv, Rzv,
-                     dzv, extra, res, vres);
+        if (stc && gz == 0) {  // free surface
+          res = 0.f;
+          vres = 0.f;
+        } else if (bk >= 0) {
+          const long long BP = S.bnd_pitch;
+          advance_node_stacey(ADJ, Bs[a * BW + sc], Vs[a * BW + sc], X, Z, ixv, Rxv, izv, Rzv, extra,
+                              S.bnd_coef[bk], S.bnd_coef[BP + bk], res, vres);
+          if (!ADJ && (S.flags & F_ADJ)) S.bnd_hist[(long long)(t + 1) * BP + bk] = res;
+        } else {
+          advance_node(ADJ, damp, Bs[a * BW + sc], Vs[a * BW + sc], X, Z, ixv, Rxv, dxv, izv, Rzv,
+                       dzv, extra, res, vres);
+        }
         out[g] = res;
         vout[g] = vres;
         if (ADJ && grad_on) {
@@ -1498,6 +1565,13 @@ struct SolveIo {
   double* loglik_out;     // or null
   const int* st;          // workspace status word
   int* status_out;        // or null
+  // Stacey mode: per boundary slot the node's reference index and the plan's alpha and
+  // gamma; the set-up writes e1, e2 and g of this solve's velocity into bnd_coef
+  int bnd_n, bnd_pitch;
+  const int* bnd_ref;
+  const double* bnd_alpha;
+  const double* bnd_gamma;
+  float* bnd_coef;
 };
 
 // clears every solve's zero-start state and stages c^2 (row blockIdx.y = solve)
@@ -1513,6 +1587,21 @@ __global__ void batch_setup_kernel(const SolveIo* __restrict__ io, int s0) {
   for (long long i = t0; i < s.npoints; i += stride) {
     const double v = s.vel[i];
     s.c2[s.pos[i]] = (float)(v * v);
+  }
+  // Stacey mode: a = c alpha, e1 = (1 - a) / (1 + a), e2 = 1 / (1 + a), g = gamma / c
+  for (long long k = t0; k < s.bnd_n; k += stride) {
+    const int ref = s.bnd_ref[k];
+    float e1 = 0.f, e2 = 0.f, g = 0.f;
+    if (ref >= 0) {
+      const double c = s.vel[ref];
+      const double a = c * s.bnd_alpha[k];
+      e1 = (float)((1.0 - a) / (1.0 + a));
+      e2 = (float)(1.0 / (1.0 + a));
+      g = (float)(s.bnd_gamma[k] / c);
+    }
+    s.bnd_coef[k] = e1;
+    s.bnd_coef[s.bnd_pitch + k] = e2;
+    s.bnd_coef[2LL * s.bnd_pitch + k] = g;
   }
 }
 
@@ -1570,6 +1659,10 @@ struct sem_plan_s {
   long long fstride;
   char* noalloc_scratch = nullptr;  // device address of the allocation-free entry point's
                                     // scratch array on this plan's device
+  int bnd_n = 0;                    // Stacey mode: boundary slots (0: the sponge)
+  int* bnd_ref = nullptr;
+  double* bnd_alpha = nullptr;
+  double* bnd_gamma = nullptr;
   float* D = nullptr;
   float* beta = nullptr;
   float* tx = nullptr;
@@ -1811,8 +1904,11 @@ PersistFn persist_kernel_for(int N) {
 
 struct Workspace {
   long long c2, W, V, ckpt, ring, L, Mu, grad, grad64, misfit, status;  // byte offsets
+  long long bnd_coef, bnd_hist;  // Stacey mode (-1 when absent)
   long long bytes;
 };
+// floats per row of the boundary tables
+inline int bnd_pitch_of(const sem_plan_s* p) { return (p->bnd_n + 63) / 64 * 64; }
 
 // The strip kernel's band loads: one tiled tensor map per solve over its workspace seen as
 // [field slot][row][column] floats (c2, W, V, checkpoints, ring, L and Mu all start at
@@ -1870,6 +1966,12 @@ Workspace layout(const sem_plan_s* p, int flags, int k, int* nseg_out) {
   }
   w.misfit = o; o += round_up((long long)(2 * p->nrec + 1) * 8, 256);  // misfit, rmax, scale
   w.status = o; o += 256;
+  w.bnd_coef = w.bnd_hist = -1;
+  if (p->bnd_n > 0) {
+    const long long row = (long long)bnd_pitch_of(p) * 4;  // bytes, a multiple of 256
+    w.bnd_coef = o; o += 3 * row;                          // e1, e2, g
+    if (adj) { w.bnd_hist = o; o += (long long)(p->nt + 1) * row; }  // b_t of the slots
+  }
   w.bytes = o;
   *nseg_out = nseg;
   return w;
@@ -1954,6 +2056,26 @@ int sem_plan_create(const sem_plan_desc_t* d, sem_plan_t** out) {
     sem_plan_destroy(p);
     return rc;
   }
+  if (d->boundary_mode == 1) {
+    if (d->bnd_n != 2 * nzg + nxg || !d->bnd_ref || !d->bnd_alpha || !d->bnd_gamma) {
+      sem_plan_destroy(p);
+      return fail(SEM_ERR_ARG, "Stacey mode needs bnd_n = 2 nzg + nxg and the three boundary tables");
+    }
+    for (int k = 0; k < d->bnd_n; ++k)
+      if (d->bnd_ref[k] >= d->npoints) {
+        sem_plan_destroy(p);
+        return fail(SEM_ERR_ARG, "bnd_ref out of range");
+      }
+    p->bnd_n = d->bnd_n;
+    if ((rc = upload(&p->bnd_ref, d->bnd_ref, d->bnd_n)) || (rc = upload(&p->bnd_alpha, d->bnd_alpha, d->bnd_n)) ||
+        (rc = upload(&p->bnd_gamma, d->bnd_gamma, d->bnd_n))) {
+      sem_plan_destroy(p);
+      return rc;
+    }
+  } else if (d->boundary_mode != 0) {
+    sem_plan_destroy(p);
+    return fail(SEM_ERR_ARG, "boundary_mode must be 0 (sponge) or 1 (Stacey sides and bottom, free top)");
+  }
   {
     sem_plan_s::Lists L;  // lists of the default 8x8 tiles, used by sem_forward_noalloc
     if ((rc = get_lists(p, kNoAllocTile, kNoAllocTile, &L))) {
@@ -1981,6 +2103,7 @@ int sem_plan_destroy(sem_plan_t* p) {
   if (!p) return SEM_OK;
   cudaFree(p->D); cudaFree(p->beta); cudaFree(p->tx); cudaFree(p->tz); cudaFree(p->src_term);
   cudaFree(p->rec_base); cudaFree(p->rec_w); cudaFree(p->node_pos);
+  cudaFree(p->bnd_ref); cudaFree(p->bnd_alpha); cudaFree(p->bnd_gamma);
   for (auto& kv : p->lists) {
     cudaFree(kv.second.rec_off); cudaFree(kv.second.rec_ids);
     cudaFree(kv.second.inj_off); cudaFree(kv.second.inj_ids);
@@ -2143,6 +2266,9 @@ static int run_group(sem_batch_t* b, const sem_solve_t* solves, int32_t n,
     d.status = (int*)(a + ws[i].status);
     d.ws = (const float*)a;
     d.tmap = nullptr;
+    d.bnd_n = p->bnd_n; d.bnd_pitch = bnd_pitch_of(p);
+    d.bnd_coef = p->bnd_n ? (const float*)(a + ws[i].bnd_coef) : nullptr;
+    d.bnd_hist = ws[i].bnd_hist >= 0 ? (float*)(a + ws[i].bnd_hist) : nullptr;
     if (use_strip) {
       rc = encode_band_map(&b->h_tmaps[oi], a, p, field_slots(ws[i], p, s.flags & SEM_F_ADJOINT));
       if (rc) return rc;
@@ -2203,6 +2329,10 @@ static int run_group(sem_batch_t* b, const sem_solve_t* solves, int32_t n,
       zero(ws[i].grad, 3 * F);   // float32 partial and float64 accumulator
     }
     zero(ws[i].misfit, ws[i].status - ws[i].misfit + 256);
+    if (ws[i].bnd_hist >= 0) zero(ws[i].bnd_hist, (long long)bnd_pitch_of(p) * 4);  // b_0 = 0
+    io.bnd_n = p->bnd_n; io.bnd_pitch = bnd_pitch_of(p);
+    io.bnd_ref = p->bnd_ref; io.bnd_alpha = p->bnd_alpha; io.bnd_gamma = p->bnd_gamma;
+    io.bnd_coef = p->bnd_n ? (float*)(a + ws[i].bnd_coef) : nullptr;
     io.grad_out = ((s.flags & SEM_F_ADJOINT) && s.grad_out) ? s.grad_out : nullptr;
     io.gacc = (const double*)(a + ws[i].grad64);
     io.adj_scale = (const double*)(a + ws[i].misfit) + 2 * p->nrec;
@@ -2603,6 +2733,8 @@ int sem_forward_noalloc(const sem_plan_t* p, const double* velocity, float* rec_
   int dev = -1;
   CUDA_TRY(cudaGetDevice(&dev));
   if (dev != p->device) return fail(SEM_ERR_ARG, "plan was created on another device");
+  if (p->bnd_n > 0)
+    return fail(SEM_ERR_UNSUPPORTED, "sem_forward_noalloc runs the sponge boundary mode only");
   // device address of the scratch array on this device, looked up when the plan was made
   char* const base = p->noalloc_scratch;
   if (!base) return fail(SEM_ERR_ARG, "plan has no scratch address");
@@ -2764,6 +2896,10 @@ SolveIo solve_io(const sem_solve_t& s, const Workspace& ws, char* a) {
     zero(ws.grad, 3 * F);  // float32 partial and float64 accumulator
   }
   zero(ws.misfit, ws.status - ws.misfit + 256);
+  if (ws.bnd_hist >= 0) zero(ws.bnd_hist, (long long)bnd_pitch_of(p) * 4);  // b_0 = 0
+  io.bnd_n = p->bnd_n; io.bnd_pitch = bnd_pitch_of(p);
+  io.bnd_ref = p->bnd_ref; io.bnd_alpha = p->bnd_alpha; io.bnd_gamma = p->bnd_gamma;
+  io.bnd_coef = p->bnd_n ? (float*)(a + ws.bnd_coef) : nullptr;
   io.grad_out = ((s.flags & SEM_F_ADJOINT) && s.grad_out) ? s.grad_out : nullptr;
   io.gacc = (const double*)(a + ws.grad64);
   io.adj_scale = (const double*)(a + ws.misfit) + 2 * p->nrec;
@@ -3060,6 +3196,9 @@ int sem_engine_step(sem_engine_t* e, void* stream_v) {
     d.status = (int*)(a + j->ws.status);
     d.ws = (const float*)a;
     d.tmap = nullptr;
+    d.bnd_n = p->bnd_n; d.bnd_pitch = bnd_pitch_of(p);
+    d.bnd_coef = p->bnd_n ? (const float*)(a + j->ws.bnd_coef) : nullptr;
+    d.bnd_hist = j->ws.bnd_hist >= 0 ? (float*)(a + j->ws.bnd_hist) : nullptr;
     if (use_strip) {
       if (!j->has_tmap) {
         rc = encode_band_map(&j->tmap, a, p, field_slots(j->ws, p, adj));

@@ -60,9 +60,34 @@ def receiver_weights(positions, xmin, zmin, dx, dz, nelx, nelz, npol):
     return base, w
 
 
+def boundary_slots(nelx, nelz, npol):
+    """Slot of every node of the absorbing edges in the per-solve boundary tables:
+    (gx = 0, gz) -> gz, (gx = nxg - 1, gz) -> nzg + gz, (gx, gz = nzg - 1) -> 2 nzg + gx
+    for the bottom row's inner columns.  Returns (nb, gx (nb,), gz (nb,), used (nb,))."""
+    nxg, nzg = nelx * npol + 1, nelz * npol + 1
+    nb = 2 * nzg + nxg
+    gx = np.concatenate([np.zeros(nzg, int), np.full(nzg, nxg - 1), np.arange(nxg)])
+    gz = np.concatenate([np.arange(nzg), np.arange(nzg), np.full(nxg, nzg - 1)])
+    used = np.ones(nb, dtype=bool)
+    used[2 * nzg] = used[2 * nzg + nxg - 1] = False  # bottom corners sit in the side lists
+    return nb, gx, gz, used
+
+
 def build_plan_arrays(xmin, xmax, zmin, zmax, nelx, nelz, npol, dt, nt, src_xz, f0, amp,
-                      receivers, pml_thickness, sponge_cmax, coords=None, node_grid=None):
-    """All float64 inputs of ``sem_plan_create`` for one mesh/time/source/receiver set."""
+                      receivers, pml_thickness, sponge_cmax, coords=None, node_grid=None,
+                      boundary="sponge"):
+    """All float64 inputs of ``sem_plan_create`` for one mesh/time/source/receiver set.
+
+    ``boundary='sponge'`` is the reference's cubic-ramp sponge on all four sides.
+    ``boundary='stacey'`` (an extension) uses first-order Stacey absorbing edges on the
+    sides and the bottom and a free surface (u = 0) on the top row, without the sponge:
+    (1 + a) u+ = 2 u - (1 - a) u- + dt^2 M^-1 (f - K u) with a = dt c beta / (2 M) on the
+    absorbing edges, beta the node's boundary quadrature weight.  Per boundary slot the
+    plan carries the node's reference index, alpha = dt beta / (2 M) (a = c alpha) and
+    gamma = beta / (4 dt), the factor of the gradient's boundary-impedance term
+    (g = gamma / c per solve)."""
+    if boundary not in ("sponge", "stacey"):
+        raise ValueError(f"boundary must be 'sponge' or 'stacey', got {boundary!r}")
     N = int(npol)
     nodes = gll_points(N)
     w = gll_weights(nodes)
@@ -86,8 +111,11 @@ def build_plan_arrays(xmin, xmax, zmin, zmax, nelx, nelz, npol, dt, nt, src_xz, 
     wl3z = assemble_1d(nelz, w * lq ** 3)
     xg = grid_coords_1d(xmin, xmax, nelx, N)
     zg = grid_coords_1d(zmin, zmax, nelz, N)
-    dec_x = np.exp(-sponge_sigma_1d(xg, xmin, xmax, pml_thickness, sponge_cmax) * dt)
-    dec_z = np.exp(-sponge_sigma_1d(zg, zmin, zmax, pml_thickness, sponge_cmax) * dt)
+    if boundary == "sponge":
+        dec_x = np.exp(-sponge_sigma_1d(xg, xmin, xmax, pml_thickness, sponge_cmax) * dt)
+        dec_z = np.exp(-sponge_sigma_1d(zg, zmin, zmax, pml_thickness, sponge_cmax) * dt)
+    else:
+        dec_x, dec_z = np.ones(nxg), np.ones(nzg)
     tab_x = np.concatenate([1.0 / mx, J * seta2 * wl3x, dec_x])
     tab_z = np.concatenate([dt * dt / (J * mz), J * sxi2 * wl3z, dec_z])
     if coords is None or node_grid is None:
@@ -96,7 +124,18 @@ def build_plan_arrays(xmin, xmax, zmin, zmax, nelx, nelz, npol, dt, nt, src_xz, 
     g = int(node_grid[src_node])
     src = ricker_source(nt, dt, f0, amp)
     base, rw = receiver_weights(receivers, xmin, zmin, dx, dz, nelx, nelz, N)
-    return dict(nelx=int(nelx), nelz=int(nelz), npol=N, nt=int(nt), dt=float(dt),
+    bnd = {"bnd_n": 0}
+    if boundary == "stacey":
+        nb, bgx, bgz, used = boundary_slots(nelx, nelz, N)
+        side = (bgx == 0) | (bgx == nxg - 1)
+        beta = np.where(side, mz[bgz] * (dz / 2.0), 0.0) + np.where(bgz == nzg - 1, mx[bgx] * (dx / 2.0), 0.0)
+        mass = J * mx[bgx] * mz[bgz]
+        ids = np.empty(nxg * nzg, dtype=np.int64)
+        ids[np.asarray(node_grid, dtype=np.int64)] = np.arange(nxg * nzg)
+        ref = np.where(used & (bgz > 0), ids[bgz * nxg + bgx], -1).astype(np.int32)
+        bnd = {"bnd_n": int(nb), "bnd_ref": ref, "bnd_alpha": 0.5 * dt * beta / mass,
+               "bnd_gamma": beta / (4.0 * dt)}
+    return dict(nelx=int(nelx), nelz=int(nelz), npol=N, nt=int(nt), dt=float(dt), boundary=boundary, **bnd,
                 npoints=int(nxg * nzg), node_grid=np.ascontiguousarray(node_grid, dtype=np.int64),
                 gll_D=np.ascontiguousarray(D), gll_beta=w * lq, tab_x=tab_x, tab_z=tab_z,
                 src_term=dt * dt * src, src_gx=g % nxg, src_gz=g // nxg, src_node=src_node,
@@ -135,6 +174,14 @@ class SEMPlan:
         d.src_gx, d.src_gz, d.nrec = a["src_gx"], a["src_gz"], a["nrec"]
         d.rec_base = rb.ctypes.data_as(C.POINTER(C.c_int32))
         d.rec_w = _dptr(rw)
+        self.boundary = a["boundary"]
+        d.boundary_mode = 1 if a["boundary"] == "stacey" else 0
+        if d.boundary_mode:
+            bk = [np.ascontiguousarray(a[k]) for k in ("bnd_ref", "bnd_alpha", "bnd_gamma")]
+            self._keep += bk
+            d.bnd_n = a["bnd_n"]
+            d.bnd_ref = bk[0].ctypes.data_as(C.POINTER(C.c_int32))
+            d.bnd_alpha, d.bnd_gamma = _dptr(bk[1]), _dptr(bk[2])
         h = C.c_void_p()
         _lib.check(lib.sem_plan_create(C.byref(d), C.byref(h)))
         self.handle = h

@@ -309,6 +309,14 @@ class SEMSimulation:
         return None
 
     # ------------------------------------------------------------------ device plumbing
+    def _boundary(self):
+        """``method.boundary``: 'sponge' (the reference's, default) or 'stacey' (extension:
+        Stacey absorbing sides and bottom, free surface on top, no sponge)."""
+        b = str(self.config["method"].get("boundary", "sponge"))
+        if b not in ("sponge", "stacey"):
+            raise ValueError(f"method.boundary must be 'sponge' or 'stacey', got {b!r}")
+        return b
+
     def _plan(self):
         key = (float(self.dt), int(self.nt))
         p = self._plans.get(key)
@@ -318,7 +326,7 @@ class SEMSimulation:
                     float(self.zmax), int(self.nelem_x), int(self.nelem_z), int(self.npol), float(self.dt),
                     int(self.nt), float(self.src_x), float(self.src_z), float(self.src_f0),
                     float(self.src_amp), rec.tobytes(), float(self.config["method"]["pml_thickness"]),
-                    float(self.vmax))
+                    float(self.vmax), self._boundary())
             with _PLAN_LOCK:
                 p = _PLAN_CACHE.get(gkey)
                 if p is not None:
@@ -328,7 +336,8 @@ class SEMSimulation:
                             nelx=self.nelem_x, nelz=self.nelem_z, npol=self.npol, dt=self.dt, nt=self.nt,
                             src_xz=(self.src_x, self.src_z), f0=self.src_f0, amp=self.src_amp,
                             receivers=rec, pml_thickness=float(self.config["method"]["pml_thickness"]),
-                            sponge_cmax=self.vmax, coords=self.global_coords, node_grid=self.node_grid)
+                            sponge_cmax=self.vmax, coords=self.global_coords, node_grid=self.node_grid,
+                            boundary=self._boundary())
                 with _PLAN_LOCK:
                     # another thread may have built the same plan meanwhile: keep the first
                     p = _PLAN_CACHE.setdefault(gkey, p)

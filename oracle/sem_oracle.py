@@ -40,6 +40,22 @@ faster than the reference's; timings quoted from it are therefore conservative.
 ``mode='exact'`` additionally applies the sponge inside the adjoint loop, which makes
 the gradient the exact discrete adjoint of the forward map (the reference's adjoint
 omits it; see ``core.py:1252-1275``).
+
+``method.boundary = 'stacey'`` selects an extension boundary mode that the reference
+does not have: first-order Stacey absorbing conditions on the sides and the bottom and a
+free surface (pressure release, u = 0) on the top, without the sponge.  Forward:
+M u'' + C u' + K u = f with C = diag(c_i beta_i), beta_i the boundary quadrature weight
+of node i (sum of w_a h/2 over its absorbing element edges), discretised by central
+differences:  (1 + a) u+ = 2 u - (1 - a) u- + dt^2 M^-1 (f - K u),  a = dt c beta / (2 M),
+then u+ = 0 on the top row.  Its exact discrete adjoint is the same recurrence run
+backwards with the residual source, and the gradient adds to the stiffness term a
+boundary-impedance term from d a / d c:
+d loglik / d c_i += beta_i / (2 dt) * lambda_i * (u_i(t+1) - u_i(t-1)) at every adjoint step.
+
+``device=`` runs the same float64 time loops on another torch device.  The tests at
+the full sizes of the benchmark configurations (up to 1.28 M nodes and 5000 steps,
+where the float64 forward history alone is 51 GB) use torch's CUDA backend for speed;
+the arithmetic is the same float64 code that the golden vectors pin on the CPU.
 """
 from __future__ import annotations
 
@@ -385,21 +401,71 @@ def build_sim(config: dict, velocity: np.ndarray | None = None, dt_cfl_velocity=
         pos = circle_receivers(src_x, src_z, float(rc["radius"]), int(rc["num_receivers"]))
     R = receiver_matrix(pos, xmin, zmin, dx, dz, nelx, nelz, conn, npol, len(coords))
     M = lumped_mass(conn, dx, dz, npol, len(coords))
-    decay, mask = sponge_decay(xmin, xmax, zmin, zmax, float(config["method"]["pml_thickness"]),
-                               coords, dt, float(vmax_cfg))
+    mode = config["method"].get("boundary", "sponge")
+    extra = {"boundary": mode}
+    if mode == "sponge":
+        decay, mask = sponge_decay(xmin, xmax, zmin, zmax, float(config["method"]["pml_thickness"]),
+                                   coords, dt, float(vmax_cfg))
+    elif mode == "stacey":
+        decay, mask = np.ones(len(coords)), np.zeros(len(coords), dtype=bool)
+        beta, top = stacey_weights(grid, nelx, nelz, npol, dx, dz)
+        extra.update(beta=beta, top=top)
+    else:
+        raise ValueError(f"unknown boundary mode {mode!r}")
     ops = sem_operators(dx, dz, npol)
     return OracleSim(xmin, xmax, zmin, zmax, nelx, nelz, npol, coords, conn, grid, dx, dz, dt, nt,
-                     src_node, src, R, M, decay, mask, ops, velocity)
+                     src_node, src, R, M, decay, mask, ops, velocity, extra)
 
 
-def _torch_csr(R: sp.csr_matrix):
+def stacey_weights(grid, nelx, nelz, npol, dx, dz):
+    """Boundary quadrature weight of every node on the absorbing edges (x = xmin, x = xmax,
+    z = zmax): the sum over its element edges of the 1-D GLL weight times the edge
+    half-length; and the top-row (z = zmin, free surface) mask.  Reference node order."""
+    w = gll_weights(gll_points(npol))
+    N = npol
+    nxg, nzg = nelx * N + 1, nelz * N + 1
+    gx, gz = grid[:, 0], grid[:, 1]
+    bx = np.zeros(nxg)   # along the bottom edge, by column
+    bz = np.zeros(nzg)   # along the side edges, by row
+    for e in range(nelx):
+        bx[e * N:(e + 1) * N + 1] += w * (dx / 2.0)
+    for e in range(nelz):
+        bz[e * N:(e + 1) * N + 1] += w * (dz / 2.0)
+    beta = np.zeros(len(grid))
+    side = (gx == 0) | (gx == nxg - 1)
+    beta[side] += bz[gz[side]]
+    bot = gz == nzg - 1
+    beta[bot] += bx[gx[bot]]
+    return beta, gz == 0
+
+
+def _torch_csr(R: sp.csr_matrix, device="cpu"):
     return torch.sparse_csr_tensor(torch.from_numpy(R.indptr.astype(np.int64)),
                                    torch.from_numpy(R.indices.astype(np.int64)),
                                    torch.from_numpy(R.data.astype(np.float64)), size=R.shape,
-                                   dtype=torch.float64)
+                                   dtype=torch.float64).to(device)
 
 
-def forward(sim: OracleSim, velocity=None, convention: str = "run", keep_history: bool = False):
+def _stacey_terms(sim: OracleSim, c, device):
+    """(a, top mask, beta) of the Stacey / free-surface mode, or None for the sponge."""
+    if sim.extra.get("boundary", "sponge") != "stacey":
+        return None
+    beta = sim.extra["beta"]
+    a = 0.5 * sim.dt * np.asarray(c, dtype=np.float64) * beta / sim.M
+    return (torch.from_numpy(a).to(device), torch.from_numpy(sim.extra["top"]).to(device),
+            torch.from_numpy(beta).to(device))
+
+
+def _stacey_step(st, u, u_prev, f):
+    """(1 + a) u+ = 2 u - (1 - a) u- + f, then u+ = 0 on the free surface."""
+    a, top, _ = st
+    u_next = (2.0 * u - (1.0 - a) * u_prev + f) / (1.0 + a)
+    u_next[top] = 0.0
+    return u_next
+
+
+def forward(sim: OracleSim, velocity=None, convention: str = "run", keep_history: bool = False,
+            device="cpu"):
     """Forward time loop.
 
     convention='run'     : rec[it] = R u_curr recorded before the update (core.py:632-639)
@@ -407,24 +473,28 @@ def forward(sim: OracleSim, velocity=None, convention: str = "run", keep_history
     Returns rec (nt, nrec) and optionally the post-update history (nt, P)."""
     c = sim.velocity if velocity is None else np.asarray(velocity, dtype=np.float64)
     Gx, Gz, S, w2D = sim.ops
-    K = stiffness_csr(c, sim.conn, Gx, Gz, S, w2D, sim.npoints)
-    R = _torch_csr(sim.R)
+    K = stiffness_csr(c, sim.conn, Gx, Gz, S, w2D, sim.npoints).to(device)
+    R = _torch_csr(sim.R, device)
     P = sim.npoints
-    Minv = torch.from_numpy(1.0 / sim.M)
+    Minv = torch.from_numpy(1.0 / sim.M).to(device)
     Msrc = float(sim.M[sim.src_node])
     dt2 = sim.dt * sim.dt
-    idx = torch.from_numpy(np.nonzero(sim.pml_mask)[0])
-    dec = torch.from_numpy(sim.decay)[idx]
-    src = torch.from_numpy(sim.src)
-    u_prev = torch.zeros(P, dtype=torch.float64)
-    u_curr = torch.zeros(P, dtype=torch.float64)
-    rec = torch.zeros((sim.nt, R.shape[0]), dtype=torch.float64)
-    hist = torch.zeros((sim.nt, P), dtype=torch.float64) if keep_history else None
+    idx = torch.from_numpy(np.nonzero(sim.pml_mask)[0]).to(device)
+    dec = torch.from_numpy(sim.decay).to(device)[idx]
+    src = torch.from_numpy(sim.src).to(device)
+    u_prev = torch.zeros(P, dtype=torch.float64, device=device)
+    u_curr = torch.zeros(P, dtype=torch.float64, device=device)
+    rec = torch.zeros((sim.nt, R.shape[0]), dtype=torch.float64, device=device)
+    hist = torch.zeros((sim.nt, P), dtype=torch.float64, device=device) if keep_history else None
     sn = sim.src_node
+    st = _stacey_terms(sim, c, device)
     for it in range(sim.nt):
         rhs = -torch.matmul(K, u_curr)
         rhs[sn] += src[it] * Msrc
-        u_next = 2.0 * u_curr - u_prev + dt2 * (Minv * rhs)
+        if st is None:
+            u_next = 2.0 * u_curr - u_prev + dt2 * (Minv * rhs)
+        else:
+            u_next = _stacey_step(st, u_curr, u_prev, dt2 * (Minv * rhs))
         if convention == "run":
             rec[it] = torch.matmul(R, u_curr)
         if len(idx):
@@ -435,7 +505,7 @@ def forward(sim: OracleSim, velocity=None, convention: str = "run", keep_history
             rec[it] = torch.matmul(R, u_curr)
         if keep_history:
             hist[it] = u_curr
-    return rec.numpy(), (hist if keep_history else None)
+    return rec.cpu().numpy(), (hist if keep_history else None)
 
 
 def sensitivity_step(u, lam, conn_t, Gx_t, Gz_t, S_t, w2D_t, npoints):
@@ -451,13 +521,13 @@ def sensitivity_step(u, lam, conn_t, Gx_t, Gz_t, S_t, w2D_t, npoints):
     lz = ll @ Gz_t.T
     gq = w2D_t * (ux * lx + uz * lz)
     loc = gq @ S_t
-    out = torch.zeros(npoints, dtype=torch.float64)
+    out = torch.zeros(npoints, dtype=torch.float64, device=u.device)
     out.scatter_add_(0, gi, loc.reshape(-1))
     return out
 
 
 def forward_adjoint(sim: OracleSim, y_obs_aligned: np.ndarray, sigma: float,
-                    velocity=None, mode: str = "reference", window=None):
+                    velocity=None, mode: str = "reference", window=None, device="cpu"):
     """run_forward_and_adjoint (core.py:1067-1278) on a given nodal velocity.
 
     Returns dict(loglik, clean (nt,nrec), dJ_dv (P,) = reference's ``dJ_dv``,
@@ -466,34 +536,41 @@ def forward_adjoint(sim: OracleSim, y_obs_aligned: np.ndarray, sigma: float,
     (CO2_plume/one_stage/single_cubic/sem_waveform/core.py:1441-1552)."""
     c = sim.velocity if velocity is None else np.asarray(velocity, dtype=np.float64)
     Gx, Gz, S, w2D = sim.ops
-    K = stiffness_csr(c, sim.conn, Gx, Gz, S, w2D, sim.npoints)
-    R = _torch_csr(sim.R)
-    RT = _torch_csr(sim.R.T.tocsr())
+    K = stiffness_csr(c, sim.conn, Gx, Gz, S, w2D, sim.npoints).to(device)
+    R = _torch_csr(sim.R, device)
+    RT = _torch_csr(sim.R.T.tocsr(), device)
     P = sim.npoints
     nt = sim.nt
-    Minv = torch.from_numpy(1.0 / (sim.M + 1e-30))
+    Minv = torch.from_numpy(1.0 / (sim.M + 1e-30)).to(device)
     Msrc = float(sim.M[sim.src_node])
     dt2 = sim.dt * sim.dt
-    idx = torch.from_numpy(np.nonzero(sim.pml_mask)[0])
-    dec = torch.from_numpy(sim.decay)[idx]
-    src = torch.from_numpy(sim.src)
+    idx = torch.from_numpy(np.nonzero(sim.pml_mask)[0]).to(device)
+    dec = torch.from_numpy(sim.decay).to(device)[idx]
+    src = torch.from_numpy(sim.src).to(device)
     it0, it1, decim = (0, nt, 1) if window is None else window
     nt_eff = it1 - it0
-    u_prev = torch.zeros(P, dtype=torch.float64)
-    u_curr = torch.zeros(P, dtype=torch.float64)
-    hist = torch.zeros((nt_eff, P), dtype=torch.float64)
+    u_prev = torch.zeros(P, dtype=torch.float64, device=device)
+    u_curr = torch.zeros(P, dtype=torch.float64, device=device)
+    hist = torch.zeros((nt_eff, P), dtype=torch.float64, device=device)
     sn = sim.src_node
+    st = _stacey_terms(sim, c, device)
+    if st is not None and (it0, it1, decim) != (0, nt, 1):
+        raise ValueError("the Stacey boundary mode supports the full misfit window only")
     for it in range(nt):
         rhs = -torch.matmul(K, u_curr)
         rhs[sn] += src[it] * Msrc
-        u_next = 2.0 * u_curr - u_prev + dt2 * (Minv * rhs)
+        if st is None:
+            u_next = 2.0 * u_curr - u_prev + dt2 * (Minv * rhs)
+        else:
+            u_next = _stacey_step(st, u_curr, u_prev, dt2 * (Minv * rhs))
         if len(idx):
             u_curr[idx] *= dec
             u_next[idx] *= dec
         u_prev, u_curr = u_curr, u_next
         if it0 <= it < it1:
             hist[it - it0] = u_curr
-    d_syn = torch.matmul(R, hist.T).T.numpy()
+    d_syn = torch.stack([torch.matmul(R, hist[i]) for i in range(nt_eff)]).cpu().numpy() \
+        if device != "cpu" else torch.matmul(R, hist.T).T.numpy()
     d_dec = d_syn[::decim]
     y = np.asarray(y_obs_aligned, dtype=np.float64)
     resid_dec = d_dec - y
@@ -501,26 +578,35 @@ def forward_adjoint(sim: OracleSim, y_obs_aligned: np.ndarray, sigma: float,
     resid[::decim] = resid_dec
     sigma2 = float(sigma) ** 2 + 1e-24
     loglik = -0.5 * float(np.sum(resid_dec * resid_dec)) / sigma2
-    rs = torch.from_numpy(resid.T.copy()) * (1.0 / sigma2)
-    conn_t = torch.from_numpy(sim.conn)
-    Gx_t, Gz_t, S_t, w2D_t = (torch.from_numpy(a) for a in (Gx, Gz, S, w2D))
-    lam_n = torch.zeros(P, dtype=torch.float64)
-    lam_c = torch.zeros(P, dtype=torch.float64)
-    acc = torch.zeros(P, dtype=torch.float64)
+    rs = (torch.from_numpy(resid.T.copy()) * (1.0 / sigma2)).to(device)
+    conn_t = torch.from_numpy(sim.conn).to(device)
+    Gx_t, Gz_t, S_t, w2D_t = (torch.from_numpy(a).to(device) for a in (Gx, Gz, S, w2D))
+    lam_n = torch.zeros(P, dtype=torch.float64, device=device)
+    lam_c = torch.zeros(P, dtype=torch.float64, device=device)
+    acc = torch.zeros(P, dtype=torch.float64, device=device)
+    if st is not None:
+        # boundary-impedance term per c^2: beta / (4 dt c) lambda (u(t+1) - u(t-1))
+        bfac = st[2] / (4.0 * sim.dt * torch.from_numpy(np.asarray(c, dtype=np.float64)).to(device))
     for it in range(nt_eff - 1, -1, -1):
         rhs = torch.matmul(RT, rs[:, it]) - torch.matmul(K, lam_c)
-        lam_p = 2.0 * lam_c - lam_n + dt2 * (Minv * rhs)
+        if st is None:
+            lam_p = 2.0 * lam_c - lam_n + dt2 * (Minv * rhs)
+        else:
+            lam_p = _stacey_step(st, lam_c, lam_n, dt2 * (Minv * rhs))
         acc += sensitivity_step(hist[it], lam_c, conn_t, Gx_t, Gz_t, S_t, w2D_t, P)
+        if st is not None and it + 1 < nt_eff:
+            u_lo = hist[it - 1] if it >= 1 else torch.zeros_like(lam_c)
+            acc += bfac * lam_c * (hist[it + 1] - u_lo)
         if mode == "exact" and len(idx):
             lam_c[idx] *= dec
             lam_p[idx] *= dec
         lam_n, lam_c = lam_c, lam_p
-    dJ = (2.0 * torch.from_numpy(c) * acc).numpy()
+    dJ = (2.0 * torch.from_numpy(c) * acc.cpu()).numpy()
     return {"loglik": loglik, "clean": d_syn, "dJ_dv": dJ, "dL_dv": -dJ, "resid": resid}
 
 
-def misfit_loglik(sim: OracleSim, velocity, y_obs_aligned, sigma, convention="fwdadj"):
+def misfit_loglik(sim: OracleSim, velocity, y_obs_aligned, sigma, convention="fwdadj", device="cpu"):
     """-0.5 |d(c) - y|^2 / sigma^2 with d from the chosen receiver convention."""
-    rec, _ = forward(sim, velocity, convention=convention)
+    rec, _ = forward(sim, velocity, convention=convention, device=device)
     r = rec - y_obs_aligned
     return -0.5 * float(np.sum(r * r)) / (float(sigma) ** 2 + 1e-24)
