@@ -57,7 +57,7 @@ WORKLOAD_ELBO = ("batched ELBO sampling (256 models, 100x50 el, N=4, 80601 nodes
                  "100 receivers)")
 
 
-def workload(nmodels=256, nelx=100, nelz=50, nt=3000, nrec=100, seed0=0):
+def workload(nmodels=256, nelx=100, nelz=50, nt=3000, nrec=100, seed0=0, boundary="sponge"):
     from mun_b200.bspline import grid_basis, layered_velocity
     from mun_b200.mesh import create_global_mesh
     xmin, xmax, zmin, zmax, N = 0.0, 2000.0, 0.0, 1000.0, 4
@@ -73,7 +73,8 @@ def workload(nmodels=256, nelx=100, nelz=50, nt=3000, nrec=100, seed0=0):
     rec = np.stack([np.linspace(xmin, xmax, nrec), np.full(nrec, 10.0)], 1)
     plan_kw = dict(xmin=xmin, xmax=xmax, zmin=zmin, zmax=zmax, nelx=nelx, nelz=nelz, npol=N, dt=dt,
                    nt=nt, src_xz=(1000.0, 20.0), f0=10.0, amp=1.0, receivers=rec,
-                   pml_thickness=200.0, sponge_cmax=3000.0, coords=coords, node_grid=node_grid)
+                   pml_thickness=200.0, sponge_cmax=3000.0, coords=coords, node_grid=node_grid,
+                   boundary=boundary)
     return dict(plan_kw=plan_kw, vels=vels, v_true=v_true, thetas=thetas, B=B, coords=coords,
                 npoints=len(coords), dt=dt, nt=nt, sigma=1e-3)
 
@@ -174,7 +175,8 @@ def oracle_solve_s(W, nts, threads):
            "time": {"total_time": (nts - 0.5) * W["dt"], "dt": W["dt"]},
            "source": {"position": kw["src_xz"], "frequency": kw["f0"], "amplitude": kw["amp"]},
            "receivers": {"positions": kw["receivers"]},
-           "method": {"polynomial_order": kw["npol"], "pml_thickness": kw["pml_thickness"]},
+           "method": {"polynomial_order": kw["npol"], "pml_thickness": kw["pml_thickness"],
+                      "boundary": kw.get("boundary", "sponge")},
            "velocity": {"outside_velocity": kw["sponge_cmax"]}}
     t0 = time.perf_counter()
     sim = so.build_sim(cfg, W["vels"][0], dt=W["dt"])
@@ -218,7 +220,7 @@ def run_plain(args):
     rec = np.stack([np.linspace(xmin, xmax, 50), np.full(50, 10.0)], 1)
     kw = dict(xmin=xmin, xmax=xmax, zmin=zmin, zmax=zmax, nelx=nelx, nelz=nelz, npol=N, dt=dt, nt=nt,
               src_xz=(1000.0, 20.0), f0=10.0, amp=1.0, receivers=rec, pml_thickness=200.0,
-              sponge_cmax=3000.0, coords=coords, node_grid=ng)
+              sponge_cmax=3000.0, coords=coords, node_grid=ng, boundary=args.boundary)
     plan = SEMPlan(**kw)
     dev = torch.device("cuda")
     obs = SolveSpec(plan, torch.as_tensor(v_obs, device=dev), shift=True)
@@ -240,6 +242,7 @@ def run_plain(args):
             ms.append(ev0.elapsed_time(ev1))
     ms = np.array(ms)
     out = {"workload": "plain: 40x20 el, N=4, 13041 nodes, 2000 steps, 50 receivers, fwd+adj",
+           "boundary": args.boundary,
            "gpu_ms_per_solve": float(ms.mean()), "gpu_solves_per_s": 1e3 / float(ms.mean()),
            "p50_ms": float(np.percentile(ms, 50)), "p99_ms": float(np.percentile(ms, 99)),
            "kernel": b.last_kernel, "shape": b.last_shape, "graph_chunk": args.graph_chunk,
@@ -396,8 +399,10 @@ def run_uneven(args, steps=None, warmup=None, plain=None, cpu_sample=None, emit=
            "batched_ms": float(np.mean(ms)), "kernel": b.last_kernel, "groups": b.last_groups,
            "autotuned": None if tuned is None else {"kernel": tuned["kernel"], "tile": list(tuned["tile"]),
                                                     "graph_chunk": tuned["graph_chunk"],
-                                                    "ckpt_k": "automatic schedule",
+                                                    "strip_bands": tuned["strip_bands"],
+                                                    "ckpt_k": "automatic schedule (memory-budget cost model)",
                                                     "tuning_s": round(tune_s, 1)},
+           "shape (tile_ex, tile_ez, strip_bands)": list(b.last_shape),
            "plain_estimated": len(plans) / (plain_total / 1e3), "plain_solves_timed": len(plain_ms),
            "batched_over_plain": batched / (len(plans) / (plain_total / 1e3)),
            "mnode_steps_per_s": node_steps / (np.mean(ms) / 1e3) / 1e6,
@@ -584,6 +589,44 @@ def run_single(args, steps=None, warmup=None, cpu_sample=None, emit=True):
     return out
 
 
+def stacey_leg(args, steps=2, warmup=1):
+    """The batched ELBO step with the boundary the configuration states: Stacey absorbing
+    sides and bottom, free surface on top (an extension mode; the reference has only the
+    sponge).  Device-timed steps of the 256 models and float64-oracle parity of one."""
+    import torch
+    from mun_b200 import Batch, SEMPlan, SolveSpec
+    W = workload(nmodels=args.models, nt=args.nt, boundary="stacey")
+    plan = SEMPlan(**W["plan_kw"])
+    dev = torch.device("cuda")
+    stream = torch.cuda.Stream()
+    batch = Batch(kernel=args.kernel)
+    with torch.cuda.stream(stream):
+        obs = SolveSpec(plan, torch.as_tensor(W["v_true"], device=dev), shift=True)
+        batch.run([obs])
+    stream.synchronize()
+    y = obs.rec.double()
+    inv_s2 = 1.0 / (W["sigma"] ** 2 + 1e-24)
+    vel = torch.as_tensor(W["vels"], device=dev)
+    specs = [SolveSpec(plan, vel[i], adjoint=True, y_obs=y, inv_sigma2=inv_s2) for i in range(args.models)]
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ms = []
+    for it in range(warmup + steps):
+        with torch.cuda.stream(stream):
+            ev0.record(stream)
+            batch.run(specs)
+            ev1.record(stream)
+        ev1.synchronize()
+        if it >= warmup:
+            ms.append(ev0.elapsed_time(ev1))
+    out = {"workload": "batched ELBO sampling, 256 models, Stacey absorbing sides and bottom, free surface "
+                       "on top (no sponge)",
+           "value": args.models / (np.mean(ms) / 1e3), "unit": "solves/s", "ms_per_step": float(np.mean(ms)),
+           "kernel": batch.last_kernel, "groups": batch.last_groups,
+           "status": int(torch.cat([s.status for s in specs]).max().item())}
+    out["parity"] = parity_leg(W, specs, y, [1])
+    return out
+
+
 def parity_leg(W, specs, y, which):
     """Relative errors of solves ``which`` of the timed batch (their last run) against the
     float64 oracle on the host, same velocity and observations: seismogram (rel. L2),
@@ -597,7 +640,8 @@ def parity_leg(W, specs, y, which):
            "time": {"total_time": (W["nt"] - 0.5) * W["dt"], "dt": W["dt"]},
            "source": {"position": kw["src_xz"], "frequency": kw["f0"], "amplitude": kw["amp"]},
            "receivers": {"positions": kw["receivers"]},
-           "method": {"polynomial_order": kw["npol"], "pml_thickness": kw["pml_thickness"]},
+           "method": {"polynomial_order": kw["npol"], "pml_thickness": kw["pml_thickness"],
+                      "boundary": kw.get("boundary", "sponge")},
            "velocity": {"outside_velocity": kw["sponge_cmax"]}}
     yy = y.cpu().numpy()
     rel = lambda a, b: float(np.linalg.norm(a - b) / np.linalg.norm(b))  # noqa: E731
@@ -613,7 +657,9 @@ def parity_leg(W, specs, y, which):
     e = np.array(rows).max(axis=0)
     return {"models": list(which), "seis_rel_l2": float(e[0]), "grad_rel_l2": float(e[1]),
             "loglik_rel": float(e[2]), "tolerance": 1e-4, "pass": bool((e <= 1e-4).all()),
-            "oracle": "float64 CPU restatement of the reference path, full 3000 steps",
+            "oracle": "float64 CPU restatement of the reference path, full 3000 steps"
+                      + ("" if kw.get("boundary", "sponge") == "sponge" else
+                         " (its Stacey / free-surface extension mode)"),
             "wall_s": time.perf_counter() - t0}
 
 
@@ -643,6 +689,8 @@ def main():
     ap.add_argument("--serve-cap-gb", type=float, default=150.0)
     ap.add_argument("--serve-ticks", type=int, default=32)
     ap.add_argument("--clocks-log", default="", help="nvidia-smi clock samples (default: a temp file)")
+    ap.add_argument("--boundary", default="sponge", choices=["sponge", "stacey"],
+                    help="plain workload: the reference's sponge, or Stacey sides/bottom with a free surface")
     ap.add_argument("--no-extras", action="store_true",
                     help="default workload: skip the parity, single, uneven and serving legs")
     args = ap.parse_args()
@@ -804,6 +852,9 @@ def main():
     torch.cuda.synchronize()
     torch.cuda.empty_cache()
     if rank == 0 and not args.no_extras:
+        extras["stacey"] = stacey_leg(args)
+        gc.collect()
+        torch.cuda.empty_cache()
         extras["single"] = run_single(args, steps=2, warmup=1, cpu_sample=0, emit=False)
         extras["uneven"] = run_uneven(args, steps=1, warmup=1, plain=4, cpu_sample=0, emit=False)
         extras["serving"] = run_serving(args, requests=100, emit=False)

@@ -19,6 +19,7 @@ from .solver import Batch, SolveSpec
 
 TILE_CANDIDATES = [(0, 0), (8, 8), (16, 8), (8, 4), (16, 4), (4, 4), (2, 2)]  # (0, 0): automatic
 GRAPH_CANDIDATES = [0, 32]
+STRIP_BAND_CANDIDATES = [0, 4, 8]  # strip kernel: element rows per CTA (0: automatic)
 
 _cache = {}
 
@@ -36,7 +37,10 @@ def _proxy_plan(plan, nt_proxy):
 
 
 def tune(specs, nt_proxy=48, repeats=2, candidates=None, verbose=False):
-    """Return ``dict(kernel=..., tile=..., graph_chunk=..., ckpt_k=...)`` for ``specs``."""
+    """Return ``dict(kernel=..., tile=..., graph_chunk=..., strip_bands=..., ckpt_k=...)``
+    for ``specs``: the elements per CTA (tile shape, or strip chunk height), the kernel
+    variant and the graph chunk, timed; ``ckpt_k = 0`` leaves the checkpoint interval and
+    the group split to the library's memory-budget cost model at run time."""
     key = signature(specs)
     if key in _cache:
         return _cache[key]
@@ -56,13 +60,15 @@ def tune(specs, nt_proxy=48, repeats=2, candidates=None, verbose=False):
 
     # the persistent kernel is one launch per run (graphs do not apply); it falls back to
     # per-tick tile launches by itself when the tiles are not all resident
-    cands = candidates or ([(1, t, g) for t in TILE_CANDIDATES for g in GRAPH_CANDIDATES]
-                           + [(3, t, 0) for t in TILE_CANDIDATES]
-                           + [(2, (0, 0), g) for g in GRAPH_CANDIDATES])
+    cands = candidates or ([(1, t, g, 0) for t in TILE_CANDIDATES for g in GRAPH_CANDIDATES]
+                           + [(3, t, 0, 0) for t in TILE_CANDIDATES]
+                           + [(2, (0, 0), g, sb) for g in GRAPH_CANDIDATES for sb in STRIP_BAND_CANDIDATES])
     best, best_t = None, float("inf")
     stream = torch.cuda.Stream()
-    for kernel, tile, chunk in cands:
-        b = Batch(tile=tile if kernel in (1, 3) else (8, 8), graph_chunk=chunk, kernel=kernel)
+    for cand in cands:
+        kernel, tile, chunk, bands = tuple(cand) + (0,) * (4 - len(cand))
+        b = Batch(tile=tile if kernel in (1, 3) else (8, 8), graph_chunk=chunk, kernel=kernel,
+                  strip_bands=bands)
         try:
             with torch.cuda.stream(stream):
                 b.run(proxy_specs())  # warm-up (plan lists, graph instantiation)
@@ -79,12 +85,13 @@ def tune(specs, nt_proxy=48, repeats=2, candidates=None, verbose=False):
         except (ValueError, RuntimeError):
             continue
         if verbose:
-            print(f"kernel={kernel} tile={tile} graph_chunk={chunk}: {1e3 * el:.2f} ms")
+            print(f"kernel={kernel} tile={tile} graph_chunk={chunk} strip_bands={bands}: {1e3 * el:.2f} ms")
         if el < best_t:
-            best_t, best = el, (kernel, tile, chunk)
-    kernel, tile, chunk = best
+            best_t, best = el, (kernel, tile, chunk, bands)
+    kernel, tile, chunk, bands = best
     # ckpt_k 0: the library picks the checkpoint interval and group split at run time
-    res = {"kernel": kernel, "tile": tile, "graph_chunk": chunk, "ckpt_k": 0, "proxy_ms": 1e3 * best_t}
+    res = {"kernel": kernel, "tile": tile, "graph_chunk": chunk, "strip_bands": bands, "ckpt_k": 0,
+           "proxy_ms": 1e3 * best_t}
     _cache[key] = res
     return res
 
@@ -93,4 +100,4 @@ def tuned_batch(specs, **kw):
     """A ``Batch`` configured by ``tune`` (checkpointing stays automatic)."""
     cfg = tune(specs, **kw)
     return Batch(tile=cfg["tile"] if cfg["kernel"] in (1, 3) else (8, 8), graph_chunk=cfg["graph_chunk"],
-                 kernel=cfg["kernel"]), cfg
+                 kernel=cfg["kernel"], strip_bands=cfg["strip_bands"]), cfg

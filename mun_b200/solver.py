@@ -70,7 +70,10 @@ def choose_ckpt_k(plan, n_solves, budget_bytes=None):
 class Batch:
     """Owns a ``sem_batch_t`` (workspace arena, descriptors, tick counter)."""
 
-    def __init__(self, tile=(0, 0), threads=256, graph_chunk=0, kernel=0, strip_bands=0):
+    def __init__(self, tile=(0, 0), threads=256, graph_chunk=0, kernel=0, strip_bands=0, autotune=False):
+        """``autotune=True``: each ``run`` takes its kernel, tile shape or strip chunk height
+        and graph chunk from ``mun_b200.autotune.tune`` for the batch's signature (timed once
+        per signature on a short proxy, then cached); results do not depend on the choice."""
         lib = _lib.load()
         h = C.c_void_p()
         _lib.check(lib.sem_batch_create(C.byref(h)))
@@ -78,6 +81,8 @@ class Batch:
         self.tile, self.threads, self.graph_chunk = tuple(tile), int(threads), int(graph_chunk)
         self.kernel = int(kernel)  # 0 auto, 1 tile, 2 strip, 3 persistent tile
         self.strip_bands = int(strip_bands)  # strip kernel: element rows per CTA (0 auto)
+        self.autotune = bool(autotune)
+        self.last_tuned = None
         self._side = None
 
     def __del__(self):
@@ -126,6 +131,15 @@ class Batch:
 
     def run(self, specs, tile=None, graph_chunk=None, memory_budget=None, kernel=None):
         n = len(specs)
+        strip_bands = self.strip_bands
+        if self.autotune and n:
+            from .autotune import tune
+            cfg = tune(specs)
+            self.last_tuned = cfg
+            kernel = cfg["kernel"] if kernel is None else kernel
+            tile = (cfg["tile"] if cfg["kernel"] in (1, 3) else (8, 8)) if tile is None else tile
+            graph_chunk = cfg["graph_chunk"] if graph_chunk is None else graph_chunk
+            strip_bands = cfg["strip_bands"]
         arr = (_lib.Solve * max(n, 1))()
         keep = []
         for i, s in enumerate(specs):
@@ -179,7 +193,7 @@ class Batch:
         t = tile or self.tile
         cfg = _lib.LaunchCfg(int(t[0]), int(t[1]), self.threads,
                              int(self.graph_chunk if graph_chunk is None else graph_chunk),
-                             int(self.kernel if kernel is None else kernel), self.strip_bands,
+                             int(self.kernel if kernel is None else kernel), int(strip_bands),
                              int(memory_budget or 0))
         cur = torch.cuda.current_stream()
         if cfg.graph_chunk > 0 and cur.cuda_stream == 0:

@@ -29,3 +29,21 @@ def test_tuned_configuration_gives_the_same_numbers():
     b.run(sp)
     for a, c in zip(ref, sp):
         assert torch.equal(a.grad, c.grad) and torch.equal(a.rec, c.rec)
+
+
+def test_batch_autotune_option_gives_the_same_numbers():
+    g = load("inject_n2")
+    plan = plan_for(g["config"], g["dt"], g["nt"])
+    y = dev(aligned_obs(g))
+
+    def specs():
+        return [SolveSpec(plan, dev(np.asarray(g["velocity"]) * (1 - 0.01 * i)), adjoint=True, y_obs=y,
+                          inv_sigma2=1e6, ckpt_k=0) for i in range(5)]
+    ref = specs()
+    Batch().run(ref)
+    b = Batch(autotune=True)
+    sp = specs()
+    b.run(sp)
+    assert b.last_tuned is not None and b.last_tuned["strip_bands"] in (0, 4, 8)
+    for a, c in zip(ref, sp):
+        assert torch.equal(a.grad, c.grad) and torch.equal(a.rec, c.rec) and torch.equal(a.loglik, c.loglik)
