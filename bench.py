@@ -558,6 +558,15 @@ def run_single(args, steps=None, warmup=None, cpu_sample=None, emit=True):
     # fits, so there is no replay
     m_auto, s2, ticks_auto, tick_ms_auto = timed(0)
     same = bool(torch.equal(s.grad, s2.grad) and torch.equal(s.rec, s2.rec))
+    # the same automatic schedule in one cooperative launch (persistent strip kernel)
+    b_auto = b
+    b = Batch(kernel=4)
+    m_pers, s3, _, _ = timed(0)
+    pers = {"ms_per_solve": m_pers, "solves_per_s": 1e3 / m_pers, "kernel": b.last_kernel,
+            "bitwise_equal": bool(torch.equal(s3.grad, s2.grad) and torch.equal(s3.rec, s2.rec)),
+            "hbm_frac_56B": BYTES_PER_NODE_STEP_FWDADJ * plan.npoints * nt / (m_pers / 1e3) / 1e9
+            / float(peaks()[0].get("hbm_gbs", 6650.0))}
+    b = b_auto
     alg = BYTES_PER_NODE_STEP_FWDADJ * plan.npoints * nt
     pk, pk_kind = peaks()
     peak = float(pk.get("hbm_gbs", 6650.0))
@@ -582,8 +591,8 @@ def run_single(args, steps=None, warmup=None, cpu_sample=None, emit=True):
            "mnode_steps_per_s": plan.npoints * nt / (m / 1e3) / 1e6,
            "achieved_gbs_56B": alg / (m / 1e3) / 1e9, "hbm_frac_56B": alg / (m / 1e3) / 1e9 / peak,
            "peak_kind": pk_kind, "ticks": ticks_k250, "tick_loop_ms": tick_ms,
-           "auto_schedule": auto, "cpu": cpu,
-           "status": int(s.status.item()) | int(s2.status.item())}
+           "auto_schedule": auto, "persistent_strip": pers, "cpu": cpu,
+           "status": int(s.status.item()) | int(s2.status.item()) | int(s3.status.item())}
     if emit:
         print(json.dumps(out), flush=True)
     return out

@@ -119,8 +119,12 @@ typedef struct {
                                  (the tile kernel's ticks in one cooperative launch with
                                  a grid barrier between ticks, for one-order groups
                                  whose tiles are all resident at once; otherwise the
-                                 tile kernel per tick); auto picks strips when the
-                                 batch has at least one strip per SM                   */
+                                 tile kernel per tick), 4 persistent strip kernel (the
+                                 strip kernel's ticks in one cooperative launch, each CTA
+                                 waiting only for its four neighbours' previous tick, for
+                                 one-order groups whose chunks are all resident at once;
+                                 otherwise the strip kernel per tick); auto picks strips
+                                 when the batch has at least one strip per SM            */
   int32_t strip_bands;        /* strip kernel: element rows per CTA; 0 = automatic
                                  (full-height strips when the batch's strips give 2
                                  CTAs per SM, else chunks of >= 4 rows so that strips
@@ -162,7 +166,8 @@ int64_t sem_batch_last_ticks(const sem_batch_t* batch);
  * around each group's tick launches; set-up and output kernels excluded), in ms.
  * Waits for those events. */
 int sem_batch_last_tick_ms(const sem_batch_t* batch, double* ms_out);
-/* kernel variant used by the last sem_run: 1 tile, 2 strip, 3 persistent tile */
+/* kernel variant used by the last sem_run: 1 tile, 2 strip, 3 persistent tile,
+ * 4 persistent strip */
 int32_t sem_batch_last_kernel(const sem_batch_t* batch);
 
 /* Single-solve conveniences (plain path): forward with receivers in the run()

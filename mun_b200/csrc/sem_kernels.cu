@@ -925,7 +925,7 @@ __device__ __forceinline__ void load_seg_all(const float* p, bool valid, bool fr
 // the other's branches.  A chunk below the first starts with a halo band (element row
 // zb0 - 1): only its z-line segments (the carry into row zb0 * N) and its adjoint
 // injection carry are computed there; the chunk above owns that band.
-template <int N, bool ADJ>
+template <int N, bool ADJ, bool COH>
 __device__ __forceinline__ void strip_tick(const SolveDev& S, const int act, const int t,
                                            const int seg, float* smem, int* s_abort) {
   constexpr int NP = N + 1;
@@ -1163,11 +1163,13 @@ __device__ __forceinline__ void strip_tick(const SolveDev& S, const int act, con
     }
     if (ADJ && in_win && j1 > j0) {  // adjoint source of receivers in this element row
       const int cnt = j1 - j0;
-      const double ascale = *S.adj_scale;
+      // (COH: written by other CTAs of this launch, read past L1)
+      const double ascale = COH ? __ldcg(S.adj_scale) : *S.adj_scale;
       const long long yrow = (long long)((t - S.it0) / S.decim) * S.nrec;
       for (int q = tid; q < cnt; q += NT) {
         const int r = S.inj_tile_ids[j0 + q];
-        const double res = (double)S.rec_out[(long long)t * S.nrec + r] - S.yobs[yrow + r];
+        const float* rp = S.rec_out + (long long)t * S.nrec + r;
+        const double res = (double)(COH ? __ldcg(rp) : *rp) - S.yobs[yrow + r];
         sres[q] = (float)(res * ascale);
       }
       __syncthreads();
@@ -1440,9 +1442,9 @@ __global__ void __launch_bounds__(kStripCols, (N <= 4) ? SEM_STRIP_MIN_BLOCKS : 
     return;
   }
   if (act == A_ADJ)
-    strip_tick<N, true>(S, act, t, seg, smem, &s_abort);
+    strip_tick<N, true, false>(S, act, t, seg, smem, &s_abort);
   else
-    strip_tick<N, false>(S, act, t, seg, smem, &s_abort);
+    strip_tick<N, false, false>(S, act, t, seg, smem, &s_abort);
 }
 
 // ----------------------------------------------------------------------------
@@ -1507,6 +1509,114 @@ __global__ void __launch_bounds__(256) sem_persist_kernel(const SolveDev* __rest
     if (!grid_barrier(bar, target, &s_ok)) {
       if (threadIdx.x == 0) atomicOr(S.status, SEM_ERR_TIMEOUT);
       return;
+    }
+  }
+}
+
+// ----------------------------------------------------------------------------
+// persistent strip kernel: one cooperative launch runs the whole tick program of a group
+// of strip chunks that are all resident at once (a single large solve, or a few), so a
+// tick costs no launch and no grid drain.  A CTA starts tick t when its four neighbours
+// (strips left and right, chunks above and below: the only CTAs whose nodes its bands
+// read and use) have published tick t - 1; the adjoint-scale tick of a solve takes a
+// barrier over that solve's CTAs before and after it.  Every wait is bounded (kWaitNs)
+// and ends the launch with SEM_ERR_TIMEOUT.  Bitwise the same arithmetic as the per-tick
+// strip kernel (the same strip_tick, with loads of data this launch wrote taken past L1).
+// ----------------------------------------------------------------------------
+__device__ __forceinline__ unsigned ld_acquire_u32(const unsigned* p) {
+  unsigned v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void st_release_u32(unsigned* p, unsigned v) {
+  asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+// true once every CTA nb[0..nn) has published at least `want` ticks; false after kWaitNs
+__device__ __forceinline__ bool wait_neighbours(const unsigned* done, const int* nb, int nn,
+                                                unsigned want) {
+  const long long t0 = global_ns();
+  for (int i = 0; i < nn; ++i)
+    while (ld_acquire_u32(done + nb[i]) < want)
+      if (global_ns() - t0 > kWaitNs) return false;
+  return true;
+}
+
+template <int N>
+__global__ void __launch_bounds__(kStripCols, (N <= 4) ? SEM_STRIP_MIN_BLOCKS : 3)
+    sem_strip_persist_kernel(const SolveDev* __restrict__ solves, const int* __restrict__ cta_solve,
+                             int tick0, int tick1, unsigned* __restrict__ done,
+                             unsigned long long* __restrict__ sbar) {
+  extern __shared__ __align__(128) float smem[];
+  __shared__ SolveDev S;
+  __shared__ int s_act, s_t, s_seg, s_abort, s_ok;
+  __shared__ int s_nb[4], s_nn, s_local;           // neighbour CTAs (kept out of registers)
+  __shared__ unsigned long long s_arrivals, s_per_solve;
+  const int sid = cta_solve[blockIdx.x];
+  {
+    const unsigned long long* src = reinterpret_cast<const unsigned long long*>(solves + sid);
+    unsigned long long* dst = reinterpret_cast<unsigned long long*>(&S);
+    for (int i = threadIdx.x; i < (int)(sizeof(SolveDev) / 8); i += kStripCols) dst[i] = src[i];
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const int zch = S.zchunk > 0 ? S.zchunk : S.nelz;
+    const int nzc = (S.nelz + zch - 1) / zch;
+    const int local = blockIdx.x - S.tile_base;
+    const int strip = local / nzc, chunk = local - strip * nzc;
+    int nn = 0;
+    if (strip > 0) s_nb[nn++] = blockIdx.x - nzc;
+    if (strip + 1 < S.tiles_x) s_nb[nn++] = blockIdx.x + nzc;
+    if (chunk > 0) s_nb[nn++] = blockIdx.x - 1;
+    if (chunk + 1 < nzc) s_nb[nn++] = blockIdx.x + 1;
+    s_nn = nn;
+    s_local = local;
+    s_per_solve = (unsigned long long)S.tiles_x * nzc;
+    s_arrivals = 0;  // this solve's barrier target so far
+  }
+  __syncthreads();
+  for (int tick = tick0; tick < tick1; ++tick) {
+    if (threadIdx.x == 0) {
+      int act, t, seg;
+      decode(S, tick - S.start_tick, act, t, seg);
+      s_act = act; s_t = t; s_seg = seg; s_abort = 0x7fffffff;
+    }
+    __syncthreads();
+    const int act = s_act;
+    bool ok = true;
+    if (act == A_SCALE) {
+      // every CTA of the solve has read out its receivers; one picks the scale; all see it
+      const unsigned long long a1 = s_arrivals + s_per_solve, a2 = a1 + s_per_solve;
+      ok = grid_barrier(sbar + sid, a1, &s_ok);
+      if (ok && s_local == 0 && threadIdx.x == 0) {
+        double m = 0.0;
+        for (int r = 0; r < S.nrec; ++r) m = fmax(m, __ldcg(S.rmax + r));
+        *S.adj_scale = (m > 0.0 && isfinite(m)) ? ldexp(1.0, -ilogb(m)) : 1.0;
+      }
+      ok = ok && grid_barrier(sbar + sid, a2, &s_ok);
+      if (threadIdx.x == 0) s_arrivals = a2;
+    } else if (act != A_NONE) {
+      if (threadIdx.x == 0) s_ok = wait_neighbours(done, s_nb, s_nn, (unsigned)(tick - tick0)) ? 1 : 0;
+      __syncthreads();
+      ok = s_ok != 0;
+      if (ok) {
+        // the neighbours' generic-proxy stores come before this tick's bulk / tensor loads
+        asm volatile("fence.proxy.async.global;" ::: "memory");
+        if (act == A_ADJ)
+          strip_tick<N, true, true>(S, act, s_t, s_seg, smem, &s_abort);
+        else
+          strip_tick<N, false, true>(S, act, s_t, s_seg, smem, &s_abort);
+        __syncthreads();
+        if (s_abort != 0x7fffffff) return;  // a copy wait gave up: status set, copies drained
+      }
+    }
+    if (!ok) {
+      if (threadIdx.x == 0) atomicOr(S.status, SEM_ERR_TIMEOUT);
+      return;
+    }
+    __syncthreads();  // every thread's stores of this tick are issued
+    if (threadIdx.x == 0) {
+      __threadfence();
+      st_release_u32(done + blockIdx.x, (unsigned)(tick - tick0 + 1));
     }
   }
 }
@@ -1888,6 +1998,20 @@ KernelFn kernel_for(int N) {
   return nullptr;
 }
 
+typedef void (*StripPersistFn)(const SolveDev*, const int*, int, int, unsigned*, unsigned long long*);
+StripPersistFn strip_persist_kernel_for(int N) {
+  switch (N) {
+    case 1: return sem_strip_persist_kernel<1>;
+    case 2: return sem_strip_persist_kernel<2>;
+    case 3: return sem_strip_persist_kernel<3>;
+    case 4: return sem_strip_persist_kernel<4>;
+    case 5: return sem_strip_persist_kernel<5>;
+    case 6: return sem_strip_persist_kernel<6>;
+    case 7: return sem_strip_persist_kernel<7>;
+  }
+  return nullptr;
+}
+
 typedef void (*PersistFn)(const SolveDev*, const int*, int, int, int, int, unsigned long long*);
 PersistFn persist_kernel_for(int N) {
   switch (N) {
@@ -2004,6 +2128,8 @@ struct sem_batch_s {
   CUtensorMap* d_tmaps = nullptr;       // strip kernel: band-load tensor map of each solve
   int tmaps_cap = 0;
   std::vector<CUtensorMap> h_tmaps;
+  char* d_sync = nullptr;               // persistent strip kernel: per-CTA tick counters and
+  long long sync_cap = 0;               //   per-solve barrier counters
 };
 
 extern "C" {
@@ -2134,6 +2260,7 @@ int sem_batch_destroy(sem_batch_t* b) {
   for (cudaEvent_t e : b->tick_ev) cudaEventDestroy(e);
   cudaFree(b->d_io);
   cudaFree(b->arena); cudaFree(b->d_tick); cudaFree(b->d_solves); cudaFree(b->d_cta); cudaFree(b->d_tmaps);
+  cudaFree(b->d_sync);
   delete b;
   return SEM_OK;
 }
@@ -2182,7 +2309,7 @@ static int run_group(sem_batch_t* b, const sem_solve_t* solves, int32_t n,
     min_chunk_ctas += (long long)ns * ((p->nelz + kMinChunk - 1) / kMinChunk);
     nelz_max = std::max(nelz_max, p->nelz);
   }
-  bool use_strip = (cfg.kernel == 2);
+  bool use_strip = (cfg.kernel == 2 || cfg.kernel == 4);
   if (cfg.kernel == 0) use_strip = strip_fills(min_chunk_ctas, sms);
   const int zchunk = use_strip ? strip_zchunk(total_strips, nelz_max, sms, cfg.strip_bands) : 0;
   b->last_kernel = use_strip ? 2 : 1;
@@ -2451,7 +2578,45 @@ static int run_group(sem_batch_t* b, const sem_solve_t* solves, int32_t n,
     }
     cudaGetLastError();  // a refused occupancy query leaves the per-tick path
   }
-  b->last_kernel = persisted ? 3 : b->last_kernel;
+  // persistent strip kernel: one cooperative launch over every chunk of a one-order group,
+  // when all of them are resident at once (else per-tick strip launches)
+  if (cfg.kernel == 4 && use_strip && launches.size() == 1) {
+    const Launch& Lc = launches[0];
+    StripPersistFn pf = strip_persist_kernel_for(Lc.N);
+    int nb = 0;
+    const long long sync_bytes = round_up(Lc.ncta * 4, 256) + round_up((long long)n * 8, 256);
+    if (pf && raise_smem_limit((const void*)pf, Lc.smem) == cudaSuccess &&
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, pf, strip_threads(Lc.N), Lc.smem) == cudaSuccess &&
+        (long long)nb * sms >= Lc.ncta) {
+      if (sync_bytes > b->sync_cap) {
+        cudaFree(b->d_sync);
+        b->d_sync = nullptr;
+        b->sync_cap = 0;
+        CUDA_TRY(cudaMalloc((void**)&b->d_sync, sync_bytes));
+        b->sync_cap = sync_bytes;
+      }
+      CUDA_TRY(cudaMemsetAsync(b->d_sync, 0, sync_bytes, stream));
+      unsigned* done = reinterpret_cast<unsigned*>(b->d_sync);
+      unsigned long long* sbar =
+          reinterpret_cast<unsigned long long*>(b->d_sync + round_up(Lc.ncta * 4, 256));
+      cudaLaunchConfig_t lc = {};
+      lc.gridDim = dim3((unsigned)Lc.ncta);
+      lc.blockDim = dim3(strip_threads(Lc.N));
+      lc.dynamicSmemBytes = Lc.smem;
+      lc.stream = stream;
+      cudaLaunchAttribute at[1];
+      at[0].id = cudaLaunchAttributeCooperative;
+      at[0].val.cooperative = 1;
+      lc.attrs = at;
+      lc.numAttrs = 1;
+      CUDA_TRY(cudaLaunchKernelEx(&lc, pf, gdesc[0], (const int*)(b->d_cta + Lc.cta0), 0, max_prog, done, sbar));
+      b->last_launches += 1;
+      persisted = true;
+      b->last_kernel = 4;
+    }
+    cudaGetLastError();  // a refused occupancy query leaves the per-tick path
+  }
+  b->last_kernel = (persisted && b->last_kernel != 4) ? 3 : b->last_kernel;
   if (!persisted && cfg.graph_chunk > 0 && stream != nullptr && stream != cudaStreamLegacy &&
       stream != cudaStreamPerThread) {
     cudaGraph_t graph = nullptr;
@@ -2590,7 +2755,7 @@ int auto_schedule(const sem_solve_t* sv, int n, const sem_launch_cfg_t& cfg, lon
         nchunk_min += strips[i] * ((s.plan->nelz + kMinChunk - 1) / kMinChunk);
         nelz_max = std::max(nelz_max, s.plan->nelz);
       }
-      const bool strip = cfg.kernel == 2 || (cfg.kernel == 0 && strip_fills(nchunk_min, sms));
+      const bool strip = cfg.kernel == 2 || cfg.kernel == 4 || (cfg.kernel == 0 && strip_fills(nchunk_min, sms));
       long long nstrip_ctas = 0;
       if (strip) {
         const int zc = strip_zchunk(nstrip, nelz_max, sms, cfg.strip_bands);
@@ -2625,8 +2790,9 @@ int sem_run(sem_batch_t* b, const sem_solve_t* solves, int32_t n, const sem_laun
   sem_launch_cfg_t cfg = cfg_in ? *cfg_in : sem_launch_cfg_t{0, 0, 256, 0, 0, 0, 0};
   if (!(cfg.tile_ex == 0 && cfg.tile_ez == 0) && (cfg.tile_ex < 1 || cfg.tile_ez < 1))
     return fail(SEM_ERR_ARG, "tile size must be >= 1 (or 0 x 0: automatic)");
-  if (cfg.kernel < 0 || cfg.kernel > 3)
-    return fail(SEM_ERR_ARG, "kernel must be 0 (auto), 1 (tile), 2 (strip), 3 (persistent tile)");
+  if (cfg.kernel < 0 || cfg.kernel > 4)
+    return fail(SEM_ERR_ARG,
+                "kernel must be 0 (auto), 1 (tile), 2 (strip), 3 (persistent tile), 4 (persistent strip)");
   if (cfg.threads < 32 || cfg.threads > 256 || cfg.threads % 32) cfg.threads = 256;
   if (cfg.memory_budget < 0) return fail(SEM_ERR_ARG, "memory_budget must be >= 0");
   if (cfg.strip_bands < 0) return fail(SEM_ERR_ARG, "strip_bands must be >= 0");

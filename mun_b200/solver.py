@@ -79,7 +79,7 @@ class Batch:
         _lib.check(lib.sem_batch_create(C.byref(h)))
         self.handle, self._lib = h, lib
         self.tile, self.threads, self.graph_chunk = tuple(tile), int(threads), int(graph_chunk)
-        self.kernel = int(kernel)  # 0 auto, 1 tile, 2 strip, 3 persistent tile
+        self.kernel = int(kernel)  # 0 auto, 1 tile, 2 strip, 3 persistent tile, 4 persistent strip
         self.strip_bands = int(strip_bands)  # strip kernel: element rows per CTA (0 auto)
         self.autotune = bool(autotune)
         self.last_tuned = None
@@ -126,8 +126,8 @@ class Batch:
 
     @property
     def last_kernel(self):
-        return {1: "tile", 2: "strip", 3: "persistent"}.get(int(self._lib.sem_batch_last_kernel(self.handle)),
-                                                            "none")
+        return {1: "tile", 2: "strip", 3: "persistent", 4: "persistent strip"}.get(
+            int(self._lib.sem_batch_last_kernel(self.handle)), "none")
 
     def run(self, specs, tile=None, graph_chunk=None, memory_budget=None, kernel=None):
         n = len(specs)

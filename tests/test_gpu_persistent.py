@@ -72,3 +72,46 @@ def test_persistent_falls_back_when_tiles_are_not_resident():
     b.run(got)
     assert b.last_kernel == "tile"
     _same(ref, got)
+
+
+@pytest.mark.parametrize("name", ["inject_n1", "inject_n3", "inject_n6", "circle_n5", "layered_cfg0"])
+@pytest.mark.parametrize("bands", [0, 2])
+def test_persistent_strip_equals_strip_kernel(name, bands):
+    """Persistent strip kernel (kernel 4): the strip kernel's tick body for the whole tick
+    program in one cooperative launch, CTAs synchronised with their four neighbours only;
+    bitwise the per-tick strip kernel, with full-height strips and with 2-row chunks (the
+    chunks above and below are neighbours too), replay (k = 5) and several solves."""
+    g = load(name)
+    plan = plan_for(g["config"], g["dt"], g["nt"])
+    a = _specs(g, plan, 3)
+    Batch(kernel=2, strip_bands=bands).run(a)
+    b = _specs(g, plan, 3)
+    bb = Batch(kernel=4, strip_bands=bands)
+    bb.run(b)
+    torch.cuda.synchronize()
+    assert bb.last_kernel == "persistent strip"
+    _same(a, b)
+
+
+def test_persistent_strip_stacey_and_forward_only():
+    from mun_b200 import SEMPlan
+    import numpy as np
+    g = load("layered_cfg0")
+    cfg = g["config"]
+    d = cfg["domain"]
+    from tests.gpu_cases import receivers_of, sponge_cmax
+    plan = SEMPlan(xmin=d["xmin"], xmax=d["xmax"], zmin=d["zmin"], zmax=d["zmax"], nelx=d["nelem_x"],
+                   nelz=d["nelem_z"], npol=cfg["method"]["polynomial_order"], dt=float(g["dt"]), nt=int(g["nt"]),
+                   src_xz=cfg["source"]["position"], f0=cfg["source"]["frequency"],
+                   amp=cfg["source"]["amplitude"], receivers=receivers_of(cfg),
+                   pml_thickness=cfg["method"]["pml_thickness"], sponge_cmax=sponge_cmax(cfg), boundary="stacey")
+    for adjoint in (True, False):
+        a = _specs(g, plan, 2, adjoint=adjoint, ckpt_k=0)
+        Batch(kernel=2, strip_bands=3).run(a)
+        b = _specs(g, plan, 2, adjoint=adjoint, ckpt_k=0)
+        bb = Batch(kernel=4, strip_bands=3)
+        bb.run(b)
+        torch.cuda.synchronize()
+        assert bb.last_kernel == "persistent strip"
+        _same(a, b, adjoint)
+        assert np.isfinite(b[0].rec.cpu().numpy()).all()
