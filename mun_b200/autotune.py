@@ -1,7 +1,7 @@
 """Launch-configuration autotuner.
 
-Picks the kernel variant (tile kernel with a tile shape, persistent tile kernel, or strip
-kernel) and the CUDA-graph chunk for a batch by timing candidates on a short proxy of the
+Picks the kernel variant (tile kernel with a tile shape, persistent tile kernel, strip
+kernel or persistent strip kernel, with the strip chunk height) and the CUDA-graph chunk for a batch by timing candidates on a short proxy of the
 batch: the same meshes, orders, receivers and velocities with a few dozen time steps.
 The checkpoint interval and group split stay with the library's memory-budget schedule.
 The choice is cached per batch signature (mesh sizes, orders, solve count, adjoint or
@@ -20,6 +20,7 @@ from .solver import Batch, SolveSpec
 TILE_CANDIDATES = [(0, 0), (8, 8), (16, 8), (8, 4), (16, 4), (4, 4), (2, 2)]  # (0, 0): automatic
 GRAPH_CANDIDATES = [0, 32]
 STRIP_BAND_CANDIDATES = [0, 4, 8]  # strip kernel: element rows per CTA (0: automatic)
+PERSIST_STRIP_BAND_CANDIDATES = [0, 2, 4]  # persistent strip kernel (one launch for all ticks)
 
 _cache = {}
 
@@ -62,7 +63,8 @@ def tune(specs, nt_proxy=48, repeats=2, candidates=None, verbose=False):
     # per-tick tile launches by itself when the tiles are not all resident
     cands = candidates or ([(1, t, g, 0) for t in TILE_CANDIDATES for g in GRAPH_CANDIDATES]
                            + [(3, t, 0, 0) for t in TILE_CANDIDATES]
-                           + [(2, (0, 0), g, sb) for g in GRAPH_CANDIDATES for sb in STRIP_BAND_CANDIDATES])
+                           + [(2, (0, 0), g, sb) for g in GRAPH_CANDIDATES for sb in STRIP_BAND_CANDIDATES]
+                           + [(4, (0, 0), 0, sb) for sb in PERSIST_STRIP_BAND_CANDIDATES])
     best, best_t = None, float("inf")
     stream = torch.cuda.Stream()
     for cand in cands:
