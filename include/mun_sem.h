@@ -64,17 +64,17 @@ typedef struct {
   const int64_t* node_grid; /* [npoints] gz*nxg+gx of each node in reference order    */
   const double* gll_D;      /* [(npol+1)^2] D[a*(npol+1)+b] = l_b'(xi_a)              */
   const double* gll_beta;   /* [npol+1] w_a * l_a  (GLL weight x Lagrange quirk factor)*/
-  const double* tab_x;      /* [3*nxg] 1/mx, Rx, sponge factor along x                */
-  const double* tab_z;      /* [3*nzg] dt^2/(J mz), Rz, sponge factor along z         */
+  const double* tab_x;      /* [3*nxg] 1/mx, Rx, 1 - sponge decay factor along x     */
+  const double* tab_z;      /* [3*nzg] dt^2/(J mz), Rz, 1 - sponge decay along z     */
   const double* src_term;   /* [nt] dt^2 * s(t_it) added at the source node           */
   int32_t src_gx, src_gz;   /* source node (structured index)                         */
   int32_t nrec;
   const int32_t* rec_base;  /* [nrec*2] (gx0,gz0) first node of the receiver element  */
   const double* rec_w;      /* [nrec*(npol+1)^2] Lagrange weights, index j*(npol+1)+i */
-  /* Boundary mode.  0: the reference's sponge (its decay is the third row of tab_x and
+  /* Boundary mode.  0: the reference's sponge (1 - its decay is the third row of tab_x and
    * tab_z).  1: an extension without counterpart in the reference: first-order Stacey
    * absorbing edges on the sides and the bottom and a free surface (u = 0) on the top row;
-   * tab_x / tab_z then carry no decay (third rows 1).  The forward becomes
+   * tab_x / tab_z then carry no decay (third rows 0).  The forward becomes
    *   (1 + a) u+ = 2 u - (1 - a) u- + dt^2 M^-1 (f - K u),  a = c alpha on the absorbing
    * edges, and the adjoint is its exact discrete adjoint: the same recurrence run
    * backwards, with a boundary-impedance term in the gradient (from d a / d c): at each

@@ -245,7 +245,8 @@ __device__ __forceinline__ void misfit_add(double* m, double res) { *m = __dadd_
 // One owned node: combine the line operators, advance (b, v) or (lambda, mu), apply
 // the sponge.  Shared by both kernel variants so their arithmetic is identical.
 //   forward:  w = v - P K + src          adjoint: w = mu + P (inj - K)
-//   v' = d w, b' = d (b + w)   (d = 1 in the reference-mode adjoint)
+//   v' = d w, b' = d (b + w)   (d = 1 in the reference-mode adjoint), with d = 1 - delta
+//   applied as w - delta w and s - delta s (dxv, dzv: the tables' decay defects)
 __device__ __forceinline__ void advance_node(bool adj, bool damp, float b, float v, float X,
                                              float Z, float ixv, float Rxv, float dxv, float izv,
                                              float Rzv, float dzv, float extra, float& bout,
@@ -261,9 +262,12 @@ __device__ __forceinline__ void advance_node(bool adj, bool damp, float b, float
     wv = __fmaf_rn(P, __fsub_rn(extra, Kv), v);
   }
   if (damp) {
-    const float d = __fmul_rn(dxv, dzv);
-    vout = __fmul_rn(d, wv);
-    bout = __fmul_rn(d, __fadd_rn(b, wv));
+    // sponge: the decay d = (1 - dx)(1 - dz) applied as s - delta s, delta = 1 - d from the
+    // tables' defects (a float32 decay just below 1 would be a fixed bias every step)
+    const float dl = __fmaf_rn(-dxv, dzv, __fadd_rn(dxv, dzv));
+    vout = __fmaf_rn(-dl, wv, wv);
+    const float s = __fadd_rn(b, wv);
+    bout = __fmaf_rn(-dl, s, s);
   } else {
     vout = wv;
     bout = __fadd_rn(b, wv);
@@ -765,6 +769,10 @@ __global__ void __launch_bounds__(256) sem_tick_kernel(const SolveDev* __restric
 #ifndef SEM_STAGES_ADJ
 #define SEM_STAGES_ADJ 3
 #endif
+// adjoint ticks: D (lambda) and D (forward field) of a segment in packed FFMA2
+#ifndef SEM_PAIRED_ADJ
+#define SEM_PAIRED_ADJ 1
+#endif
 #ifndef SEM_STRIP_MIN_BLOCKS
 #define SEM_STRIP_MIN_BLOCKS 4
 #endif
@@ -800,6 +808,14 @@ __device__ __forceinline__ uint32_t smem_addr(const void* p) {
 }
 __device__ __forceinline__ void mbar_init(unsigned long long* bar, unsigned count) {
   asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
+}
+// 4-byte asynchronous global -> shared copies (the Stacey edge values, a band ahead)
+__device__ __forceinline__ void cp_async4(void* dst, const void* src) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(smem_addr(dst)), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+__device__ __forceinline__ void mbar_inval(unsigned long long* bar) {
+  asm volatile("mbarrier.inval.shared::cta.b64 [%0];" ::"r"(smem_addr(bar)) : "memory");
 }
 __device__ __forceinline__ void mbar_expect_tx(unsigned long long* bar, unsigned bytes) {
   asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)),
@@ -880,6 +896,8 @@ __host__ __device__ inline long long strip_xch_floats(int N, bool adj) {
   if (adj) f += NP * kStripCols + kStripInj;                         // inj | res
   return (f + 31) & ~31LL;
 }
+constexpr int kStripBndSide = 3 * 2 * 5 * 8;                   // Stacey edge values by band
+constexpr int kStripBndFloats = kStripBndSide + 5 * kStripCols;  // + the bottom row
 __host__ __device__ inline long long strip_smem_floats(int N, bool adj) {
   const long long fwd = kStages * strip_stage_floats(N, false) + strip_xch_floats(N, false);
   const long long adjf = kStagesAdj * strip_stage_floats(N, true) + strip_xch_floats(N, true);
@@ -925,7 +943,7 @@ __device__ __forceinline__ void load_seg_all(const float* p, bool valid, bool fr
 // the other's branches.  A chunk below the first starts with a halo band (element row
 // zb0 - 1): only its z-line segments (the carry into row zb0 * N) and its adjoint
 // injection carry are computed there; the chunk above owns that band.
-template <int N, bool ADJ, bool COH>
+template <int N, bool ADJ, bool COH, bool STC>
 __device__ __forceinline__ void strip_tick(const SolveDev& S, const int act, const int t,
                                            const int seg, float* smem, int* s_abort) {
   constexpr int NP = N + 1;
@@ -969,6 +987,10 @@ __device__ __forceinline__ void strip_tick(const SolveDev& S, const int act, con
   float* const xs0 = stages + NST * stage_f;      // 2 exchange buffers: Xs [NP][SEGS][NP] (+ SXs)
   float* const sacc = xs0 + 2 * XSZ;              // adjoint: injection rows [NP][NT]
   float* const sres = sacc + NP * NT;             // adjoint: band residuals [kStripInj]
+  // Stacey mode: the edge values of a band (e1, e2, g, b_t, b_{t+2}) for the left and right
+  // columns, 3 buffers by band, and of the bottom row, behind the tick kind's own layout
+  float* const sbnd = smem + strip_smem_floats(N, ADJ);  // [3][2 sides][5][8]
+  float* const bbot = sbnd + kStripBndSide;              // [5][NT]
 
   // ---------------- which fields
   const float* cur;
@@ -1046,6 +1068,34 @@ __device__ __forceinline__ void strip_tick(const SolveDev& S, const int act, con
   };
   for (int r = 0; r < min(NST, nbands); ++r) issue(ezs + r);
 
+  // Stacey mode: this CTA's edges (strip 0 owns column 0, the last strip column nxg - 1,
+  // the last chunk row nzg - 1) and the asynchronous fetch of their values one band ahead
+  const bool side_l = STC && sx0 == 0;
+  const bool side_r = STC && so1 == nxg;
+  const bool bottom = STC && zb1 == nelz && !final_only;
+  const bool bgterm = ADJ && t >= S.it0 && t < S.it1 && t <= S.nt - 2;  // impedance term
+  auto bnd_fetch = [&](int ez, int buf) {
+    if (tid < 2 * 5 * NP) {
+      const int sd = tid / (5 * NP), q = (tid / NP) % 5, a = tid % NP;
+      const int gz = ez * N + a;
+      if ((sd == 0 ? side_l : side_r) && (q < 2 || bgterm) && gz > 0 && gz < nzg) {
+        const long long k = (sd == 0 ? 0 : nzg) + gz, BP = S.bnd_pitch;
+        const float* src = q < 3 ? S.bnd_coef + q * BP + k : S.bnd_hist + (q == 3 ? t : t + 2) * BP + k;
+        cp_async4(sbnd + ((buf * 2 + sd) * 5 + q) * 8 + a, src);
+      }
+    }
+  };
+  if (STC) {
+    if (bottom && gx > 0 && gx < nxg - 1 && owned) {
+      const long long k = 2 * nzg + gx, BP = S.bnd_pitch;
+      for (int q = 0; q < (bgterm ? 5 : 2); ++q) {
+        const float* src = q < 3 ? S.bnd_coef + q * BP + k : S.bnd_hist + (q == 3 ? t : t + 2) * BP + k;
+        cp_async4(bbot + q * NT + tid, src);
+      }
+    }
+    if (!final_only) bnd_fetch(ezs, 0);
+  }
+
   // D and beta: per-order constants (c_D[N], c_B[N])
 #define Dr(a, b) c_D[N][(a) * NP + (b)]
 #define Bt(a) c_B[N][(a)]
@@ -1076,7 +1126,7 @@ __device__ __forceinline__ void strip_tick(const SolveDev& S, const int act, con
   const bool g_start = grad_on && grad_partial_starts(S, t);
   const bool g_fold = grad_on && grad_folds(S, t);
   double* const grad64p = S.grad64;
-  const bool stc = S.bnd_n > 0;  // Stacey / free-surface mode
+  constexpr bool stc = STC;  // Stacey / free-surface mode (compiled out of the sponge path)
   const bool in_win = ADJ && t >= S.it0 && t < S.it1 && ((t - S.it0) % S.decim) == 0;
   const int ms = t - ((S.flags & F_SHIFT) ? 1 : 0);
   const bool rec_on = !ADJ && (act == A_FWD || act == A_FINAL) && ms >= 0 && ms < S.nt;
@@ -1128,6 +1178,13 @@ __device__ __forceinline__ void strip_tick(const SolveDev& S, const int act, con
     if (ADJ && grad_on && !g_start && owned && !halo) {
 #pragma unroll
       for (int a = 0; a < N; ++a) gpre[a] = gradp[gb + a * pitch];
+    }
+    if (STC && !final_only) {
+      // this band's edge values (fetched a band ago) are complete once each issuing thread
+      // has waited for its copies; the phase-A barrier publishes them.  The next band's go
+      // to the buffer no thread reads now (phase B of band rel - 1 reads (rel - 1) % 3).
+      cp_async_wait_all();
+      if (rel + 1 < nbands) bnd_fetch(ez + 1, (rel + 1) % 3);
     }
     if (!mbar_wait(bars + slot, (unsigned)((rel / NST) & 1))) atomicMin(s_abort, ez);
     const bool last = (ez == nelz - 1);
@@ -1192,6 +1249,35 @@ __device__ __forceinline__ void strip_tick(const SolveDev& S, const int act, con
     // ---- phase A, x-lines: one thread per (band row, element segment)
     auto xline = [&](int a, int sgi, unsigned m, bool nxt) {
       const int o = a * BW + off + sgi * N;  // column (e0 - 1 + sgi) * N of row a
+      if constexpr (ADJ && SEM_PAIRED_ADJ) {
+        // adjoint ticks: D (lambda) and D (forward field) of the segment as the two halves
+        // of packed FFMA2 (per half the scalar fmaf sequence: bitwise the same)
+        float u[NP], w[NP], c[NP], q[NP];
+        float2 d2[NP];
+        load_seg<N>(Bs + o, u, m, nxt);
+        load_seg<N>(Us + o, w, m, nxt);
+        load_seg<N>(Cs + o, c, m, nxt);
+#pragma unroll
+        for (int a2 = 0; a2 < NP; ++a2) {
+          float2 v = make_float2(0.f, 0.f);
+#pragma unroll
+          for (int b = 0; b < NP; ++b) v = __ffma2_rn(c_D2[N][a2 * NP + b], make_float2(u[b], w[b]), v);
+          d2[a2] = v;
+          q[a2] = Bt(a2) * c[a2] * v.x;
+        }
+        float* xo = Xs + (a * SEGS + sgi) * NP;
+#pragma unroll
+        for (int i = 0; i < NP; ++i) {
+          float v = 0.f;
+#pragma unroll
+          for (int a2 = 0; a2 < NP; ++a2) v = fmaf(Dr(a2, i), q[a2], v);
+          xo[i] = v;
+        }
+        float* so = SXs + (a * SEGS + sgi) * NP;
+#pragma unroll
+        for (int a2 = 0; a2 < NP; ++a2) so[a2] = sens_product(Bt(a2), d2[a2].y, d2[a2].x);
+        return;
+      }
       float u[NP], c[NP], du[NP], q[NP];
       load_seg<N>(Bs + o, u, m, nxt);
       load_seg<N>(Cs + o, c, m, nxt);
@@ -1266,7 +1352,29 @@ __device__ __forceinline__ void strip_tick(const SolveDev& S, const int act, con
         if (last && xitem_last) xline(N, tid, mL, nextL);
       }
       // ---- phase A, z-lines: one thread per owned column (the band is the segment)
-      if (owned) {
+      if (ADJ && SEM_PAIRED_ADJ && owned) {
+        float q[NP];
+        float2 u2[NP], d2[NP];
+#pragma unroll
+        for (int b = 0; b < NP; ++b) u2[b] = make_float2(Bs[b * BW + sc], Us[b * BW + sc]);
+#pragma unroll
+        for (int a2 = 0; a2 < NP; ++a2) {
+          float2 v = make_float2(0.f, 0.f);
+#pragma unroll
+          for (int b = 0; b < NP; ++b) v = __ffma2_rn(c_D2[N][a2 * NP + b], u2[b], v);
+          d2[a2] = v;
+          q[a2] = Bt(a2) * Cs[a2 * BW + sc] * v.x;
+        }
+#pragma unroll
+        for (int j = 0; j < NP; ++j) {
+          float v = 0.f;
+#pragma unroll
+          for (int a2 = 0; a2 < NP; ++a2) v = fmaf(Dr(a2, j), q[a2], v);
+          rz[j] = v;
+        }
+#pragma unroll
+        for (int a2 = 0; a2 < NP; ++a2) sz[a2] = sens_product(Bt(a2), d2[a2].y, d2[a2].x);
+      } else if (owned) {
         float u[NP], du[NP], q[NP];
 #pragma unroll
         for (int b = 0; b < NP; ++b) u[b] = Bs[b * BW + sc];
@@ -1355,7 +1463,15 @@ __device__ __forceinline__ void strip_tick(const SolveDev& S, const int act, con
           if (grad_on) {
             const float gprev = g_start ? 0.f : (a < N ? gpre[a < N ? a : 0] : gradp[g]);
             float inc = sens_increment(Rzv, SX, Rxv, SZ);
-            if (bk >= 0 && t <= S.nt - 2) inc = __fadd_rn(inc, bnd_sens(S, bk, t, Bs[a * BW + sc]));
+            if (STC && bk >= 0 && bgterm) {
+              // g lambda (b_{t+2} - b_t), rounded as bnd_sens
+              const float* bv = (gx == 0 || gx == nxg - 1)
+                                    ? sbnd + (((rel % 3) * 2 + (gx == 0 ? 0 : 1)) * 5) * 8 + a
+                                    : bbot + tid;
+              const int qs = (gx == 0 || gx == nxg - 1) ? 8 : NT;
+              const float du = __fsub_rn(bv[4 * qs], bv[3 * qs]);
+              inc = __fadd_rn(inc, __fmul_rn(__fmul_rn(bv[2 * qs], Bs[a * BW + sc]), du));
+            }
             gnew = __fadd_rn(gprev, inc);
           }
         }
@@ -1363,11 +1479,13 @@ __device__ __forceinline__ void strip_tick(const SolveDev& S, const int act, con
         if (stc && gz == 0) {  // free surface
           res = 0.f;
           vres = 0.f;
-        } else if (bk >= 0) {
-          const long long BP = S.bnd_pitch;
+        } else if (STC && bk >= 0) {
+          const bool sidecol = (gx == 0 || gx == nxg - 1);
+          const float* bv = sidecol ? sbnd + (((rel % 3) * 2 + (gx == 0 ? 0 : 1)) * 5) * 8 + a : bbot + tid;
+          const int qs = sidecol ? 8 : NT;
           advance_node_stacey(ADJ, Bs[a * BW + sc], Vs[a * BW + sc], X, Z, ixv, Rxv, izv, Rzv, extra,
-                              S.bnd_coef[bk], S.bnd_coef[BP + bk], res, vres);
-          if (!ADJ && (S.flags & F_ADJ)) S.bnd_hist[(long long)(t + 1) * BP + bk] = res;
+                              bv[0], bv[qs], res, vres);
+          if (!ADJ && (S.flags & F_ADJ)) S.bnd_hist[(long long)(t + 1) * S.bnd_pitch + bk] = res;
         } else {
           advance_node(ADJ, damp, Bs[a * BW + sc], Vs[a * BW + sc], X, Z, ixv, Rxv, dxv, izv, Rzv,
                        dzv, extra, res, vres);
@@ -1392,6 +1510,7 @@ __device__ __forceinline__ void strip_tick(const SolveDev& S, const int act, con
       }
     }
   }
+  if (STC) cp_async_wait_all();  // no edge-value copy outlives the tick
   if (abort_ez >= 0) {
     // drain the copies still in flight (issued bands from abort_ez on) before leaving
     if (tid == 0) atomicOr(S.status, SEM_ERR_TIMEOUT);
@@ -1403,6 +1522,16 @@ __device__ __forceinline__ void strip_tick(const SolveDev& S, const int act, con
     return;
   }
   if (__any_sync(0xffffffffu, bad) && lane == 0) atomicOr(S.status, SEM_ERR_NONFINITE);
+  if constexpr (COH) {
+    // the persistent kernel runs the next tick on the same shared memory: every copy has
+    // landed and every thread is past its last ring wait, so the barriers are invalidated
+    // before the next tick initialises them again (re-initialising a valid mbarrier is
+    // undefined)
+    __syncthreads();
+    if (tid == 0)
+      for (int s2 = 0; s2 < NST; ++s2) mbar_inval(bars + s2);
+    __syncthreads();
+  }
 }
 #undef Dr
 #undef Bt
@@ -1441,10 +1570,17 @@ __global__ void __launch_bounds__(kStripCols, (N <= 4) ? SEM_STRIP_MIN_BLOCKS : 
     }
     return;
   }
-  if (act == A_ADJ)
-    strip_tick<N, true, false>(S, act, t, seg, smem, &s_abort);
-  else
-    strip_tick<N, false, false>(S, act, t, seg, smem, &s_abort);
+  if (S.bnd_n > 0) {
+    if (act == A_ADJ)
+      strip_tick<N, true, false, true>(S, act, t, seg, smem, &s_abort);
+    else
+      strip_tick<N, false, false, true>(S, act, t, seg, smem, &s_abort);
+  } else {
+    if (act == A_ADJ)
+      strip_tick<N, true, false, false>(S, act, t, seg, smem, &s_abort);
+    else
+      strip_tick<N, false, false, false>(S, act, t, seg, smem, &s_abort);
+  }
 }
 
 // ----------------------------------------------------------------------------
@@ -1516,9 +1652,10 @@ __global__ void __launch_bounds__(256) sem_persist_kernel(const SolveDev* __rest
 // ----------------------------------------------------------------------------
 // persistent strip kernel: one cooperative launch runs the whole tick program of a group
 // of strip chunks that are all resident at once (a single large solve, or a few), so a
-// tick costs no launch and no grid drain.  A CTA starts tick t when its four neighbours
-// (strips left and right, chunks above and below: the only CTAs whose nodes its bands
-// read and use) have published tick t - 1; the adjoint-scale tick of a solve takes a
+// tick costs no launch and no grid drain.  A CTA starts tick t when the eight CTAs around
+// it (the only CTAs whose nodes its bands read and use: halo columns, the halo band
+// above, the shared row below, and a receiver element's corner node) have published tick
+// t - 1; the adjoint-scale tick of a solve takes a
 // barrier over that solve's CTAs before and after it.  Every wait is bounded (kWaitNs)
 // and ends the launch with SEM_ERR_TIMEOUT.  Bitwise the same arithmetic as the per-tick
 // strip kernel (the same strip_tick, with loads of data this launch wrote taken past L1).
@@ -1531,14 +1668,20 @@ __device__ __forceinline__ unsigned ld_acquire_u32(const unsigned* p) {
 __device__ __forceinline__ void st_release_u32(unsigned* p, unsigned v) {
   asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
-// true once every CTA nb[0..nn) has published at least `want` ticks; false after kWaitNs
+// Thread i < nn waits until CTA nb[i] has published at least `want` ticks (false after
+// kWaitNs); all threads must call it.  Returns true when every wait succeeded.
 __device__ __forceinline__ bool wait_neighbours(const unsigned* done, const int* nb, int nn,
                                                 unsigned want) {
-  const long long t0 = global_ns();
-  for (int i = 0; i < nn; ++i)
-    while (ld_acquire_u32(done + nb[i]) < want)
-      if (global_ns() - t0 > kWaitNs) return false;
-  return true;
+  bool ok = true;
+  if ((int)threadIdx.x < nn) {
+    const unsigned* p = done + nb[threadIdx.x];
+    if (ld_acquire_u32(p) < want) {
+      const long long t0 = global_ns();
+      while (ld_acquire_u32(p) < want)
+        if (global_ns() - t0 > kWaitNs) { ok = false; break; }
+    }
+  }
+  return __syncthreads_and(ok) != 0;
 }
 
 template <int N>
@@ -1549,7 +1692,7 @@ __global__ void __launch_bounds__(kStripCols, (N <= 4) ? SEM_STRIP_MIN_BLOCKS : 
   extern __shared__ __align__(128) float smem[];
   __shared__ SolveDev S;
   __shared__ int s_act, s_t, s_seg, s_abort, s_ok;
-  __shared__ int s_nb[4], s_nn, s_local;           // neighbour CTAs (kept out of registers)
+  __shared__ int s_nb[8], s_nn, s_local;           // neighbour CTAs (kept out of registers)
   __shared__ unsigned long long s_arrivals, s_per_solve;
   const int sid = cta_solve[blockIdx.x];
   {
@@ -1563,11 +1706,15 @@ __global__ void __launch_bounds__(kStripCols, (N <= 4) ? SEM_STRIP_MIN_BLOCKS : 
     const int nzc = (S.nelz + zch - 1) / zch;
     const int local = blockIdx.x - S.tile_base;
     const int strip = local / nzc, chunk = local - strip * nzc;
+    // the eight surrounding CTAs: a receiver element read out of a band can reach the node
+    // at a chunk's corner, which the diagonal neighbour owns
     int nn = 0;
-    if (strip > 0) s_nb[nn++] = blockIdx.x - nzc;
-    if (strip + 1 < S.tiles_x) s_nb[nn++] = blockIdx.x + nzc;
-    if (chunk > 0) s_nb[nn++] = blockIdx.x - 1;
-    if (chunk + 1 < nzc) s_nb[nn++] = blockIdx.x + 1;
+    for (int ds = -1; ds <= 1; ++ds)
+      for (int dc = -1; dc <= 1; ++dc) {
+        const int st = strip + ds, ch = chunk + dc;
+        if ((ds || dc) && st >= 0 && st < S.tiles_x && ch >= 0 && ch < nzc)
+          s_nb[nn++] = (int)blockIdx.x + ds * nzc + dc;
+      }
     s_nn = nn;
     s_local = local;
     s_per_solve = (unsigned long long)S.tiles_x * nzc;
@@ -1595,16 +1742,21 @@ __global__ void __launch_bounds__(kStripCols, (N <= 4) ? SEM_STRIP_MIN_BLOCKS : 
       ok = ok && grid_barrier(sbar + sid, a2, &s_ok);
       if (threadIdx.x == 0) s_arrivals = a2;
     } else if (act != A_NONE) {
-      if (threadIdx.x == 0) s_ok = wait_neighbours(done, s_nb, s_nn, (unsigned)(tick - tick0)) ? 1 : 0;
-      __syncthreads();
-      ok = s_ok != 0;
+      ok = wait_neighbours(done, s_nb, s_nn, (unsigned)(tick - tick0));
       if (ok) {
         // the neighbours' generic-proxy stores come before this tick's bulk / tensor loads
         asm volatile("fence.proxy.async.global;" ::: "memory");
-        if (act == A_ADJ)
-          strip_tick<N, true, true>(S, act, s_t, s_seg, smem, &s_abort);
-        else
-          strip_tick<N, false, true>(S, act, s_t, s_seg, smem, &s_abort);
+        if (S.bnd_n > 0) {
+          if (act == A_ADJ)
+            strip_tick<N, true, true, true>(S, act, s_t, s_seg, smem, &s_abort);
+          else
+            strip_tick<N, false, true, true>(S, act, s_t, s_seg, smem, &s_abort);
+        } else {
+          if (act == A_ADJ)
+            strip_tick<N, true, true, false>(S, act, s_t, s_seg, smem, &s_abort);
+          else
+            strip_tick<N, false, true, false>(S, act, s_t, s_seg, smem, &s_abort);
+        }
         __syncthreads();
         if (s_abort != 0x7fffffff) return;  // a copy wait gave up: status set, copies drained
       }
@@ -2337,7 +2489,7 @@ static int run_group(sem_batch_t* b, const sem_solve_t* solves, int32_t n,
   }
   if (use_strip) b->h_tmaps.resize(n);
   b->h_cta.clear();
-  struct Group { int N; long long cta0, ncta; bool adj; };
+  struct Group { int N; long long cta0, ncta; bool adj, stc; };
   std::vector<Group> groups;
   long long off = 0;
   int max_prog = 0;
@@ -2359,9 +2511,10 @@ static int run_group(sem_batch_t* b, const sem_solve_t* solves, int32_t n,
     }
     if (rc) return rc;
     if (groups.empty() || groups.back().N != p->npol)
-      groups.push_back(Group{p->npol, (long long)b->h_cta.size(), 0, false});
+      groups.push_back(Group{p->npol, (long long)b->h_cta.size(), 0, false, false});
     Group& G = groups.back();
     G.adj |= (s.flags & SEM_F_ADJOINT) != 0;
+    G.stc |= p->bnd_n > 0;
     char* a = b->arena + off;
     base[i] = off;
     SolveDev& d = b->h_solves[oi];
@@ -2491,7 +2644,7 @@ static int run_group(sem_batch_t* b, const sem_solve_t* solves, int32_t n,
   for (auto& G : groups) {
     KernelFn fn = use_strip ? strip_kernel_for(G.N) : kernel_for(G.N);
     if (!fn) return fail(SEM_ERR_UNSUPPORTED, "polynomial order");
-    const size_t smem = (size_t)(use_strip ? strip_smem_floats(G.N, G.adj)
+    const size_t smem = (size_t)(use_strip ? strip_smem_floats(G.N, G.adj) + (G.stc ? kStripBndFloats : 0)
                                            : smem_floats(G.N, cfg.tile_ex, cfg.tile_ez, G.adj)) *
                         sizeof(float);
     if (smem > 227 * 1024) return fail(SEM_ERR_ARG, "tile too large for shared memory");
@@ -2685,12 +2838,13 @@ int auto_schedule(const sem_solve_t* sv, int n, const sem_launch_cfg_t& cfg, lon
     int tx, tz;
     tiles[i] = tiles_of(p, cfg.tile_ex, cfg.tile_ez, &tx, &tz);
   }
-  bool any_adj = false;
+  bool any_adj = false, any_stc = false;
   for (int i = 0; i < n; ++i) any_adj |= (sv[i].flags & SEM_F_ADJOINT) != 0;
+  for (int i = 0; i < n; ++i) any_stc |= sv[i].plan->bnd_n > 0;
   const int N0 = sv[0].plan->npol;
   auto occupancy = [&](bool strip) -> long long {
     KernelFn fn = strip ? strip_kernel_for(N0) : kernel_for(N0);
-    const size_t smem = (size_t)(strip ? strip_smem_floats(N0, any_adj)
+    const size_t smem = (size_t)(strip ? strip_smem_floats(N0, any_adj) + (any_stc ? kStripBndFloats : 0)
                                        : smem_floats(N0, cfg.tile_ex, cfg.tile_ez, any_adj)) * 4;
     int nb = 1;
     if (smem <= 227 * 1024 &&
@@ -3310,7 +3464,7 @@ int sem_engine_step(sem_engine_t* e, void* stream_v) {
     e->tmaps_cap = cap;
   }
   if (use_strip) e->h_tmaps.resize(n);
-  struct Group { int N; long long cta0, ncta; bool adj; int first; };
+  struct Group { int N; long long cta0, ncta; bool adj, stc; int first; };
   std::vector<Group> groups;
   for (int oi = 0; oi < n; ++oi) {
     EngineJob* j = order[oi];
@@ -3327,9 +3481,10 @@ int sem_engine_step(sem_engine_t* e, void* stream_v) {
     }
     if (rc) return rc;
     if (groups.empty() || groups.back().N != p->npol)
-      groups.push_back(Group{p->npol, (long long)e->h_cta.size(), 0, false, oi});
+      groups.push_back(Group{p->npol, (long long)e->h_cta.size(), 0, false, false, oi});
     Group& G = groups.back();
     G.adj |= (j->s.flags & SEM_F_ADJOINT) != 0;
+    G.stc |= p->bnd_n > 0;
     char* a = e->arena + j->off;
     SolveDev& d = e->h_solves[oi];
     d.nelx = p->nelx; d.nelz = p->nelz; d.nxg = p->nxg; d.nzg = p->nzg; d.pitch = p->pitch;
@@ -3402,7 +3557,7 @@ int sem_engine_step(sem_engine_t* e, void* stream_v) {
     for (auto& G : groups) {
       KernelFn fn = use_strip ? strip_kernel_for(G.N) : kernel_for(G.N);
       if (!fn) return fail(SEM_ERR_UNSUPPORTED, "polynomial order");
-      const size_t smem = (size_t)(use_strip ? strip_smem_floats(G.N, G.adj)
+      const size_t smem = (size_t)(use_strip ? strip_smem_floats(G.N, G.adj) + (G.stc ? kStripBndFloats : 0)
                                              : smem_floats(G.N, tex, tez, G.adj)) * sizeof(float);
       if (smem > 227 * 1024) return fail(SEM_ERR_ARG, "tile too large for shared memory");
       if (c == 0)

@@ -111,13 +111,18 @@ def build_plan_arrays(xmin, xmax, zmin, zmax, nelx, nelz, npol, dt, nt, src_xz, 
     wl3z = assemble_1d(nelz, w * lq ** 3)
     xg = grid_coords_1d(xmin, xmax, nelx, N)
     zg = grid_coords_1d(zmin, zmax, nelz, N)
+    # the sponge decay exp(-sigma dt) enters as its defect delta = 1 - exp(-sigma dt),
+    # computed here in float64 (expm1); the kernels apply  s - delta s  with one rounding.
+    # A decay factor just below 1 rounded to float32 is a fixed bias applied at every step,
+    # which dominated the float32 seismogram error (2.3e-6 of 2.6e-6 on the plain
+    # workload's golden, emulated); the small defect keeps its relative accuracy.
     if boundary == "sponge":
-        dec_x = np.exp(-sponge_sigma_1d(xg, xmin, xmax, pml_thickness, sponge_cmax) * dt)
-        dec_z = np.exp(-sponge_sigma_1d(zg, zmin, zmax, pml_thickness, sponge_cmax) * dt)
+        del_x = -np.expm1(-sponge_sigma_1d(xg, xmin, xmax, pml_thickness, sponge_cmax) * dt)
+        del_z = -np.expm1(-sponge_sigma_1d(zg, zmin, zmax, pml_thickness, sponge_cmax) * dt)
     else:
-        dec_x, dec_z = np.ones(nxg), np.ones(nzg)
-    tab_x = np.concatenate([1.0 / mx, J * seta2 * wl3x, dec_x])
-    tab_z = np.concatenate([dt * dt / (J * mz), J * sxi2 * wl3z, dec_z])
+        del_x, del_z = np.zeros(nxg), np.zeros(nzg)
+    tab_x = np.concatenate([1.0 / mx, J * seta2 * wl3x, del_x])
+    tab_z = np.concatenate([dt * dt / (J * mz), J * sxi2 * wl3z, del_z])
     if coords is None or node_grid is None:
         coords, _, node_grid = create_global_mesh(xmin, xmax, zmin, zmax, nelx, nelz, N)
     src_node = find_closest_node(float(src_xz[0]), float(src_xz[1]), coords)

@@ -77,7 +77,7 @@ def sens_apply(a, ug, wg):
 def forward(a, c, shift=False):
     """(b, v) forward recurrence exactly as the kernel runs it (float64)."""
     ix, Rx, dx, iz, Rz, dz = tables(a)
-    d = dz[:, None] * dx[None, :]
+    d = (1.0 - dz)[:, None] * (1.0 - dx)[None, :]   # the tables carry the decay defects
     P = mass_inv_dt2(a)
     nxg, nzg = grids(a)
     v = np.zeros((nzg, nxg))

@@ -37,4 +37,4 @@ def test_boundary_tables_match_oracle(N, nelx, nelz):
     assert np.allclose(c[r] * a["bnd_alpha"][k], a_oracle, rtol=1e-13, atol=0)
     assert np.allclose(a["bnd_gamma"][k], sim.extra["beta"][r] / (4 * dt), rtol=1e-13, atol=0)
     # no sponge in this mode
-    assert np.all(a["tab_x"][2 * nxg:] == 1.0) and np.all(a["tab_z"][2 * nzg:] == 1.0)
+    assert np.all(a["tab_x"][2 * nxg:] == 0.0) and np.all(a["tab_z"][2 * nzg:] == 0.0)
