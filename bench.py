@@ -699,7 +699,8 @@ def main():
     ap.add_argument("--serve-ticks", type=int, default=32)
     ap.add_argument("--clocks-log", default="", help="nvidia-smi clock samples (default: a temp file)")
     ap.add_argument("--boundary", default="sponge", choices=["sponge", "stacey"],
-                    help="plain workload: the reference's sponge, or Stacey sides/bottom with a free surface")
+                    help="the reference's sponge, or Stacey sides/bottom with a free surface (plain and "
+                         "default workloads)")
     ap.add_argument("--no-extras", action="store_true",
                     help="default workload: skip the parity, single, uneven and serving legs")
     args = ap.parse_args()
@@ -726,7 +727,7 @@ def main():
         import datetime
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
 
-    W = workload(nmodels=args.models, nt=args.nt, seed0=1000 * rank)
+    W = workload(nmodels=args.models, nt=args.nt, seed0=1000 * rank, boundary=args.boundary)
     plan = SEMPlan(**W["plan_kw"])
     dev = torch.device("cuda", local)
     tex, tez = parse_tile(args.tile)
