@@ -630,7 +630,8 @@ def stacey_leg(args, steps=2, warmup=1):
     out = {"workload": "batched ELBO sampling, 256 models, Stacey absorbing sides and bottom, free surface "
                        "on top (no sponge)",
            "value": args.models / (np.mean(ms) / 1e3), "unit": "solves/s", "ms_per_step": float(np.mean(ms)),
-           "kernel": batch.last_kernel, "groups": batch.last_groups,
+           "kernel": batch.last_kernel, "groups": batch.last_groups, "ticks": batch.last_ticks,
+           "tick_loop_ms": batch.last_tick_ms(),
            "status": int(torch.cat([s.status for s in specs]).max().item())}
     out["parity"] = parity_leg(W, specs, y, [1])
     return out

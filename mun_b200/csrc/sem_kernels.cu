@@ -769,6 +769,11 @@ __global__ void __launch_bounds__(256) sem_tick_kernel(const SolveDev* __restric
 #ifndef SEM_STAGES_ADJ
 #define SEM_STAGES_ADJ 3
 #endif
+// Stacey edge values a band ahead: 0 = register staging by 50 carrier threads,
+// 1 = cp.async copies
+#ifndef SEM_BND_ASYNC
+#define SEM_BND_ASYNC 0
+#endif
 // adjoint ticks: D (lambda) and D (forward field) of a segment in packed FFMA2
 #ifndef SEM_PAIRED_ADJ
 #define SEM_PAIRED_ADJ 1
@@ -1074,26 +1079,40 @@ __device__ __forceinline__ void strip_tick(const SolveDev& S, const int act, con
   const bool side_r = STC && so1 == nxg;
   const bool bottom = STC && zb1 == nelz && !final_only;
   const bool bgterm = ADJ && t >= S.it0 && t < S.it1 && t <= S.nt - 2;  // impedance term
-  auto bnd_fetch = [&](int ez, int buf) {
-    if (tid < 2 * 5 * NP) {
-      const int sd = tid / (5 * NP), q = (tid / NP) % 5, a = tid % NP;
-      const int gz = ez * N + a;
-      if ((sd == 0 ? side_l : side_r) && (q < 2 || bgterm) && gz > 0 && gz < nzg) {
-        const long long k = (sd == 0 ? 0 : nzg) + gz, BP = S.bnd_pitch;
-        const float* src = q < 3 ? S.bnd_coef + q * BP + k : S.bnd_hist + (q == 3 ? t : t + 2) * BP + k;
-        cp_async4(sbnd + ((buf * 2 + sd) * 5 + q) * 8 + a, src);
-      }
-    }
+  // the value thread tid < 50 carries: side sd, quantity q (e1, e2, g, b_t, b_{t+2}), row a
+  const int bsd = tid / (5 * NP), bq = (tid / NP) % 5, ba = tid % NP;
+  const bool bcarrier = STC && tid < 2 * 5 * NP && (bsd == 0 ? side_l : side_r) && (bq < 2 || bgterm);
+  auto bnd_src = [&](int ez) -> const float* {
+    const int gz = ez * N + ba;
+    if (!bcarrier || gz <= 0 || gz >= nzg) return nullptr;
+    const long long k = (bsd == 0 ? 0 : nzg) + gz, BP = S.bnd_pitch;
+    return bq < 3 ? S.bnd_coef + bq * BP + k : S.bnd_hist + (bq == 3 ? t : t + 2) * BP + k;
   };
+#if SEM_BND_ASYNC
+  auto bnd_fetch = [&](int ez, int buf) {
+    const float* src = bnd_src(ez);
+    if (src) cp_async4(sbnd + ((buf * 2 + bsd) * 5 + bq) * 8 + ba, src);
+  };
+#else
+  float bnd_next = 0.f;  // this carrier's value for the next band, loaded a band ahead
+#endif
   if (STC) {
     if (bottom && gx > 0 && gx < nxg - 1 && owned) {
       const long long k = 2 * nzg + gx, BP = S.bnd_pitch;
       for (int q = 0; q < (bgterm ? 5 : 2); ++q) {
         const float* src = q < 3 ? S.bnd_coef + q * BP + k : S.bnd_hist + (q == 3 ? t : t + 2) * BP + k;
+#if SEM_BND_ASYNC
         cp_async4(bbot + q * NT + tid, src);
+#else
+        bbot[q * NT + tid] = *src;  // once per tick, before the first band
+#endif
       }
     }
+#if SEM_BND_ASYNC
     if (!final_only) bnd_fetch(ezs, 0);
+#else
+    if (!final_only && bnd_src(ezs)) bnd_next = *bnd_src(ezs);
+#endif
   }
 
   // D and beta: per-order constants (c_D[N], c_B[N])
@@ -1180,11 +1199,21 @@ __device__ __forceinline__ void strip_tick(const SolveDev& S, const int act, con
       for (int a = 0; a < N; ++a) gpre[a] = gradp[gb + a * pitch];
     }
     if (STC && !final_only) {
+#if SEM_BND_ASYNC
       // this band's edge values (fetched a band ago) are complete once each issuing thread
       // has waited for its copies; the phase-A barrier publishes them.  The next band's go
       // to the buffer no thread reads now (phase B of band rel - 1 reads (rel - 1) % 3).
       cp_async_wait_all();
       if (rel + 1 < nbands) bnd_fetch(ez + 1, (rel + 1) % 3);
+#else
+      // each carrier parks this band's value (loaded a band ago) for the phase-A barrier to
+      // publish, and loads the next band's; phase B of band rel - 1 reads (rel - 1) % 3
+      if (bcarrier) {
+        sbnd[(((rel % 3) * 2 + bsd) * 5 + bq) * 8 + ba] = bnd_next;
+        const float* nsrc = rel + 1 < nbands ? bnd_src(ez + 1) : nullptr;
+        if (nsrc) bnd_next = *nsrc;
+      }
+#endif
     }
     if (!mbar_wait(bars + slot, (unsigned)((rel / NST) & 1))) atomicMin(s_abort, ez);
     const bool last = (ez == nelz - 1);
@@ -1510,7 +1539,9 @@ __device__ __forceinline__ void strip_tick(const SolveDev& S, const int act, con
       }
     }
   }
+#if SEM_BND_ASYNC
   if (STC) cp_async_wait_all();  // no edge-value copy outlives the tick
+#endif
   if (abort_ez >= 0) {
     // drain the copies still in flight (issued bands from abort_ez on) before leaving
     if (tid == 0) atomicOr(S.status, SEM_ERR_TIMEOUT);
