@@ -51,6 +51,7 @@
 #include <mutex>
 #include <string>
 #include <tuple>
+#include <type_traits>
 #include <vector>
 
 #include "../../include/mun_sem.h"
@@ -814,11 +815,13 @@ __device__ __forceinline__ uint32_t smem_addr(const void* p) {
 __device__ __forceinline__ void mbar_init(unsigned long long* bar, unsigned count) {
   asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
 }
+#if SEM_BND_ASYNC
 // 4-byte asynchronous global -> shared copies (the Stacey edge values, a band ahead)
 __device__ __forceinline__ void cp_async4(void* dst, const void* src) {
   asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(smem_addr(dst)), "l"(src) : "memory");
 }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+#endif
 __device__ __forceinline__ void mbar_inval(unsigned long long* bar) {
   asm volatile("mbarrier.inval.shared::cta.b64 [%0];" ::"r"(smem_addr(bar)) : "memory");
 }
@@ -1077,6 +1080,7 @@ __device__ __forceinline__ void strip_tick(const SolveDev& S, const int act, con
   // the last chunk row nzg - 1) and the asynchronous fetch of their values one band ahead
   const bool side_l = STC && sx0 == 0;
   const bool side_r = STC && so1 == nxg;
+  const bool side_col = STC && owned && (gx == 0 || gx == nxg - 1);  // this thread's column
   const bool bottom = STC && zb1 == nelz && !final_only;
   const bool bgterm = ADJ && t >= S.it0 && t < S.it1 && t <= S.nt - 2;  // impedance term
   // the value thread tid < 50 carries: side sd, quantity q (e1, e2, g, b_t, b_{t+2}), row a
@@ -1145,7 +1149,7 @@ __device__ __forceinline__ void strip_tick(const SolveDev& S, const int act, con
   const bool g_start = grad_on && grad_partial_starts(S, t);
   const bool g_fold = grad_on && grad_folds(S, t);
   double* const grad64p = S.grad64;
-  constexpr bool stc = STC;  // Stacey / free-surface mode (compiled out of the sponge path)
+  // Stacey / free-surface mode (STC) is compiled out of the sponge path
   const bool in_win = ADJ && t >= S.it0 && t < S.it1 && ((t - S.it0) % S.decim) == 0;
   const int ms = t - ((S.flags & F_SHIFT) ? 1 : 0);
   const bool rec_on = !ADJ && (act == A_FWD || act == A_FINAL) && ms >= 0 && ms < S.nt;
@@ -1452,8 +1456,13 @@ __device__ __forceinline__ void strip_tick(const SolveDev& S, const int act, con
       }
       continue;
     }
-    // ---- phase B: combine and advance the owned nodes of the band, row by row
-    if (owned) {
+    // ---- phase B: combine and advance the owned nodes of the band, row by row.  Two
+    // compiled copies: EDGE (Stacey mode, where a band can hold free-surface or
+    // absorbing-edge nodes of this thread: its column is an edge, or the band is the
+    // first or the last) checks every node; the other is the plain update, so interior
+    // columns of middle bands pay nothing for the boundary mode.
+    auto phase_b = [&](auto edge_c) {
+      constexpr bool EDGE = decltype(edge_c)::value;
 #pragma unroll
       for (int a = 0; a < NP; ++a) {
         if (a == N && !last) break;
@@ -1482,7 +1491,11 @@ __device__ __forceinline__ void strip_tick(const SolveDev& S, const int act, con
         const float izv = tzb[a], Rzv = tzb[8 + a], dzv = tzb[16 + a];
         const int g = gb + a * pitch;
         const int gz = ez * N + a;
-        const int bk = (stc && gz > 0) ? bnd_slot(S, gx, gz) : -1;
+        // Stacey mode: the free surface is row 0; the absorbing edges are the side columns
+        // (fixed per thread) and the bottom row (row N of the last band)
+        const bool top_row = EDGE && ez == 0 && a == 0;
+        const bool edge_node = EDGE && !top_row && (side_col || (last && a == N));
+        const int bk = !edge_node ? -1 : (gx == 0 ? gz : gx == nxg - 1 ? nzg + gz : 2 * nzg + gx);
         float extra;
         float gnew = 0.f;
         if (!ADJ) {
@@ -1492,12 +1505,11 @@ __device__ __forceinline__ void strip_tick(const SolveDev& S, const int act, con
           if (grad_on) {
             const float gprev = g_start ? 0.f : (a < N ? gpre[a < N ? a : 0] : gradp[g]);
             float inc = sens_increment(Rzv, SX, Rxv, SZ);
-            if (STC && bk >= 0 && bgterm) {
+            if (edge_node && bgterm) {
               // g lambda (b_{t+2} - b_t), rounded as bnd_sens
-              const float* bv = (gx == 0 || gx == nxg - 1)
-                                    ? sbnd + (((rel % 3) * 2 + (gx == 0 ? 0 : 1)) * 5) * 8 + a
-                                    : bbot + tid;
-              const int qs = (gx == 0 || gx == nxg - 1) ? 8 : NT;
+              const float* bv = side_col ? sbnd + (((rel % 3) * 2 + (gx == 0 ? 0 : 1)) * 5) * 8 + a
+                                         : bbot + tid;
+              const int qs = side_col ? 8 : NT;
               const float du = __fsub_rn(bv[4 * qs], bv[3 * qs]);
               inc = __fadd_rn(inc, __fmul_rn(__fmul_rn(bv[2 * qs], Bs[a * BW + sc]), du));
             }
@@ -1505,13 +1517,12 @@ __device__ __forceinline__ void strip_tick(const SolveDev& S, const int act, con
           }
         }
         float res, vres;
-        if (stc && gz == 0) {  // free surface
+        if (top_row) {  // free surface
           res = 0.f;
           vres = 0.f;
-        } else if (STC && bk >= 0) {
-          const bool sidecol = (gx == 0 || gx == nxg - 1);
-          const float* bv = sidecol ? sbnd + (((rel % 3) * 2 + (gx == 0 ? 0 : 1)) * 5) * 8 + a : bbot + tid;
-          const int qs = sidecol ? 8 : NT;
+        } else if (edge_node) {
+          const float* bv = side_col ? sbnd + (((rel % 3) * 2 + (gx == 0 ? 0 : 1)) * 5) * 8 + a : bbot + tid;
+          const int qs = side_col ? 8 : NT;
           advance_node_stacey(ADJ, Bs[a * BW + sc], Vs[a * BW + sc], X, Z, ixv, Rxv, izv, Rzv, extra,
                               bv[0], bv[qs], res, vres);
           if (!ADJ && (S.flags & F_ADJ)) S.bnd_hist[(long long)(t + 1) * S.bnd_pitch + bk] = res;
@@ -1529,6 +1540,12 @@ __device__ __forceinline__ void strip_tick(const SolveDev& S, const int act, con
         }
         bad |= !isfinite(res);
       }
+    };
+    if (owned) {
+      if (STC && (side_col || last || ez == 0))
+        phase_b(std::true_type{});
+      else
+        phase_b(std::false_type{});
       zc = rz[N];
       if (ADJ) szc = sz[N];
       if (ADJ && in_win) {  // carry the injection row shared with the next band
