@@ -283,10 +283,11 @@ __device__ __forceinline__ int bnd_slot(const SolveDev& s, int gx, int gz) {
   if (gz == s.nzg - 1) return 2 * s.nzg + gx;
   return -1;
 }
-// One node of an absorbing edge: (1 + a) u+ = 2 u - (1 - a) u- + F in the (b, v) state,
-//   w = e1 v + e2 F,  v' = w,  b' = b + w   (e1 = (1 - a) / (1 + a), e2 = 1 / (1 + a)),
-// F = extra - P K (forward) or P (extra - K) (adjoint, the same recurrence run backwards);
-// there is no sponge in this mode.  Shared by both kernels.
+// One node in the Stacey mode: (1 + a) u+ = 2 u - (1 - a) u- + F in the (b, v) state,
+//   w = e1 v + e2 F,  v' = w,  b' = b + w   (e1 = (1 - a) / (1 + a), e2 = 1 / (1 + a) on the
+// absorbing edges, e1 = e2 = 1 elsewhere), F = extra - P K (forward) or P (extra - K)
+// (adjoint, the same recurrence run backwards); there is no sponge in this mode.  Every
+// node of a Stacey solve takes this form in both kernels.
 __device__ __forceinline__ void advance_node_stacey(bool adj, float b, float v, float X, float Z,
                                                     float ixv, float Rxv, float izv, float Rzv,
                                                     float extra, float e1, float e2, float& bout,
@@ -700,14 +701,17 @@ __device__ __forceinline__ void tile_tick(const SolveDev& S, const int act, cons
       }
     }
     float res, vres;
-    if (stc && gz == 0) {  // free surface
-      res = 0.f;
-      vres = 0.f;
-    } else if (bk >= 0) {
+    if (stc) {
+      // Stacey mode: w = e1 v + e2 F at every node, e1 = e2 = 1 off the absorbing edges
+      // (the strip kernel's form, so both give the same bits); u = 0 on the free surface
       const long long BP = S.bnd_pitch;
-      advance_node_stacey(adj, b, v, X, Z, ixv, Rxv, izv, Rzv, extra, S.bnd_coef[bk], S.bnd_coef[BP + bk],
-                          res, vres);
-      if (!adj && (S.flags & F_ADJ)) S.bnd_hist[(long long)(t + 1) * BP + bk] = res;
+      const float e1 = bk >= 0 ? S.bnd_coef[bk] : 1.f, e2 = bk >= 0 ? S.bnd_coef[BP + bk] : 1.f;
+      advance_node_stacey(adj, b, v, X, Z, ixv, Rxv, izv, Rzv, extra, e1, e2, res, vres);
+      if (gz == 0) {
+        res = 0.f;
+        vres = 0.f;
+      }
+      if (bk >= 0 && !adj && (S.flags & F_ADJ)) S.bnd_hist[(long long)(t + 1) * BP + bk] = res;
     } else {
       advance_node(adj, damp, b, v, X, Z, ixv, Rxv, dxv, izv, Rzv, dzv, extra, res, vres);
     }
@@ -1456,11 +1460,8 @@ __device__ __forceinline__ void strip_tick(const SolveDev& S, const int act, con
       }
       continue;
     }
-    // ---- phase B: combine and advance the owned nodes of the band, row by row.  Two
-    // compiled copies: EDGE (Stacey mode, where a band can hold free-surface or
-    // absorbing-edge nodes of this thread: its column is an edge, or the band is the
-    // first or the last) checks every node; the other is the plain update, so interior
-    // columns of middle bands pay nothing for the boundary mode.
+    // ---- phase B: combine and advance the owned nodes of the band, row by row (EDGE:
+    // the Stacey mode's copy, compiled out of the sponge path)
     auto phase_b = [&](auto edge_c) {
       constexpr bool EDGE = decltype(edge_c)::value;
 #pragma unroll
@@ -1517,15 +1518,19 @@ __device__ __forceinline__ void strip_tick(const SolveDev& S, const int act, con
           }
         }
         float res, vres;
-        if (top_row) {  // free surface
-          res = 0.f;
-          vres = 0.f;
-        } else if (edge_node) {
+        if constexpr (EDGE) {
+          // Stacey mode: one update for every node, w = e1 v + e2 F, with e1 = e2 = 1 off
+          // the absorbing edges (selects, so a warp holding an edge column does not diverge)
           const float* bv = side_col ? sbnd + (((rel % 3) * 2 + (gx == 0 ? 0 : 1)) * 5) * 8 + a : bbot + tid;
           const int qs = side_col ? 8 : NT;
-          advance_node_stacey(ADJ, Bs[a * BW + sc], Vs[a * BW + sc], X, Z, ixv, Rxv, izv, Rzv, extra,
-                              bv[0], bv[qs], res, vres);
-          if (!ADJ && (S.flags & F_ADJ)) S.bnd_hist[(long long)(t + 1) * S.bnd_pitch + bk] = res;
+          const float e1 = edge_node ? bv[0] : 1.f, e2 = edge_node ? bv[qs] : 1.f;
+          advance_node_stacey(ADJ, Bs[a * BW + sc], Vs[a * BW + sc], X, Z, ixv, Rxv, izv, Rzv, extra, e1,
+                              e2, res, vres);
+          if (top_row) {  // free surface
+            res = 0.f;
+            vres = 0.f;
+          }
+          if (edge_node && !ADJ && (S.flags & F_ADJ)) S.bnd_hist[(long long)(t + 1) * S.bnd_pitch + bk] = res;
         } else {
           advance_node(ADJ, damp, Bs[a * BW + sc], Vs[a * BW + sc], X, Z, ixv, Rxv, dxv, izv, Rzv,
                        dzv, extra, res, vres);
@@ -1542,10 +1547,7 @@ __device__ __forceinline__ void strip_tick(const SolveDev& S, const int act, con
       }
     };
     if (owned) {
-      if (STC && (side_col || last || ez == 0))
-        phase_b(std::true_type{});
-      else
-        phase_b(std::false_type{});
+      phase_b(std::integral_constant<bool, STC>{});
       zc = rz[N];
       if (ADJ) szc = sz[N];
       if (ADJ && in_win) {  // carry the injection row shared with the next band
