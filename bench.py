@@ -50,7 +50,7 @@ IMPL_BYTES_PER_NODE = {"forward_tick": 20, "adjoint_tick": 32.5}
 # DRAM bytes per node and tick of the strip kernel from one ncu capture (dram__bytes_read +
 # dram__bytes_write of one forward and one adjoint tick of a 128-model group, 10.3 M nodes),
 # scaled to a launch by its nodes
-TRAFFIC_B_PER_NODE = {"fwd": 16.8, "adj": 29.2}
+TRAFFIC_B_PER_NODE = {"fwd": 17.0, "adj": 29.3}
 
 
 WORKLOAD_ELBO = ("batched ELBO sampling (256 models, 100x50 el, N=4, 80601 nodes, 3000 steps, "
