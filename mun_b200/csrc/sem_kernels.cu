@@ -283,11 +283,11 @@ __device__ __forceinline__ int bnd_slot(const SolveDev& s, int gx, int gz) {
   if (gz == s.nzg - 1) return 2 * s.nzg + gx;
   return -1;
 }
-// One node of an absorbing edge: (1 + a) u+ = 2 u - (1 - a) u- + F in the (b, v) state,
-//   w = e1 v + e2 F,  v' = w,  b' = b + w   (e1 = (1 - a) / (1 + a), e2 = 1 / (1 + a)),
-// F = extra - P K (forward) or P (extra - K) (adjoint, the same recurrence run backwards);
-// there is no sponge in this mode (interior nodes take advance_node with zero defects).
-// Shared by both kernels.
+// One node in the Stacey mode: (1 + a) u+ = 2 u - (1 - a) u- + F in the (b, v) state,
+//   w = e1 v + e2 F,  v' = w,  b' = b + w   (e1 = (1 - a) / (1 + a), e2 = 1 / (1 + a) on the
+// absorbing edges, e1 = e2 = 1 elsewhere), F = extra - P K (forward) or P (extra - K)
+// (adjoint, the same recurrence run backwards); there is no sponge in this mode.  Every
+// node of a Stacey solve takes this form in both kernels.
 __device__ __forceinline__ void advance_node_stacey(bool adj, float b, float v, float X, float Z,
                                                     float ixv, float Rxv, float izv, float Rzv,
                                                     float extra, float e1, float e2, float& bout,
@@ -701,17 +701,19 @@ __device__ __forceinline__ void tile_tick(const SolveDev& S, const int act, cons
       }
     }
     float res, vres;
-    if (bk >= 0) {  // Stacey mode, absorbing edge
+    if (stc) {
+      // Stacey mode: w = e1 v + e2 F at every node, e1 = e2 = 1 off the absorbing edges
+      // (the strip kernel's form, so both give the same bits); u = 0 on the free surface
       const long long BP = S.bnd_pitch;
-      advance_node_stacey(adj, b, v, X, Z, ixv, Rxv, izv, Rzv, extra, S.bnd_coef[bk], S.bnd_coef[BP + bk],
-                          res, vres);
-      if (!adj && (S.flags & F_ADJ)) S.bnd_hist[(long long)(t + 1) * BP + bk] = res;
+      const float e1 = bk >= 0 ? S.bnd_coef[bk] : 1.f, e2 = bk >= 0 ? S.bnd_coef[BP + bk] : 1.f;
+      advance_node_stacey(adj, b, v, X, Z, ixv, Rxv, izv, Rzv, extra, e1, e2, res, vres);
+      if (gz == 0) {
+        res = 0.f;
+        vres = 0.f;
+      }
+      if (bk >= 0 && !adj && (S.flags & F_ADJ)) S.bnd_hist[(long long)(t + 1) * BP + bk] = res;
     } else {
       advance_node(adj, damp, b, v, X, Z, ixv, Rxv, dxv, izv, Rzv, dzv, extra, res, vres);
-    }
-    if (stc && gz == 0) {  // free surface
-      res = 0.f;
-      vres = 0.f;
     }
     vout[g] = vres;
     out[g] = res;
@@ -1462,8 +1464,10 @@ __device__ __forceinline__ void strip_tick(const SolveDev& S, const int act, con
     // the Stacey mode's copy, compiled out of the sponge path)
     auto phase_b = [&](auto edge_c) {
       constexpr bool EDGE = decltype(edge_c)::value;
-      // this band's edge values of this thread's side column (Stacey mode)
-      const float* const bv_side = sbnd + (((rel % 3) * 2 + (gx == 0 ? 0 : 1)) * 5) * 8;
+      // this band's edge values of this thread's column (Stacey mode): its side column's
+      // row of the band buffer, or the bottom row's
+      const float* const bv0 = side_col ? sbnd + (((rel % 3) * 2 + (gx == 0 ? 0 : 1)) * 5) * 8 : bbot + tid;
+      const int qs = side_col ? 8 : NT;
 #pragma unroll
       for (int a = 0; a < NP; ++a) {
         if (a == N && !last) break;
@@ -1496,7 +1500,7 @@ __device__ __forceinline__ void strip_tick(const SolveDev& S, const int act, con
         // (fixed per thread) and the bottom row (row N of the last band)
         const bool top_row = EDGE && ez == 0 && a == 0;
         const bool edge_node = EDGE && !top_row && (side_col || (last && a == N));
-        const int bk = gx == 0 ? gz : gx == nxg - 1 ? nzg + gz : 2 * nzg + gx;  // used on edges only
+        const int bk = !edge_node ? -1 : (gx == 0 ? gz : gx == nxg - 1 ? nzg + gz : 2 * nzg + gx);
         float extra;
         float gnew = 0.f;
         if (!ADJ) {
@@ -1506,10 +1510,9 @@ __device__ __forceinline__ void strip_tick(const SolveDev& S, const int act, con
           if (grad_on) {
             const float gprev = g_start ? 0.f : (a < N ? gpre[a < N ? a : 0] : gradp[g]);
             float inc = sens_increment(Rzv, SX, Rxv, SZ);
-            if (EDGE && edge_node && bgterm) {
+            if (edge_node && bgterm) {
               // g lambda (b_{t+2} - b_t), rounded as bnd_sens
-              const float* bv = side_col ? bv_side + a : bbot + tid;
-              const int qs = side_col ? 8 : NT;
+              const float* bv = side_col ? bv0 + a : bv0;
               const float du = __fsub_rn(bv[4 * qs], bv[3 * qs]);
               inc = __fadd_rn(inc, __fmul_rn(__fmul_rn(bv[2 * qs], Bs[a * BW + sc]), du));
             }
@@ -1517,22 +1520,21 @@ __device__ __forceinline__ void strip_tick(const SolveDev& S, const int act, con
           }
         }
         float res, vres;
-        if (EDGE && edge_node) {
-          // Stacey mode, absorbing edge: only the warps holding an edge column diverge, and
-          // only for this update
-          const float* bv = side_col ? bv_side + a : bbot + tid;
-          const int qs = side_col ? 8 : NT;
-          advance_node_stacey(ADJ, Bs[a * BW + sc], Vs[a * BW + sc], X, Z, ixv, Rxv, izv, Rzv, extra,
-                              bv[0], bv[qs], res, vres);
-          if (!ADJ && (S.flags & F_ADJ)) S.bnd_hist[(long long)(t + 1) * S.bnd_pitch + bk] = res;
+        if constexpr (EDGE) {
+          // Stacey mode: one update for every node, w = e1 v + e2 F, with e1 = e2 = 1 off
+          // the absorbing edges (selects, so a warp holding an edge column does not diverge)
+          const float* bv = side_col ? bv0 + a : bv0;
+          const float e1 = edge_node ? bv[0] : 1.f, e2 = edge_node ? bv[qs] : 1.f;
+          advance_node_stacey(ADJ, Bs[a * BW + sc], Vs[a * BW + sc], X, Z, ixv, Rxv, izv, Rzv, extra, e1,
+                              e2, res, vres);
+          if (top_row) {  // free surface
+            res = 0.f;
+            vres = 0.f;
+          }
+          if (edge_node && !ADJ && (S.flags & F_ADJ)) S.bnd_hist[(long long)(t + 1) * S.bnd_pitch + bk] = res;
         } else {
-          // interior (in the Stacey mode the tables' defects are 0: the undamped update)
           advance_node(ADJ, damp, Bs[a * BW + sc], Vs[a * BW + sc], X, Z, ixv, Rxv, dxv, izv, Rzv,
                        dzv, extra, res, vres);
-        }
-        if (EDGE && top_row) {  // free surface
-          res = 0.f;
-          vres = 0.f;
         }
         out[g] = res;
         vout[g] = vres;
