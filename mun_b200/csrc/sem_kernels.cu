@@ -59,6 +59,10 @@
 namespace {
 
 constexpr int kMaxN = 7;       // supported polynomial orders 1..7
+// tile kernel: the tick body compiled separately for adjoint and forward-like ticks
+#ifndef SEM_TILE_SPLIT
+#define SEM_TILE_SPLIT 1
+#endif
 constexpr int kMaxInj = 1024;  // receivers whose element touches one tile (checked on the host)
 constexpr int kInjCache = 8;   // adjoint-source receivers of a tile staged before the tile
 
@@ -324,12 +328,14 @@ __device__ __forceinline__ double ld_xd(const double* p) {
 
 // One tick of one element tile (act != A_NONE), shared by the per-tick tile kernel and
 // the persistent kernel (COH: cross-CTA data read coherently).
-template <int N, bool COH>
+// SPLIT: compiled for one tick kind, ADJ (adjoint ticks) or not (forward, read-out, scale);
+// without SPLIT one body decides at run time (same arithmetic either way)
+template <int N, bool COH, bool SPLIT = false, bool ADJ = false>
 __device__ __forceinline__ void tile_tick(const SolveDev& S, const int act, const int t,
                                           const int seg, const int tex, const int tez,
                                           float* smem) {
   constexpr int NP = N + 1;
-  const bool adj = (act == A_ADJ);
+  const bool adj = SPLIT ? ADJ : (act == A_ADJ);
   if (act == A_SCALE) {
     // one CTA per solve picks the power of two that brings max|r| to ~1, so the
     // float32 adjoint field and the sensitivity products stay far from underflow
@@ -749,7 +755,14 @@ __global__ void __launch_bounds__(256) sem_tick_kernel(const SolveDev* __restric
   grid_dep_wait();  // the previous tick's fields are complete from here on
   const int act = s_act;
   if (act == A_NONE) return;
+#if SEM_TILE_SPLIT
+  if (act == A_ADJ)
+    tile_tick<N, false, true, true>(S, act, s_t, s_seg, tex, tez, smem);
+  else
+    tile_tick<N, false, true, false>(S, act, s_t, s_seg, tex, tez, smem);
+#else
   tile_tick<N, false>(S, act, s_t, s_seg, tex, tez, smem);
+#endif
 }
 
 // ----------------------------------------------------------------------------
@@ -1690,7 +1703,14 @@ __global__ void __launch_bounds__(256) sem_persist_kernel(const SolveDev* __rest
     }
     __syncthreads();
     const int act = s_act;
+#if SEM_TILE_SPLIT
+    if (act == A_ADJ)
+      tile_tick<N, true, true, true>(S, act, s_t, s_seg, tex, tez, smem);
+    else if (act != A_NONE)
+      tile_tick<N, true, true, false>(S, act, s_t, s_seg, tex, tez, smem);
+#else
     if (act != A_NONE) tile_tick<N, true>(S, act, s_t, s_seg, tex, tez, smem);
+#endif
     if (tick + 1 == tick1) break;
     target += gridDim.x;
     if (!grid_barrier(bar, target, &s_ok)) {
