@@ -61,7 +61,7 @@ namespace {
 constexpr int kMaxN = 7;       // supported polynomial orders 1..7
 // tile kernel: the tick body compiled separately for adjoint and forward-like ticks
 #ifndef SEM_TILE_SPLIT
-#define SEM_TILE_SPLIT 1
+#define SEM_TILE_SPLIT 0
 #endif
 constexpr int kMaxInj = 1024;  // receivers whose element touches one tile (checked on the host)
 constexpr int kInjCache = 8;   // adjoint-source receivers of a tile staged before the tile
