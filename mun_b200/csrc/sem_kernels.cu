@@ -2892,7 +2892,7 @@ double tick_rounds(long long ctas, long long slots, int sms) {
 
 struct GroupPlan { int begin, end, k; };
 
-// Automatic schedule for solves with ckpt_k = 0: split the batch (sorted by length)
+// Automatic schedule for solves with ckpt_k = 0: split the batch (in the caller's order)
 // into g consecutive groups of equal size run one after another, each with the largest
 // checkpoint interval whose workspace fits the memory budget (k = nt: no replay), and
 // pick the g with the smallest modelled time.  Explicit ckpt_k values are kept.
@@ -3050,18 +3050,10 @@ int sem_run(sem_batch_t* b, const sem_solve_t* solves, int32_t n, const sem_laun
     budget = (long long)(0.85 * (double)((long long)fr + b->arena_bytes)) - (512LL << 20);
     budget = std::max(budget, 1LL << 20);
   }
-  // Groups run one after another and a group lasts as long as its longest solve, so the
-  // solves are grouped by length: sorted by step count, then by mesh size (stable).  Each
-  // solve writes its own outputs and its numbers do not depend on its batch, so the order
-  // changes nothing but the time.
-  std::vector<sem_solve_t> sv(solves, solves + n);
-  std::stable_sort(sv.begin(), sv.end(), [](const sem_solve_t& x, const sem_solve_t& y) {
-    if (x.plan->nt != y.plan->nt) return x.plan->nt > y.plan->nt;
-    return x.plan->npoints > y.plan->npoints;
-  });
   std::vector<GroupPlan> groups;
-  int rc = auto_schedule(sv.data(), n, cfg, budget, &groups);
+  int rc = auto_schedule(solves, n, cfg, budget, &groups);
   if (rc) return rc;
+  std::vector<sem_solve_t> sv(solves, solves + n);
   for (const GroupPlan& g : groups) {
     for (int i = g.begin; i < g.end; ++i)
       if ((sv[i].flags & SEM_F_ADJOINT) && sv[i].ckpt_k <= 0) sv[i].ckpt_k = g.k;
