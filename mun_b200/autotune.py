@@ -17,7 +17,9 @@ import torch
 from .plan import SEMPlan
 from .solver import Batch, SolveSpec
 
-TILE_CANDIDATES = [(0, 0), (8, 8), (16, 8), (8, 4), (16, 4), (4, 4), (2, 2)]  # (0, 0): automatic
+# (0, 0): automatic.  4x3 and 3x3 tiles own at most 256 nodes at order 4 (one per thread of
+# the 256-thread CTA), so a tick's node update is one pass
+TILE_CANDIDATES = [(0, 0), (8, 8), (16, 8), (8, 4), (16, 4), (4, 4), (4, 3), (3, 3), (2, 2)]
 GRAPH_CANDIDATES = [0, 32]
 STRIP_BAND_CANDIDATES = [0, 4, 8]  # strip kernel: element rows per CTA (0: automatic)
 PERSIST_STRIP_BAND_CANDIDATES = [0, 2, 4]  # persistent strip kernel (one launch for all ticks)
