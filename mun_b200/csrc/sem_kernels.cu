@@ -59,10 +59,6 @@
 namespace {
 
 constexpr int kMaxN = 7;       // supported polynomial orders 1..7
-// tile kernel: passes of the haloed staging loop unrolled (loads issued before the stores)
-#ifndef SEM_TILE_STAGE_UNROLL
-#define SEM_TILE_STAGE_UNROLL 2
-#endif
 // tile kernel: the tick body compiled separately for adjoint and forward-like ticks
 #ifndef SEM_TILE_SPLIT
 #define SEM_TILE_SPLIT 0
@@ -477,7 +473,7 @@ __device__ __forceinline__ void tile_tick(const SolveDev& S, const int act, cons
     const int c0 = max(gxs, 0), c1 = min(gxs + (ex1 - ex0 + 2) * N + 1, S.nxg);
     const bool need_c = (act != A_FINAL);
     const int ncol = c1 - c0, tot = ncol * (r1 - r0);
-#pragma unroll SEM_TILE_STAGE_UNROLL
+#pragma unroll 2
     for (int i = threadIdx.x; i < tot; i += nthr) {
       const int rr = i / ncol, r = r0 + rr, c = c0 + (i - rr * ncol);
       const long long gi = (long long)r * S.pitch + c;
