@@ -74,12 +74,32 @@ def sens_apply(a, ug, wg):
     return Rz[:, None] * _sens(ug, wg, N, D, beta, 1) + Rx[None, :] * _sens(ug, wg, N, D, beta, 0)
 
 
+def stacey_weights(a, c):
+    """Per-node (e1, e2) of the Stacey mode's update w = e1 v + e2 F on the grid: a = c alpha
+    on the absorbing edges' slots, e1 = (1 - a) / (1 + a), e2 = 1 / (1 + a); 1 elsewhere."""
+    nxg, nzg = grids(a)
+    e1, e2 = np.ones((nzg, nxg)), np.ones((nzg, nxg))
+    from mun_b200.plan import boundary_slots
+    _, gx, gz, _ = boundary_slots(a["nelx"], a["nelz"], a["npol"])
+    ref = a["bnd_ref"]
+    k = np.nonzero(ref >= 0)[0]
+    av = np.asarray(c, dtype=np.float64)[ref[k]] * a["bnd_alpha"][k]
+    e1[gz[k], gx[k]] = (1.0 - av) / (1.0 + av)
+    e2[gz[k], gx[k]] = 1.0 / (1.0 + av)
+    return e1, e2
+
+
 def forward(a, c, shift=False):
-    """(b, v) forward recurrence exactly as the kernel runs it (float64)."""
+    """(b, v) forward recurrence exactly as the kernel runs it (float64).  Sponge mode:
+    v, b <- d w, d (b + w) with w = v + F; Stacey mode: w = e1 v + e2 F, v, b <- w, b + w,
+    and both zero on the free surface (top grid row)."""
     ix, Rx, dx, iz, Rz, dz = tables(a)
     d = (1.0 - dz)[:, None] * (1.0 - dx)[None, :]   # the tables carry the decay defects
     P = mass_inv_dt2(a)
     nxg, nzg = grids(a)
+    stacey = a.get("boundary") == "stacey"
+    if stacey:
+        e1, e2 = stacey_weights(a, c)
     v = np.zeros((nzg, nxg))
     cur = np.zeros((nzg, nxg))
     N = a["npol"]
@@ -98,9 +118,15 @@ def forward(a, c, shift=False):
     for t in range(a["nt"]):
         if not shift:
             rec[t] = read(cur)
-        w = v - P * K_apply(a, c, cur)
-        w[a["src_gz"], a["src_gx"]] += a["src_term"][t]
-        v, cur = d * w, d * (cur + w)
+        F = -P * K_apply(a, c, cur)
+        F[a["src_gz"], a["src_gx"]] += a["src_term"][t]
+        if stacey:
+            w = e1 * v + e2 * F
+            v, cur = w, cur + w
+            v[0], cur[0] = 0.0, 0.0
+        else:
+            w = v + F
+            v, cur = d * w, d * (cur + w)
         hist.append(cur)
         if shift:
             rec[t] = read(cur)

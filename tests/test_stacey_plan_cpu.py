@@ -38,3 +38,32 @@ def test_boundary_tables_match_oracle(N, nelx, nelz):
     assert np.allclose(a["bnd_gamma"][k], sim.extra["beta"][r] / (4 * dt), rtol=1e-13, atol=0)
     # no sponge in this mode
     assert np.all(a["tab_x"][2 * nxg:] == 0.0) and np.all(a["tab_z"][2 * nzg:] == 0.0)
+
+
+def test_kernel_recurrence_in_stacey_mode_matches_oracle():
+    """The kernels' one-field Stacey update w = e1 v + e2 F (e1, e2 from the plan's slot
+    tables, free surface zeroed), run in float64 from the plan tables alone, against the
+    oracle's three-level recurrence (1 + a) u+ = 2u - (1 - a) u- + dt^2 M^-1 (f - K u)."""
+    from tests import kernel_model as km
+    N, nelx, nelz, nt = 4, 10, 6, 400
+    xmax, zmax = 500.0, 300.0
+    rec = np.stack([np.linspace(30.0, 470.0, 9), np.full(9, 15.0)], 1)
+    cfg = {"domain": {"xmin": 0.0, "xmax": xmax, "zmin": 0.0, "zmax": zmax, "nelem_x": nelx, "nelem_z": nelz},
+           "time": {"total_time": 1.0, "dt": 1.0},
+           "source": {"position": (250.0, 30.0), "frequency": 25.0, "amplitude": 1.0},
+           "receivers": {"positions": rec},
+           "method": {"polynomial_order": N, "pml_thickness": 100.0, "boundary": "stacey"},
+           "velocity": {"outside_velocity": 2600.0}}
+    sim0 = so.build_sim(cfg)
+    x, z = sim0.coords[:, 0], sim0.coords[:, 1]
+    c = 2000.0 + 300.0 * np.sin(x / 90.0) * np.cos(z / 70.0)
+    sim = so.build_sim(cfg, c, dt_cfl_velocity=np.full(len(c), 2600.0))
+    sim.nt = nt
+    sim.src = so.ricker_source(nt, sim.dt, 25.0, 1.0)
+    ref, _ = so.forward(sim, c, convention="fwdadj")
+    a = build_plan_arrays(0.0, xmax, 0.0, zmax, nelx, nelz, N, sim.dt, nt, (250.0, 30.0), 25.0, 1.0, rec,
+                          100.0, 2600.0, boundary="stacey")
+    mine, _ = km.forward(a, c, shift=True)
+    err = float(np.linalg.norm(mine - ref) / np.linalg.norm(ref))
+    assert np.abs(ref[-100:]).max() > 1e-3 * np.abs(ref).max()   # the edges are reached in the window
+    assert err < 1e-11, err
