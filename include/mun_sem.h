@@ -109,8 +109,8 @@ typedef struct {
 /* Launch configuration (the autotuner's knobs). */
 typedef struct {
   int32_t tile_ex, tile_ez;   /* tile kernel: elements per CTA tile in x and z; 0 x 0 =
-                                 automatic (largest of 8x8 .. 2x1 whose tiles over the
-                                 batch give every SM two CTAs, else 2x1)            */
+                                 automatic (of 8x8 .. 2x1 the finest whose CTAs over
+                                 the batch are all resident at once, else 8x8)      */
   int32_t threads;            /* tile kernel: threads per CTA (multiple of 32, <= 256) */
   int32_t graph_chunk;        /* ticks per captured CUDA graph; 0 = plain launches    */
   int32_t kernel;             /* 0 auto, 1 tile kernel (one CTA per element tile),
