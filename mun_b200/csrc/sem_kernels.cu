@@ -247,6 +247,29 @@ __device__ __forceinline__ float sens_product(float beta, float dw, float du) {
 // Squared residual accumulated into a receiver's misfit (multiply, then add).
 __device__ __forceinline__ void misfit_add(double* m, double res) { *m = __dadd_rn(*m, __dmul_rn(res, res)); }
 
+// One receiver's read-out sum_e w_e u_e computed by one thread with the roundings of the
+// one-warp form the tile kernel uses: lane l sums terms l, l + 32, ... by FMA from zero,
+// then the lanes are combined by the xor-shuffle tree (offsets 16, 8, 4, 2, 1), whose
+// value on lane 0 is the pairwise tree below.  u_e is b[(e / NP) * bw + e % NP].
+template <int N>
+__device__ __forceinline__ float rec_dot_tree(const float* __restrict__ wr, const float* b, int bw) {
+  constexpr int NP = N + 1, NE = NP * NP;
+  float v[32];
+#pragma unroll
+  for (int l = 0; l < 32; ++l) {
+    float a = 0.f;
+#pragma unroll
+    for (int e = l; e < NE; e += 32) a = fmaf(__ldg(wr + e), b[(e / NP) * bw + (e % NP)], a);
+    v[l] = a;
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+#pragma unroll
+    for (int l = 0; l < o; ++l) v[l] = __fadd_rn(v[l], v[l + o]);
+  }
+  return v[0];
+}
+
 // One owned node: combine the line operators, advance (b, v) or (lambda, mu), apply
 // the sponge.  Shared by both kernel variants so their arithmetic is identical.
 //   forward:  w = v - P K + src          adjoint: w = mu + P (inj - K)
@@ -963,6 +986,85 @@ __device__ __forceinline__ void load_seg_all(const float* p, bool valid, bool fr
   }
 }
 
+// Receivers read out of one band of a strip, one thread each (the sum as rec_dot_tree,
+// bitwise the tile kernel's one-warp form), with their misfit terms.  Out of line: the
+// band loop's register allocation does not carry this block, which runs in few bands.
+template <int N>
+__device__ __noinline__ void strip_read_out(const SolveDev& S, const float* Bs, int X0, int r0, int cnt,
+                                            int ms) {
+  constexpr int NP = N + 1;
+  constexpr int BW = (kStripCols + 3 + 3) & ~3;
+  const bool mis = (S.flags & F_MISFIT) && ms >= S.it0 && ms < S.it1 && ((ms - S.it0) % S.decim) == 0;
+  for (int q = threadIdx.x; q < cnt; q += kStripCols) {
+    const int r = S.rec_tile_ids[r0 + q];
+    // the misfit terms are fetched before the sum so that their loads overlap it
+    double y = 0.0, m0 = 0.0, rm0 = 0.0;
+    if (mis) {
+      y = S.yobs[(long long)((ms - S.it0) / S.decim) * S.nrec + r];
+      m0 = S.misfit[r];
+      rm0 = S.rmax[r];
+    }
+    const float acc = rec_dot_tree<N>(S.rec_w + (long long)r * NP * NP, Bs + (S.rec_base[2 * r] - X0), BW);
+    S.rec_out[(long long)ms * S.nrec + r] = acc;
+    if (mis) {
+      const double res = (double)acc - y;
+      S.misfit[r] = __dadd_rn(m0, __dmul_rn(res, res));
+      S.rmax[r] = fmax(rm0, fabs(res));
+    }
+  }
+}
+
+// Adjoint source of the receivers of one band of a strip (adjoint ticks in the misfit
+// window): residuals one thread each, then the weights and element bases of up to kw
+// receivers at a time in scr (an exchange buffer that phase A of the band does not write;
+// phase B of the previous band, its last reader, is behind the first barrier below), and
+// each owned column adds the terms of the receivers whose element holds it, in receiver
+// order: per node the same FMAs in the same order as one warp walking the receivers.
+// Every thread of the CTA calls it (it holds barriers).  Out of line as strip_read_out.
+template <int N, bool COH>
+__device__ __noinline__ void strip_inject(const SolveDev& S, int t, int j0, int cnt, float* sacc, float* sres,
+                                          float* scr, int kw_max, bool owned, int gx) {
+  constexpr int NP = N + 1, NE = NP * NP, NT = kStripCols;
+  const int tid = threadIdx.x;
+  // (COH: written by other CTAs of this launch, read past L1)
+  const double ascale = COH ? __ldcg(S.adj_scale) : *S.adj_scale;
+  const long long yrow = (long long)((t - S.it0) / S.decim) * S.nrec;
+  for (int q = tid; q < cnt; q += NT) {
+    const int r = S.inj_tile_ids[j0 + q];
+    const float* rp = S.rec_out + (long long)t * S.nrec + r;
+    const double res = (double)(COH ? __ldcg(rp) : *rp) - S.yobs[yrow + r];
+    sres[q] = (float)(res * ascale);
+  }
+  int* const sbx = reinterpret_cast<int*>(scr + kw_max * NE);
+  float iacc[NP];
+#pragma unroll
+  for (int j = 0; j < NP; ++j) iacc[j] = owned ? sacc[j * NT + tid] : 0.f;
+  for (int c0 = 0; c0 < cnt; c0 += kw_max) {
+    const int kw = min(kw_max, cnt - c0);
+    __syncthreads();
+    for (int k = tid; k < kw * NE; k += NT) {
+      const int q = k / NE;
+      scr[k] = S.rec_w[(long long)S.inj_tile_ids[j0 + c0 + q] * NE + (k - q * NE)];
+    }
+    for (int q = tid; q < kw; q += NT) sbx[q] = S.rec_base[2 * S.inj_tile_ids[j0 + c0 + q]];
+    __syncthreads();
+    if (owned) {
+      for (int q = 0; q < kw; ++q) {
+        const int i = gx - sbx[q];
+        if (i >= 0 && i <= N) {
+          const float rs = sres[c0 + q];
+#pragma unroll
+          for (int j = 0; j < NP; ++j) iacc[j] = __fmaf_rn(scr[q * NE + j * NP + i], rs, iacc[j]);
+        }
+      }
+    }
+  }
+  if (owned) {
+#pragma unroll
+    for (int j = 0; j < NP; ++j) sacc[j * NT + tid] = iacc[j];
+  }
+}
+
 // One tick of one strip chunk (element rows [zb0, zb1) of one strip), instantiated for
 // forward-like ticks (FWD, FINAL, REPLAY) and for adjoint ticks so that neither carries
 // the other's branches.  A chunk below the first starts with a halo band (element row
@@ -1239,63 +1341,16 @@ __device__ __forceinline__ void strip_tick(const SolveDev& S, const int act, con
     if (!mbar_wait(bars + slot, (unsigned)((rel / NST) & 1))) atomicMin(s_abort, ez);
     const bool last = (ez == nelz - 1);
 
-    if (rec_on && !halo) {  // receivers read out of this band, one warp each
-      const int cnt = r1 - r0;
-      for (int q = warp; q < cnt; q += NW) {
-        const int r = S.rec_tile_ids[r0 + q];
-        const int bx = S.rec_base[2 * r];
-        const float* wr = S.rec_w + (long long)r * NP * NP;
-        float acc = 0.f;
-        for (int e = lane; e < NP * NP; e += 32) {
-          const int j = e / NP, i = e - j * NP;
-          acc = fmaf(wr[e], Bs[j * BW + (bx + i - X0)], acc);
-        }
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
-        if (lane == 0) {
-          S.rec_out[(long long)ms * S.nrec + r] = acc;
-          if ((S.flags & F_MISFIT) && ms >= S.it0 && ms < S.it1 && ((ms - S.it0) % S.decim) == 0) {
-            const double res = (double)acc - S.yobs[(long long)((ms - S.it0) / S.decim) * S.nrec + r];
-            misfit_add(S.misfit + r, res);
-            S.rmax[r] = fmax(S.rmax[r], fabs(res));
-          }
-        }
-      }
-    }
+    if (rec_on && !halo && r1 > r0) strip_read_out<N>(S, Bs, X0, r0, r1 - r0, ms);
     if (final_only) {
       __syncthreads();  // done with this slot
       if (*s_abort <= ez) { abort_ez = ez; break; }
       if (rel + NST < nbands) issue(ez + NST);
       continue;
     }
-    if (ADJ && in_win && j1 > j0) {  // adjoint source of receivers in this element row
-      const int cnt = j1 - j0;
-      // (COH: written by other CTAs of this launch, read past L1)
-      const double ascale = COH ? __ldcg(S.adj_scale) : *S.adj_scale;
-      const long long yrow = (long long)((t - S.it0) / S.decim) * S.nrec;
-      for (int q = tid; q < cnt; q += NT) {
-        const int r = S.inj_tile_ids[j0 + q];
-        const float* rp = S.rec_out + (long long)t * S.nrec + r;
-        const double res = (double)(COH ? __ldcg(rp) : *rp) - S.yobs[yrow + r];
-        sres[q] = (float)(res * ascale);
-      }
-      __syncthreads();
-      if (warp == 0) {
-        for (int q = 0; q < cnt; ++q) {
-          const int r = S.inj_tile_ids[j0 + q];
-          const float rs = sres[q];
-          const int bx = S.rec_base[2 * r];
-          const float* wr = S.rec_w + (long long)r * NP * NP;
-          for (int e = lane; e < NP * NP; e += 32) {
-            const int j = e / NP, i = e - j * NP;
-            const int gxx = bx + i;
-            if (gxx >= sx0 && gxx < so1)
-              sacc[j * NT + (gxx - sx0)] = __fmaf_rn(wr[e], rs, sacc[j * NT + (gxx - sx0)]);
-          }
-          __syncwarp();
-        }
-      }
-    }
+    if (ADJ && in_win && j1 > j0)  // adjoint source of receivers in this element row
+      strip_inject<N, COH>(S, t, j0, j1 - j0, sacc, sres, xs0 + ((ez + 1) & 1) * XSZ,
+                           XSZ / (NP * NP + 1), owned, gx);
     // ---- phase A, x-lines: one thread per (band row, element segment)
     auto xline = [&](int a, int sgi, unsigned m, bool nxt) {
       const int o = a * BW + off + sgi * N;  // column (e0 - 1 + sgi) * N of row a
