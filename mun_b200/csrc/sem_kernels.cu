@@ -1536,6 +1536,13 @@ __device__ __forceinline__ void strip_tick(const SolveDev& S, const int act, con
       // row of the band buffer, or the bottom row's
       const float* const bv0 = side_col ? sbnd + (((rel % 3) * 2 + (gx == 0 ? 0 : 1)) * 5) * 8 : bbot + tid;
       const int qs = side_col ? 8 : NT;
+      // fold ticks: the band's float64 gradient rows, loaded before the first store of the
+      // band (issued after those stores they would wait one after another)
+      double g64[NP];
+      if (ADJ && g_fold) {
+#pragma unroll
+        for (int a = 0; a < NP; ++a) g64[a] = (a < N || last) ? grad64p[gb + a * pitch] : 0.0;
+      }
 #pragma unroll
       for (int a = 0; a < NP; ++a) {
         if (a == N && !last) break;
@@ -1608,7 +1615,7 @@ __device__ __forceinline__ void strip_tick(const SolveDev& S, const int act, con
         vout[g] = vres;
         if (ADJ && grad_on) {
           if (g_fold)
-            grad64p[g] = __dadd_rn(grad64p[g], (double)gnew);
+            grad64p[g] = __dadd_rn(g64[a], (double)gnew);
           else
             gradp[g] = gnew;
         }
