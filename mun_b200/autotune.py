@@ -21,7 +21,7 @@ from .solver import Batch, SolveSpec
 # the 256-thread CTA), so a tick's node update is one pass
 TILE_CANDIDATES = [(0, 0), (8, 8), (16, 8), (8, 4), (16, 4), (4, 4), (4, 3), (3, 3), (2, 2)]
 GRAPH_CANDIDATES = [0, 32]
-STRIP_BAND_CANDIDATES = [0, 4, 8]  # strip kernel: element rows per CTA (0: automatic)
+STRIP_BAND_CANDIDATES = [0, 4, 5, 6, 8, 10]  # strip kernel: element rows per CTA (0: automatic)
 PERSIST_STRIP_BAND_CANDIDATES = [0, 2, 4]  # persistent strip kernel (one launch for all ticks)
 
 _cache = {}
@@ -33,10 +33,24 @@ def signature(specs):
 
 
 def _proxy_plan(plan, nt_proxy):
-    a = plan.arrays
     kw = dict(plan.kwargs)
     kw["nt"] = min(int(nt_proxy), plan.nt)
     return SEMPlan(**kw)
+
+
+def group_count(specs):
+    """Consecutive groups the library's automatic schedule is expected to run ``specs``
+    in: the solves' full forward histories (float32 fields of pitch x rows, no replay)
+    against the budget the schedule uses, 85 % of free device memory less 512 MiB."""
+    free, _ = torch.cuda.mem_get_info()
+    budget = 0.85 * free - (512 << 20)
+    total = 0
+    for s in specs:
+        p = s.plan
+        nxg, nzg = p.nelx * p.npol + 1, p.nelz * p.npol + 1
+        pitch = (nxg + 31) // 32 * 32
+        total += ((p.nt + 8) if s.adjoint else 8) * pitch * nzg * 4
+    return max(1, min(len(specs), -(-int(total) // max(int(budget), 1))))
 
 
 def tune(specs, nt_proxy=48, repeats=2, candidates=None, verbose=False):
@@ -47,10 +61,16 @@ def tune(specs, nt_proxy=48, repeats=2, candidates=None, verbose=False):
     key = signature(specs)
     if key in _cache:
         return _cache[key]
+    # the proxy keeps the batch's shape over time: each solve's step count in proportion to
+    # its own (the shortest at least 8 steps; a group lasts as long as its longest solve),
+    # and the solves in the consecutive groups the real run's memory budget will split it into
+    nt_max = max(s.plan.nt for s in specs)
     proxies = {}
     for s in specs:
         if id(s.plan) not in proxies:
-            proxies[id(s.plan)] = _proxy_plan(s.plan, nt_proxy)
+            proxies[id(s.plan)] = _proxy_plan(s.plan, max(8, -(-nt_proxy * s.plan.nt // nt_max)))
+    ngroups = group_count(specs)
+    gsize = -(-len(specs) // ngroups)
 
     def proxy_specs():
         out = []
@@ -73,16 +93,19 @@ def tune(specs, nt_proxy=48, repeats=2, candidates=None, verbose=False):
         kernel, tile, chunk, bands = tuple(cand) + (0,) * (4 - len(cand))
         b = Batch(tile=tile if kernel in (1, 3) else (8, 8), graph_chunk=chunk, kernel=kernel,
                   strip_bands=bands)
-        try:
+        def run_groups(sp):
             with torch.cuda.stream(stream):
-                b.run(proxy_specs())  # warm-up (plan lists, graph instantiation)
+                for g0 in range(0, len(sp), gsize):
+                    b.run(sp[g0:g0 + gsize])
+
+        try:
+            run_groups(proxy_specs())  # warm-up (plan lists, graph instantiation)
             stream.synchronize()
             times = []
             for _ in range(repeats):
                 sp = proxy_specs()
                 t0 = time.perf_counter()
-                with torch.cuda.stream(stream):
-                    b.run(sp)
+                run_groups(sp)
                 stream.synchronize()
                 times.append(time.perf_counter() - t0)
             el = min(times)
@@ -95,7 +118,7 @@ def tune(specs, nt_proxy=48, repeats=2, candidates=None, verbose=False):
     kernel, tile, chunk, bands = best
     # ckpt_k 0: the library picks the checkpoint interval and group split at run time
     res = {"kernel": kernel, "tile": tile, "graph_chunk": chunk, "strip_bands": bands, "ckpt_k": 0,
-           "proxy_ms": 1e3 * best_t}
+           "proxy_ms": 1e3 * best_t, "proxy_groups": ngroups}
     _cache[key] = res
     return res
 
