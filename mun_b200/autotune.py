@@ -40,16 +40,12 @@ def _proxy_plan(plan, nt_proxy):
 
 def group_count(specs):
     """Consecutive groups the library's automatic schedule is expected to run ``specs``
-    in: the solves' full forward histories (float32 fields of pitch x rows, no replay)
-    against the budget the schedule uses, 85 % of free device memory less 512 MiB."""
+    in: the solves' workspaces with full forward histories (k = nt, no replay; the
+    library's own layout, ``SEMPlan.workspace_bytes``) against the budget the schedule
+    uses, 85 % of free device memory less 512 MiB."""
     free, _ = torch.cuda.mem_get_info()
     budget = 0.85 * free - (512 << 20)
-    total = 0
-    for s in specs:
-        p = s.plan
-        nxg, nzg = p.nelx * p.npol + 1, p.nelz * p.npol + 1
-        pitch = (nxg + 31) // 32 * 32
-        total += ((p.nt + 8) if s.adjoint else 8) * pitch * nzg * 4
+    total = sum(s.plan.workspace_bytes(s.flags, s.plan.nt if s.adjoint else 2) for s in specs)
     return max(1, min(len(specs), -(-int(total) // max(int(budget), 1))))
 
 

@@ -1,6 +1,7 @@
 """Host logic of the autotuner's proxy (no GPU): the number of consecutive groups a batch's
-full forward histories need under the library's memory budget (85 % of free device
-memory less 512 MiB), with the free-memory query faked."""
+workspaces with full forward histories need under the library's memory budget (85 % of
+free device memory less 512 MiB), with the free-memory query and the plans' workspace
+sizes faked."""
 from types import SimpleNamespace
 
 import pytest
@@ -9,13 +10,15 @@ import torch
 from mun_b200 import autotune
 
 
-def _spec(nelx, nelz, npol, nt, adjoint=True):
-    return SimpleNamespace(plan=SimpleNamespace(nelx=nelx, nelz=nelz, npol=npol, nt=nt), adjoint=adjoint)
-
-
-def _history_bytes(nelx, nelz, npol, nt):
+def _history_bytes(nelx, nelz, npol, k):
     nxg, nzg = nelx * npol + 1, nelz * npol + 1
-    return (nt + 8) * ((nxg + 31) // 32 * 32) * nzg * 4
+    return (k + 8) * ((nxg + 31) // 32 * 32) * nzg * 4
+
+
+def _spec(nelx, nelz, npol, nt, adjoint=True):
+    plan = SimpleNamespace(nelx=nelx, nelz=nelz, npol=npol, nt=nt,
+                           workspace_bytes=lambda flags, k: _history_bytes(nelx, nelz, npol, k))
+    return SimpleNamespace(plan=plan, adjoint=adjoint, flags=1 if adjoint else 0)
 
 
 @pytest.mark.parametrize("free_gb,expect", [(179.0, 2), (400.0, 1), (60.0, 5)])
