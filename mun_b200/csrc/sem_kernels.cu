@@ -244,8 +244,6 @@ __device__ __forceinline__ bool grad_folds(const SolveDev& s, int t) { return (t
 __device__ __forceinline__ float sens_product(float beta, float dw, float du) {
   return __fmul_rn(__fmul_rn(beta, dw), du);
 }
-// Squared residual accumulated into a receiver's misfit (multiply, then add).
-__device__ __forceinline__ void misfit_add(double* m, double res) { *m = __dadd_rn(*m, __dmul_rn(res, res)); }
 
 // One receiver's read-out sum_e w_e u_e computed by one thread with the roundings of the
 // one-warp form the tile kernel uses: lane l sums terms l, l + 32, ... by FMA from zero,
